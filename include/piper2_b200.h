@@ -1,0 +1,266 @@
+/*
+ * piper2_b200.h -- C ABI of the B200 path-tracing accelerator and tracer for Piper2.
+ *
+ * Plain C: fixed-width integers, floats, pointers and sizes.  No CUDA, C++ or torch types cross this
+ * boundary; streams are passed as `void*` (a cudaStream_t, NULL = the legacy default stream).
+ * Every function returns PB2_OK (0) or a PB2_ERR_* code; pb2_last_error() returns the message of
+ * the last failure on the calling thread.  This replaces the reference's error path, which logs and
+ * calls std::abort() (Src/PiperCore.cpp:533-538).
+ *
+ * Device pointers ("_dev") must stay valid until the work queued on `stream` completes.  Host
+ * pointers ("_host") are read or written before the call returns.
+ *
+ * Layouts follow the reference's POD payloads where the reference has one, cited per type.
+ */
+#ifndef PIPER2_B200_H
+#define PIPER2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB2_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------------------------- */
+#define PB2_OK 0
+#define PB2_ERR_INVALID_ARGUMENT 1
+#define PB2_ERR_CUDA 2
+#define PB2_ERR_OUT_OF_MEMORY 3
+#define PB2_ERR_NOT_SUPPORTED 4
+#define PB2_ERR_DEVICE_TIMEOUT 5 /* a bounded device-side wait gave up (see the call's doc) */
+#define PB2_ERR_QUEUE_OVERFLOW 6
+
+/* ---- rays and hits (Src/Kernel/Protocol.hpp:31-35 RayInfo; Embree.cpp:281-295 ray/hit) ------ */
+typedef struct pb2_ray {
+    float org[3];
+    float tmin; /* hit accepted only for tmin < t */
+    float dir[3];
+    float tmax; /* ... and t < tmax */
+} pb2_ray; /* 32 bytes */
+
+#define PB2_INVALID_PRIM 0xFFFFFFFFu
+typedef struct pb2_hit {
+    float t;
+    uint32_t prim; /* global triangle index, PB2_INVALID_PRIM on a miss */
+    float u, v;    /* barycentrics weighting vertex index[1] and index[2] (Embree convention,
+                      Src/BuiltinComponent/Tracer/Embree/Kernel.cpp:175-178) */
+} pb2_hit; /* 16 bytes */
+
+/* ---- scene description ----------------------------------------------------------------------- */
+
+/* One triangle mesh placed in the scene.  Mirrors TriangleIndexedGeometryDesc
+ * (Src/Interface/BuiltinComponent/Tracer.hpp:51-63) plus the GSM instance (geometry + surface,
+ * Tracer.hpp:146-147) and its node transform (Tracer.hpp:148).  Transforms are translation-only:
+ * the reference inverts instance transforms with calcInverse (Src/Kernel/Transform.hpp:344-362),
+ * which is wrong for any rotation or scale, so scenes bake those into the vertices. */
+typedef struct pb2_mesh {
+    const float* vertices;    /* vert_count * 3 floats */
+    const uint32_t* indices;  /* tri_count * 3 */
+    const float* texcoords;   /* vert_count * 2 floats, or NULL */
+    uint32_t vert_count;
+    uint32_t tri_count;
+    uint32_t material;        /* index into pb2_scene.materials */
+    float translation[3];
+} pb2_mesh;
+
+/* Parallelogram primitive of the BasicShapes "Plane" geometry: PerPlaneData
+ * (Src/BuiltinComponent/Geometry/BasicShapes/Shared.hpp:22-28), byte-compatible (64 bytes).
+ * Fill it with pb2_plane_make(). */
+typedef struct pb2_plane {
+    float origin[3];
+    float u[3];
+    float v[3];
+    float normal[3];
+    float tangent[3];
+    uint32_t max_det_comp;
+} pb2_plane;
+
+/* A "Diffuse" area light over a Plane geometry (Src/BuiltinComponent/Light/AreaLight/Shared.hpp:22-26,
+ * AreaLight.cpp:36-57).  Its planes are pb2_scene.planes[first_plane .. first_plane+plane_count). */
+typedef struct pb2_area_light {
+    float radiance[3];
+    uint32_t first_plane;
+    uint32_t plane_count;
+    float translation[3];
+} pb2_area_light;
+
+/* Surfaces of the "Classic" module (Src/BuiltinComponent/Surface/Classic/Classic.cpp:30-199) with
+ * constant textures (Src/BuiltinComponent/Texture/ProceduralTexture/Kernel.cpp:21-26). */
+enum pb2_surface_type {
+    PB2_SURFACE_BLACKBODY = 0, /* no fields */
+    PB2_SURFACE_MATTE = 1,     /* color0 = Diffuse, roughness[0] = Roughness (0 -> Lambert) */
+    PB2_SURFACE_PLASTIC = 2,   /* color0 = Diffuse, color1 = Specular, roughness[0] = Roughness */
+    PB2_SURFACE_GLASS = 3,     /* color0 = Reflection, color1 = Transmission, roughness = X, Y */
+    PB2_SURFACE_MIRROR = 4,    /* color0 = Reflection */
+    PB2_SURFACE_SUBSTRATE = 5, /* color0 = Diffuse, color1 = Specular, roughness = X, Y */
+    PB2_SURFACE_CONDUCTOR = 6  /* extension, no reference counterpart: GGX reflection with the
+                                  Schlick Fresnel of color1 as F0, roughness[0] = alpha */
+};
+typedef struct pb2_material {
+    uint32_t type;
+    float color0[4];
+    float color1[4];
+    float roughness[2];
+} pb2_material; /* 44 bytes */
+
+/* Perspective camera (Src/BuiltinComponent/Sensor/PerspectiveCamera/Shared.hpp:22-29, config parse
+ * PerspectiveCamera.cpp:35-46).  `position` is the camera node's translation (the reference reads it
+ * from the node transform, Kernel.cpp:26-29).  Sizes in metres: the reference's config is in mm and
+ * is scaled by 1e-3f on load; pb2_camera_from_config() does the same conversion. */
+typedef struct pb2_camera {
+    float position[3];
+    float look_at[3];
+    float up[3];          /* normalised */
+    float sensor_size[2]; /* metres */
+    float focal_length;   /* metres */
+    float aperture_radius;/* metres = focal_length / (2 FStop) */
+} pb2_camera;
+
+typedef struct pb2_scene {
+    const pb2_mesh* meshes;
+    uint32_t mesh_count;
+    const pb2_plane* planes;
+    uint32_t plane_count;
+    const pb2_area_light* area_lights;
+    uint32_t area_light_count;
+    const pb2_material* materials;
+    uint32_t material_count;
+    float env_radiance[3]; /* the single "SampledEnvironment" light, lights[0] (Embree.cpp:1174-1188) */
+} pb2_scene;
+
+/* ---- render settings (component configs) -------------------------------------------------- */
+enum pb2_filter_type { PB2_FILTER_BOX = 0, PB2_FILTER_TRIANGLE = 1, PB2_FILTER_GAUSSIAN = 2 };
+enum pb2_fit_mode { PB2_FIT_FILL = 0, PB2_FIT_OVERSCAN = 1 };
+
+typedef struct pb2_render_settings {
+    uint32_t width, height;   /* film resolution */
+    uint32_t fit_mode;        /* pb2_fit_mode, Src/Interface/BuiltinComponent/Sensor.hpp:36-75 */
+    uint32_t samples_per_pixel;/* ScrambledSobolSampler "SamplesPerPixel": rounded up to a power of 2
+                                  (ScrambledSobolSampler.cpp:43-50) */
+    uint32_t scramble;        /* must be 0: "Scramble" is notImplemented in the reference (:51-53) */
+    uint32_t max_depth;       /* PathTracing "MaxTraceDepth" (PathTracing.cpp:38) */
+    uint32_t min_rr_depth;    /* PathTracing "MinRussianRouletteDepth" (PathTracing.cpp:39) */
+    uint32_t filter;          /* pb2_filter_type (FixedSampler.cpp:38-45) */
+    float gaussian_alpha;     /* "Alpha" of the gaussian filter */
+    pb2_camera camera;
+} pb2_render_settings;
+
+/* Render rectangle (Tracer.hpp:96-98 RenderRECT). */
+typedef struct pb2_rect {
+    uint32_t left, top, width, height;
+} pb2_rect;
+
+/* The NDC transform of calcRenderRECT (Protocol.hpp:113-115 SensorNDCAffineTransform). */
+typedef struct pb2_ndc_transform {
+    float ox, oy, sx, sy;
+} pb2_ndc_transform;
+
+/* Per-launch statistics, the counters the reference's EmbreeProfiler collects
+ * (Embree.cpp:1266-1271, PathTracing.cpp:48-54) reduced once per launch. */
+typedef struct pb2_launch_stats {
+    uint64_t closest_rays;  /* camera + continuation + pass-through + MIS-BSDF rays */
+    uint64_t shadow_rays;
+    uint64_t paths;
+    uint64_t path_vertices;
+    uint32_t depth_histogram[32];
+} pb2_launch_stats;
+
+/* ---- library --------------------------------------------------------------------------------- */
+const char* pb2_last_error(void);
+int pb2_abi_version(void);
+/* Selects the CUDA device for the calling thread (cuCtxSetCurrent analogue of
+ * Src/Infrastructure/Accelerator/CUDA/CUDA.cpp:204-210). */
+int pb2_set_device(int device);
+
+/* ---- component helpers (host) -------------------------------------------------------------- */
+/* Plane primitive from Origin/U/V (BasicShapes.cpp:70-89). */
+int pb2_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out);
+/* Camera from the PerspectiveCamera config keys in their config units (mm, FStop)
+ * (PerspectiveCamera.cpp:39-44). */
+int pb2_camera_from_config(const float position[3], const float look_at[3], const float up[3],
+                           const float sensor_size_mm[2], float focal_length_mm, float fstop,
+                           pb2_camera* out);
+/* calcRenderRECT (Src/Interface/BuiltinComponent/Sensor.hpp:38-75). */
+int pb2_calc_render_rect(uint32_t width, uint32_t height, float device_aspect, uint32_t fit_mode,
+                         pb2_ndc_transform* transform, pb2_rect* rect);
+
+/* ---- Sobol sampler (Src/BuiltinComponent/Sampler/ScrambledSobolSampler/Kernel.cpp) ----------- */
+/* sobolGenerate (:65-67) for n (index, dimension) pairs, on the device. */
+int pb2_sobol_generate(const uint64_t* index_dev, const uint32_t* dim_dev, uint32_t n, float* out_dev,
+                       void* stream);
+/* sobolStart (:52-62) for n (px, py, sample) triples: writes the global index and pixel offset. */
+int pb2_sobol_start(uint32_t log2_resolution, const uint32_t* pixel_sample_dev, uint32_t n,
+                    uint64_t* index_dev, float* offset_dev, void* stream);
+/* SHA-256 (hex) of the generated Sobol tables compiled into the library. */
+const char* pb2_sobol_table_digest(void);
+
+/* ---- acceleration structure and traversal (replaces Tracer::buildAcceleration and Embree's
+ *      rtcIntersect1/rtcOccluded1, Embree.cpp:267-391, 497-655) ------------------------------- */
+typedef struct pb2_accel pb2_accel;
+
+typedef struct pb2_accel_info {
+    uint32_t triangle_count;
+    uint32_t node_count;       /* 8-wide nodes */
+    uint32_t leaf_triangle_slots;
+    uint32_t plane_count;
+    uint64_t device_bytes;
+    float build_ms;            /* device time of the build */
+} pb2_accel_info;
+
+/* Builds the LBVH -> 8-wide quantised BVH over all scene meshes on the device.  Host scene
+ * arrays are copied during the call. */
+int pb2_accel_create(const pb2_scene* scene, void* stream, pb2_accel** out);
+int pb2_accel_destroy(pb2_accel* accel);
+int pb2_accel_get_info(const pb2_accel* accel, pb2_accel_info* info);
+
+/* Closest hit over triangles and area-light planes (planes reported with prim =
+ * PB2_PLANE_FLAG | plane index).  Ties in t resolve to the lowest prim. */
+#define PB2_PLANE_FLAG 0x80000000u
+int pb2_trace_closest(const pb2_accel* accel, const pb2_ray* rays_dev, uint32_t n, pb2_hit* hits_dev,
+                      void* stream);
+/* Any hit over triangles only (planes never occlude: mask = GSM only, Embree.cpp:378).
+ * occluded_dev[i] = 1 if some triangle has tmin < t < tmax. */
+int pb2_trace_any(const pb2_accel* accel, const pb2_ray* rays_dev, uint32_t n, uint32_t* occluded_dev,
+                  void* stream);
+/* The same two calls with host arrays: copies in, traces, copies out, synchronises `stream`. */
+int pb2_trace_closest_host(const pb2_accel* accel, const pb2_ray* rays_host, uint32_t n,
+                           pb2_hit* hits_host, void* stream);
+int pb2_trace_any_host(const pb2_accel* accel, const pb2_ray* rays_host, uint32_t n,
+                       uint32_t* occluded_host, void* stream);
+/* Traversal work counters of the last trace call on this accel (node visits, triangle tests),
+ * summed over the batch; only filled when counting is enabled. */
+int pb2_accel_set_counting(pb2_accel* accel, int enable);
+int pb2_accel_get_counters(const pb2_accel* accel, uint64_t* node_visits, uint64_t* tri_tests,
+                           void* stream);
+
+/* ---- render pipeline (Tracer::buildPipeline, Pipeline::prepare, TraceLauncher::launch;
+ *      Tracer.hpp:100-119, 153-155; Embree.cpp:978-1304) --------------------------------------- */
+typedef struct pb2_pipeline pb2_pipeline;
+
+int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* settings, void* stream,
+                        pb2_pipeline** out);
+int pb2_pipeline_destroy(pb2_pipeline* pipeline);
+/* Film resolution and full render rectangle (TraceLauncher::getFilmResolution/getRenderRECT). */
+int pb2_pipeline_get_rect(const pb2_pipeline* pipeline, pb2_rect* full_rect, pb2_ndc_transform* ndc);
+/* Renders samples [sample_begin, sample_begin + sample_count) of every pixel of `rect` (a sub-rect of
+ * the full rect) and adds them to the RGBW film `rgbw_dev` (width * height float4, the
+ * FixedSampler film, FixedSampler/Kernel.cpp:22-52).  If `sample_out_dev` is not NULL it receives
+ * per (pixel, sample) the film point and radiance, 5 floats each, in (y, x, sample) order. */
+int pb2_pipeline_launch(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample_begin,
+                        uint32_t sample_count, float* rgbw_dev, float* sample_out_dev, void* stream);
+/* Resolve radiance = rgb / w (FixedSampler.cpp:122-131) into rgb_dev (width * height * 3). */
+int pb2_film_resolve(const float* rgbw_dev, uint32_t pixel_count, float* rgb_dev, void* stream);
+int pb2_pipeline_get_stats(const pb2_pipeline* pipeline, pb2_launch_stats* stats, void* stream);
+/* Camera rays of one sample index for every pixel of `rect` (piperMain + rayGen,
+ * Tracer/Embree/Kernel.cpp:47-90, PerspectiveCamera/Kernel.cpp:22-48): rays_dev gets the ray, and
+ * points_dev the film point (2 floats), in (y, x) order. */
+int pb2_pipeline_camera_rays(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample,
+                             pb2_ray* rays_dev, float* points_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIPER2_B200_H */

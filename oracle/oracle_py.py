@@ -1,0 +1,181 @@
+"""ctypes binding of the CPU oracle (liboracle.so) and of the reference harness (librefcpu.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from piper2_b200 import capi  # noqa: E402  (struct layouts of include/piper2_b200.h)
+
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "librefcpu.so")
+
+_or = None
+_ref = None
+
+
+def oracle():
+    global _or
+    if _or is None:
+        if not os.path.exists(ORACLE_SO):
+            import build_oracle  # noqa: F401
+
+            sys.path.insert(0, HERE)
+            from build_oracle import build_oracle as _b
+
+            _b()
+        h = C.CDLL(ORACLE_SO)
+        h.or_sobol_sample.restype = C.c_float
+        h.or_sobol_sample.argtypes = [C.c_uint64, C.c_uint32]
+        h.or_sobol_interval_to_index.restype = C.c_uint64
+        h.or_sobol_interval_to_index.argtypes = [C.c_uint32] * 4
+        h.or_sobol_start.argtypes = [C.c_uint32] * 5 + [C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        h.or_sobol_digest.restype = C.c_char_p
+        h.or_remap_roughness.restype = C.c_float
+        h.or_remap_roughness.argtypes = [C.c_float]
+        h.or_camera_ray.argtypes = [C.POINTER(capi.Camera), C.c_float, C.c_float, C.c_float, C.c_float,
+                                    C.POINTER(capi.Ray)]
+        h.or_scene_create.restype = C.c_void_p
+        h.or_scene_create.argtypes = [C.POINTER(capi.Scene), C.c_int]
+        h.or_scene_destroy.argtypes = [C.c_void_p]
+        h.or_scene_triangle_count.restype = C.c_uint32
+        h.or_scene_triangle_count.argtypes = [C.c_void_p]
+        h.or_trace_closest.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+        h.or_trace_any.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
+        h.or_trace_counters.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_uint64)]
+        h.or_render.restype = C.c_int
+        h.or_render.argtypes = [C.c_void_p, C.POINTER(capi.RenderSettings), C.POINTER(capi.Rect), C.c_uint32,
+                                C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        h.or_calc_render_rect.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_uint32,
+                                          C.POINTER(capi.NDCTransform), C.POINTER(capi.Rect)]
+        h.or_plane_make.argtypes = [C.POINTER(C.c_float)] * 3 + [C.POINTER(capi.Plane)]
+        h.or_intersect_triangle.restype = C.c_int
+        h.or_intersect_triangle.argtypes = [C.POINTER(C.c_float)] * 4 + [C.POINTER(C.c_float)] * 3
+        _or = h
+    return _or
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(f"{REF_SO} not built (needs the reference sources)")
+        h = C.CDLL(REF_SO)
+        h.ref_scene_create.restype = C.c_void_p
+        h.ref_scene_create.argtypes = [C.POINTER(capi.Scene), C.POINTER(capi.RenderSettings), C.c_int]
+        h.ref_scene_destroy.argtypes = [C.c_void_p]
+        h.ref_render.restype = C.c_int
+        h.ref_render.argtypes = [C.c_void_p, C.POINTER(capi.Rect), C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                 C.c_int]
+        h.ref_sobol_generate.restype = C.c_float
+        h.ref_sobol_generate.argtypes = [C.c_uint64, C.c_uint32]
+        h.ref_sobol_start.argtypes = [C.c_uint32] * 4 + [C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        h.ref_camera_ray.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float)]
+        _ref = h
+    return _ref
+
+
+class OracleScene:
+    """A scene loaded into the oracle (use_bvh for large scenes)."""
+
+    def __init__(self, scene_data, use_bvh=True):
+        self.data = scene_data
+        self._sc, self._keep = scene_data.to_ctypes()
+        self.h = oracle().or_scene_create(C.byref(self._sc), 1 if use_bvh else 0)
+
+    def close(self):
+        if self.h:
+            oracle().or_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def trace_closest(self, rays, threads=0):
+        hits = np.zeros(len(rays), dtype=capi.HIT_DTYPE)
+        rays = np.ascontiguousarray(rays)
+        oracle().or_trace_closest(self.h, rays.ctypes.data, len(rays), hits.ctypes.data, threads or os.cpu_count())
+        return hits
+
+    def trace_any(self, rays, threads=0):
+        occ = np.zeros(len(rays), dtype=np.uint32)
+        rays = np.ascontiguousarray(rays)
+        oracle().or_trace_any(self.h, rays.ctypes.data, len(rays), occ.ctypes.data, threads or os.cpu_count())
+        return occ
+
+    def counters(self, rays, closest=True):
+        nv, nt = C.c_uint64(), C.c_uint64()
+        rays = np.ascontiguousarray(rays)
+        oracle().or_trace_counters(self.h, rays.ctypes.data, len(rays), 1 if closest else 0, C.byref(nv), C.byref(nt))
+        return nv.value, nt.value
+
+    def render(self, settings, rect=None, sample_begin=0, sample_count=None, threads=0, samples=True):
+        st = settings
+        if rect is None:
+            rect = full_rect(st)
+        if sample_count is None:
+            sample_count = st.samples_per_pixel
+        film = np.zeros((st.height, st.width, 4), dtype=np.float32)
+        out = np.zeros((rect.height, rect.width, sample_count, 5), dtype=np.float32) if samples else None
+        rc = oracle().or_render(self.h, C.byref(st), C.byref(rect), sample_begin, sample_count, film.ctypes.data,
+                                out.ctypes.data if out is not None else None, threads or os.cpu_count())
+        if rc != 0:
+            raise RuntimeError(f"or_render failed: {rc}")
+        return film, out
+
+
+class RefScene:
+    """A scene loaded into the reference harness (the reference's kernels compiled natively)."""
+
+    def __init__(self, scene_data, use_bvh=True):
+        self._sc, self._keep = scene_data.to_ctypes()
+        self.settings = scene_data.settings
+        self.h = ref().ref_scene_create(C.byref(self._sc), C.byref(self.settings), 1 if use_bvh else 0)
+
+    def close(self):
+        if self.h:
+            ref().ref_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def render(self, rect=None, sample_begin=0, sample_count=None, threads=0, samples=True):
+        st = self.settings
+        if rect is None:
+            rect = full_rect(st)
+        if sample_count is None:
+            sample_count = st.samples_per_pixel
+        film = np.zeros((st.height, st.width, 4), dtype=np.float32)
+        out = np.zeros((rect.height, rect.width, sample_count, 5), dtype=np.float32) if samples else None
+        ref().ref_render(self.h, C.byref(rect), sample_begin, sample_count, film.ctypes.data,
+                         out.ctypes.data if out is not None else None, threads or os.cpu_count())
+        return film, out
+
+    def camera_ray(self, ndc_x, ndc_y, u1, u2):
+        o = (C.c_float * 6)()
+        ref().ref_camera_ray(self.h, ndc_x, ndc_y, u1, u2, o)
+        return np.array(list(o), dtype=np.float32)
+
+
+def full_rect(settings):
+    tr, rc = capi.NDCTransform(), capi.Rect()
+    cam = settings.camera
+    oracle().or_calc_render_rect(settings.width, settings.height, cam.sensor_size[0] / cam.sensor_size[1],
+                                 settings.fit_mode, C.byref(tr), C.byref(rc))
+    return rc

@@ -1,0 +1,1591 @@
+/*
+ * pb2_oracle.c -- CPU oracle for the Piper2 render path.  TEST INFRASTRUCTURE ONLY (see pb2_oracle.h).
+ *
+ * Build: gcc -std=c11 -O2 -ffp-contract=off -fopenmp -fPIC -shared (no -march=native, no -ffast-math),
+ * so that every float operation is a single IEEE operation in the order written here, which is the
+ * order of the reference's expressions.  File:line citations are relative to the reference's tree.
+ */
+#include "pb2_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../piper2_b200/csrc/pb2_math.h"
+#include "sobol_tables.h"
+
+/* ------------------------------------------------------------------------------------------------
+ * Small vector helpers.  Each returns exactly the reference's operation order.
+ * ---------------------------------------------------------------------------------------------- */
+typedef struct v3 { float x, y, z; } v3;
+static inline v3 mk3(float x, float y, float z) { v3 r = { x, y, z }; return r; }
+static inline v3 add3(v3 a, v3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub3(v3 a, v3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 mul3s(v3 a, float s) { return mk3(a.x * s, a.y * s, a.z * s); }
+static inline v3 div3s(v3 a, float s) { return mk3(a.x / s, a.y / s, a.z / s); }
+static inline v3 neg3(v3 a) { return mk3(-a.x, -a.y, -a.z); }
+/* dot of Vector/Normal: a.x*b.x + a.y*b.y + a.z*b.z (Src/Kernel/Transform.hpp:269-277) */
+static inline float dot3(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* cross (Transform.hpp:193-196, 262-267) */
+static inline v3 cross3(v3 a, v3 b) {
+    return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+/* sqrtSafe (Src/Kernel/PhysicalQuantitySI.hpp:107-110) */
+static inline float sqrt_safe(float v) { return sqrtf(fmaxf(v, 0.0f)); }
+/* lengthSquared / length (Transform.hpp:178-186) */
+static inline float len2_3(v3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+/* Normal(Vector) normalises: v / length(v) (Transform.hpp:244-248) */
+static inline v3 normalize3(v3 a) { return div3s(a, sqrt_safe(len2_3(a))); }
+static inline v3 ld3(const float* p) { return mk3(p[0], p[1], p[2]); }
+
+typedef struct spec { float r, g, b; } spec;
+static inline spec mksp(float r, float g, float b) { spec s = { r, g, b }; return s; }
+static inline spec sp_add(spec a, spec b) { return mksp(a.r + b.r, a.g + b.g, a.b + b.b); }
+static inline spec sp_mul(spec a, spec b) { return mksp(a.r * b.r, a.g * b.g, a.b * b.b); }
+static inline spec sp_muls(spec a, float s) { return mksp(a.r * s, a.g * s, a.b * s); }
+static inline spec sp_divs(spec a, float s) { return mksp(a.r / s, a.g / s, a.b / s); }
+/* Spectrum::valid (Src/Kernel/Protocol.hpp:84-86) */
+static inline int sp_valid(spec a) { return a.r > 0.0f || a.g > 0.0f || a.b > 0.0f; }
+static const spec SP_ZERO = { 0.0f, 0.0f, 0.0f };
+
+/* Constants (PhysicalQuantitySI.hpp:235-257), as float. */
+#define K_PI 3.14159265358979323846f
+#define K_TWO_PI 6.2831853071796f
+#define K_HALF_PI 1.57079632679489661923f
+#define K_QUARTER_PI 0.785398163397448309616f
+#define K_INV_PI 0.318309886183790671538f
+#define K_SQR_PI 9.869604401089358f
+
+/* ------------------------------------------------------------------------------------------------
+ * Sobol sampler (Src/BuiltinComponent/Sampler/ScrambledSobolSampler/Kernel.cpp)
+ * ---------------------------------------------------------------------------------------------- */
+/* sobolSampleImpl (:23-29), scramble = 0 */
+float or_sobol_sample(uint64_t index, uint32_t dim) {
+    uint32_t v = 0;
+    for (uint32_t i = dim * PB2_SOBOL_MATRIX_SIZE; index; index >>= 1, i++)
+        if (index & 1) v ^= pb2_sobol_matrices32[i];
+    return (float)v * 0x1p-32f;
+}
+
+/* sobolIntervalToIndex (:31-50) */
+uint64_t or_sobol_interval_to_index(uint32_t m, uint32_t sample, uint32_t px, uint32_t py) {
+    if (m == 0) return 0;
+    const uint32_t m2 = m << 1;
+    uint64_t index = (uint64_t)sample << m2;
+    uint64_t delta = 0;
+    for (int c = 0; sample; sample >>= 1, ++c)
+        if (sample & 1) delta ^= pb2_vdc_sobol_matrices[m - 1][c];
+    uint64_t b = (((uint64_t)px << m) | py) ^ delta;
+    for (int c = 0; b; b >>= 1, ++c)
+        if (b & 1) index ^= pb2_vdc_sobol_matrices_inv[m - 1][c];
+    return index;
+}
+
+/* sobolStart (:52-62) */
+void or_sobol_start(uint32_t resolution, uint32_t log2_resolution, uint32_t px, uint32_t py, uint32_t sample,
+                    uint64_t* index, float offset[2]) {
+    const uint64_t idx = or_sobol_interval_to_index(log2_resolution, sample, px, py);
+    *index = idx;
+    offset[0] = fminf(fmaxf(or_sobol_sample(idx, 0) * (float)resolution - (float)px, 0.0f), 1.0f);
+    offset[1] = fminf(fmaxf(or_sobol_sample(idx, 1) * (float)resolution - (float)py, 0.0f), 1.0f);
+}
+
+const char* or_sobol_digest(void) { return PB2_SOBOL_TABLE_SHA256; }
+
+/* ------------------------------------------------------------------------------------------------
+ * Host-side component setup
+ * ---------------------------------------------------------------------------------------------- */
+/* MicrofacetDistribution::remapRoughness (Src/BuiltinComponent/Surface/Classic/Kernel.cpp:378-381).
+ * Roughness comes from constant textures, so the remap is done once per material on the host. */
+float or_remap_roughness(float roughness) {
+    const float x = logf(fmaxf(1e-3f, roughness));
+    return fmaxf(1e-3f, 1.62142f + (0.819955f + (0.1734f + (0.0171201f + 0.000640711f * x) * x) * x) * x);
+}
+
+/* Plane construction (Src/BuiltinComponent/Geometry/BasicShapes/BasicShapes.cpp:70-89) */
+void or_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out) {
+    const v3 uu = ld3(u), vv = ld3(v);
+    const v3 det3 = cross3(uu, vv);
+    const float area = sqrt_safe(len2_3(det3));
+    const v3 n = div3s(det3, area);
+    const v3 t = normalize3(uu);
+    const float a0 = fabsf(det3.x), a1 = fabsf(det3.y), a2 = fabsf(det3.z);
+    uint32_t sel;
+    if (a0 >= a1 && a0 >= a2) sel = 0;
+    else sel = (a1 >= a0 && a1 >= a2) ? 1 : 2;
+    memcpy(out->origin, origin, sizeof(float) * 3);
+    memcpy(out->u, u, sizeof(float) * 3);
+    memcpy(out->v, v, sizeof(float) * 3);
+    out->normal[0] = n.x; out->normal[1] = n.y; out->normal[2] = n.z;
+    out->tangent[0] = t.x; out->tangent[1] = t.y; out->tangent[2] = t.z;
+    out->max_det_comp = sel;
+}
+
+/* calcRenderRECT (Src/Interface/BuiltinComponent/Sensor.hpp:38-75) */
+void or_calc_render_rect(uint32_t width, uint32_t height, float device_aspect, uint32_t fit_mode,
+                         pb2_ndc_transform* tr, pb2_rect* rect) {
+    const float iar = (float)width / (float)height;
+    const float iiar = 1.0f / iar;
+    const float idar = 1.0f / device_aspect;
+    if (fit_mode == PB2_FIT_FILL) {
+        rect->left = 0; rect->top = 0; rect->width = width; rect->height = height;
+        if (iar > device_aspect) {
+            tr->ox = 0.0f; tr->oy = (idar - iiar) * 0.5f * device_aspect; tr->sx = 1.0f; tr->sy = iiar * device_aspect;
+        } else {
+            tr->ox = (device_aspect - iar) * 0.5f * idar; tr->oy = 0.0f; tr->sx = iar * idar; tr->sy = 1.0f;
+        }
+    } else {
+        if (iar > device_aspect) {
+            tr->ox = -(iar - device_aspect) * 0.5f * idar; tr->oy = 0.0f; tr->sx = iar * idar; tr->sy = 1.0f;
+            rect->left = (uint32_t)floorf(fmaxf(0.0f, (float)width * (iar - device_aspect) * 0.5f * iiar));
+            rect->top = 0;
+            uint32_t r = (uint32_t)ceilf((float)width * (iar + device_aspect) * 0.5f * iiar);
+            rect->width = (width < r ? width : r) - rect->left;
+            rect->height = height;
+        } else {
+            tr->ox = 0.0f; tr->oy = -(iiar - idar) * 0.5f * device_aspect; tr->sx = 1.0f; tr->sy = device_aspect * iiar;
+            rect->left = 0;
+            rect->top = (uint32_t)floorf(fmaxf(0.0f, (float)height * (iiar - idar) * 0.5f * iar));
+            rect->width = width;
+            rect->height = (uint32_t)ceilf((float)height * (iiar + idar) * 0.5f * iar) - rect->top;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * Camera (Src/BuiltinComponent/Sensor/PerspectiveCamera/Kernel.cpp:22-48)
+ * ---------------------------------------------------------------------------------------------- */
+void or_camera_ray(const pb2_camera* cam, float ndc_x, float ndc_y, float u1, float u2, pb2_ray* ray) {
+    const v3 base = ld3(cam->position);
+    const v3 look = ld3(cam->look_at);
+    const v3 forward = normalize3(sub3(look, base));
+    const v3 right = cross3(forward, ld3(cam->up));
+    const v3 up = cross3(right, forward);
+    const v3 film_hit = add3(add3(base, mul3s(right, cam->sensor_size[0] * (0.5f - ndc_x))),
+                             mul3s(up, cam->sensor_size[1] * (ndc_y - 0.5f)));
+    const float focal_distance = dot3(sub3(look, base), forward);
+    const float film_distance = 1.0f / (1.0f / cam->focal_length - 1.0f / focal_distance);
+    const v3 lens_center = add3(base, mul3s(forward, film_distance));
+    /* sampleUniformDisk (Src/Kernel/Sampling.hpp:24-29) */
+    const float ang = u1 * K_TWO_PI;
+    const float rad = sqrt_safe(u2);
+    float s, c;
+    pb2_sincosf(ang, &s, &c);
+    const float lx = rad * c, ly = rad * s;
+    const v3 lens_hit = add3(add3(lens_center, mul3s(right, cam->aperture_radius * lx)),
+                             mul3s(up, cam->aperture_radius * ly));
+    const v3 dir = sub3(lens_center, film_hit);
+    const v3 focus_hit = add3(lens_center, mul3s(dir, focal_distance / dot3(dir, forward)));
+    const v3 d = normalize3(sub3(focus_hit, lens_hit));
+    ray->org[0] = lens_hit.x; ray->org[1] = lens_hit.y; ray->org[2] = lens_hit.z;
+    ray->dir[0] = d.x; ray->dir[1] = d.y; ray->dir[2] = d.z;
+    ray->tmin = 1e-3f;
+    ray->tmax = 1e5f;
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * Scene and traversal
+ * ---------------------------------------------------------------------------------------------- */
+typedef struct or_node {
+    float bmin[3], bmax[3];
+    uint32_t first; /* leaf: first triangle slot; internal: left child (right = first + 1) */
+    uint32_t count; /* 0 = internal */
+} or_node;
+
+typedef struct or_light {
+    spec radiance;
+    uint32_t first_plane, plane_count;
+    v3 translation;
+    float area, inverse_area;
+} or_light;
+
+struct or_scene {
+    uint32_t ntri;
+    float* tri;          /* 9 floats per triangle, world space */
+    uint32_t* tri_mat;   /* material per triangle */
+    uint32_t nplane;
+    pb2_plane* planes;
+    uint32_t* plane_light; /* area light of each plane */
+    float* plane_cdf;
+    float* plane_pdf;
+    uint32_t nlight;     /* area lights */
+    or_light* lights;
+    uint32_t nmat;
+    pb2_material* mats;
+    float* alpha;        /* remapped roughness x, y per material */
+    spec env;
+    /* BVH */
+    or_node* nodes;
+    uint32_t nnodes;
+    uint32_t* order;     /* triangle slot -> triangle index */
+};
+
+uint32_t or_scene_triangle_count(const or_scene* s) { return s->ntri; }
+
+typedef struct ray_pre {
+    v3 o, d, id;
+    int kx, ky, kz;
+    float sx, sy, sz;
+    float tmin, tmax;
+} ray_pre;
+
+static void ray_prepare(const pb2_ray* r, ray_pre* p) {
+    p->o = ld3(r->org);
+    p->d = ld3(r->dir);
+    const float dd[3] = { r->dir[0], r->dir[1], r->dir[2] };
+    float inv[3];
+    for (int i = 0; i < 3; ++i) inv[i] = dd[i] != 0.0f ? 1.0f / dd[i] : copysignf(FLT_MAX, dd[i]);
+    p->id = mk3(inv[0], inv[1], inv[2]);
+    /* Woop et al. 2013, Sec. 3: kz = dominant axis, swap kx/ky to keep winding when dir[kz] < 0 */
+    int kz = 0;
+    if (fabsf(dd[1]) > fabsf(dd[kz])) kz = 1;
+    if (fabsf(dd[2]) > fabsf(dd[kz])) kz = 2;
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    if (dd[kz] < 0.0f) { int t = kx; kx = ky; ky = t; }
+    p->kx = kx; p->ky = ky; p->kz = kz;
+    p->sx = dd[kx] / dd[kz];
+    p->sy = dd[ky] / dd[kz];
+    p->sz = 1.0f / dd[kz];
+    p->tmin = r->tmin;
+    p->tmax = r->tmax;
+}
+
+static inline float comp(v3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+
+/* Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2(1), 2013), single precision with the
+ * paper's double-precision fallback for edge hits.  t = T / det; barycentrics (U, V, W) / det weight
+ * (v0, v1, v2); the returned (u, v) weight v1 and v2 (Embree's convention). */
+static int tri_test(const ray_pre* p, const float* tri, float* t_out, float* u_out, float* v_out) {
+    const v3 A = sub3(ld3(tri + 0), p->o);
+    const v3 B = sub3(ld3(tri + 3), p->o);
+    const v3 C = sub3(ld3(tri + 6), p->o);
+    const float Az_ = comp(A, p->kz), Bz_ = comp(B, p->kz), Cz_ = comp(C, p->kz);
+    const float Ax = comp(A, p->kx) - p->sx * Az_;
+    const float Ay = comp(A, p->ky) - p->sy * Az_;
+    const float Bx = comp(B, p->kx) - p->sx * Bz_;
+    const float By = comp(B, p->ky) - p->sy * Bz_;
+    const float Cx = comp(C, p->kx) - p->sx * Cz_;
+    const float Cy = comp(C, p->ky) - p->sy * Cz_;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return 0;
+    const float det = U + V + W;
+    if (det == 0.0f) return 0;
+    const float Az = p->sz * Az_, Bz = p->sz * Bz_, Cz = p->sz * Cz_;
+    const float T = U * Az + V * Bz + W * Cz;
+    const float t = T / det;
+    if (!(t > p->tmin && t < p->tmax)) return 0;
+    *t_out = t;
+    *u_out = V / det;
+    *v_out = W / det;
+    return 1;
+}
+
+int or_intersect_triangle(const float ray[8], const float v0[3], const float v1[3], const float v2[3], float* t,
+                          float* u, float* v) {
+    pb2_ray r;
+    memcpy(&r, ray, sizeof(r));
+    ray_pre p;
+    ray_prepare(&r, &p);
+    float tri[9];
+    memcpy(tri, v0, 12); memcpy(tri + 3, v1, 12); memcpy(tri + 6, v2, 12);
+    return tri_test(&p, tri, t, u, v);
+}
+
+/* planeIntersect + calcTexCoord (Src/BuiltinComponent/Geometry/BasicShapes/Kernel.cpp:30-79), in the
+ * plane's local frame; Embree hands the callback a re-normalised direction (Embree.cpp:569-577). */
+static int plane_test(const pb2_plane* pl, v3 org_local, v3 dir, float tnear, float tfar, float* t_out,
+                      int* front, float uv[2]) {
+    const v3 d = normalize3(dir);
+    const v3 delta = sub3(ld3(pl->origin), org_local);
+    const v3 n = ld3(pl->normal);
+    const float b = dot3(delta, n);
+    const float k = dot3(d, n);
+    const float t = b / k;
+    if (!(tnear < t && t < tfar)) return 0;
+    const v3 pos = sub3(mul3s(d, t), delta);
+    const v3 u = ld3(pl->u), v = ld3(pl->v);
+    float inv_det, x, y;
+    switch (pl->max_det_comp) {
+        case 0:
+            inv_det = 1.0f / (u.y * v.z - v.y * u.z);
+            x = pos.y * v.z - v.y * pos.z;
+            y = u.y * pos.z - pos.y * u.z;
+            break;
+        case 1:
+            inv_det = 1.0f / (u.z * v.x - v.z * u.x);
+            x = pos.z * v.x - v.z * pos.x;
+            y = u.z * pos.x - pos.z * u.x;
+            break;
+        default:
+            inv_det = 1.0f / (u.x * v.y - v.x * u.y);
+            x = pos.x * v.y - v.x * pos.y;
+            y = u.x * pos.y - pos.x * u.y;
+            break;
+    }
+    const float uu = x * inv_det, vv = y * inv_det;
+    if (!(0.0f <= uu && uu <= 1.0f && 0.0f <= vv && vv <= 1.0f)) return 0;
+    *t_out = t;
+    *front = k > 0.0f;
+    uv[0] = uu; uv[1] = vv;
+    return 1;
+}
+
+/* Conservative slab test: the far distance is widened by 3 ulp-scale (Ize 2013, "Robust BVH Ray
+ * Traversal"), so rounding never culls a box holding the true closest hit. */
+static inline int box_test(const ray_pre* p, const float* bmin, const float* bmax, float tbest, float* tnear_out) {
+    const float tx0 = (bmin[0] - p->o.x) * p->id.x, tx1 = (bmax[0] - p->o.x) * p->id.x;
+    const float ty0 = (bmin[1] - p->o.y) * p->id.y, ty1 = (bmax[1] - p->o.y) * p->id.y;
+    const float tz0 = (bmin[2] - p->o.z) * p->id.z, tz1 = (bmax[2] - p->o.z) * p->id.z;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), p->tmin));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.0000004f;
+    *tnear_out = tn;
+    return tn <= fminf(tf, tbest);
+}
+
+typedef struct or_hit_rec {
+    float t, u, v;
+    uint32_t prim; /* triangle index or PB2_PLANE_FLAG | plane */
+    int front;     /* planes only */
+} or_hit_rec;
+
+static inline void consider_tri(const or_scene* s, const ray_pre* p, uint32_t prim, or_hit_rec* h) {
+    float t, u, v;
+    if (tri_test(p, s->tri + 9 * (size_t)prim, &t, &u, &v)) {
+        if (t < h->t || (t == h->t && prim < h->prim)) {
+            h->t = t; h->u = u; h->v = v; h->prim = prim;
+        }
+    }
+}
+
+static void closest_tris(const or_scene* s, const ray_pre* p, or_hit_rec* h, uint64_t* nv, uint64_t* nt) {
+    if (!s->nodes) {
+        for (uint32_t i = 0; i < s->ntri; ++i) consider_tri(s, p, i, h);
+        if (nt) *nt += s->ntri;
+        return;
+    }
+    uint32_t stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const or_node* n = &s->nodes[stack[--sp]];
+        float tn;
+        if (nv) (*nv)++;
+        if (!box_test(p, n->bmin, n->bmax, h->t, &tn)) continue;
+        if (n->count) {
+            for (uint32_t i = 0; i < n->count; ++i) consider_tri(s, p, s->order[n->first + i], h);
+            if (nt) *nt += n->count;
+        } else {
+            const or_node* l = &s->nodes[n->first];
+            const or_node* r = &s->nodes[n->first + 1];
+            float tl, tr;
+            const int hl = box_test(p, l->bmin, l->bmax, h->t, &tl);
+            const int hr = box_test(p, r->bmin, r->bmax, h->t, &tr);
+            if (hl && hr) {
+                if (tl <= tr) { stack[sp++] = n->first + 1; stack[sp++] = n->first; }
+                else { stack[sp++] = n->first; stack[sp++] = n->first + 1; }
+            } else if (hl) stack[sp++] = n->first;
+            else if (hr) stack[sp++] = n->first + 1;
+        }
+    }
+}
+
+static int any_tris(const or_scene* s, const ray_pre* p, uint64_t* nv, uint64_t* nt) {
+    float t, u, v;
+    if (!s->nodes) {
+        for (uint32_t i = 0; i < s->ntri; ++i) {
+            if (nt) (*nt)++;
+            if (tri_test(p, s->tri + 9 * (size_t)i, &t, &u, &v)) return 1;
+        }
+        return 0;
+    }
+    uint32_t stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const or_node* n = &s->nodes[stack[--sp]];
+        float tn;
+        if (nv) (*nv)++;
+        if (!box_test(p, n->bmin, n->bmax, p->tmax, &tn)) continue;
+        if (n->count) {
+            for (uint32_t i = 0; i < n->count; ++i) {
+                if (nt) (*nt)++;
+                if (tri_test(p, s->tri + 9 * (size_t)s->order[n->first + i], &t, &u, &v)) return 1;
+            }
+        } else {
+            stack[sp++] = n->first + 1;
+            stack[sp++] = n->first;
+        }
+    }
+    return 0;
+}
+
+/* Closest hit of one ray over triangles then planes (planes lose ties: a plane is accepted only
+ * strictly before the current closest t, as the callback sees tFar, BasicShapes/Kernel.cpp:69). */
+static void closest_one(const or_scene* s, const pb2_ray* r, or_hit_rec* h) {
+    ray_pre p;
+    ray_prepare(r, &p);
+    h->t = r->tmax;
+    h->prim = PB2_INVALID_PRIM;
+    h->u = h->v = 0.0f;
+    h->front = 0;
+    closest_tris(s, &p, h, NULL, NULL);
+    for (uint32_t i = 0; i < s->nplane; ++i) {
+        const or_light* L = &s->lights[s->plane_light[i]];
+        const v3 ol = sub3(p.o, L->translation);
+        float t, uv[2];
+        int front;
+        if (plane_test(&s->planes[i], ol, p.d, r->tmin, h->t, &t, &front, uv)) {
+            h->t = t; h->prim = PB2_PLANE_FLAG | i; h->front = front; h->u = uv[0]; h->v = uv[1];
+        }
+    }
+}
+
+void or_trace_closest(const or_scene* s, const pb2_ray* rays, uint32_t n, pb2_hit* hits, int threads) {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads > 0 ? threads : 1)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        or_hit_rec h;
+        closest_one(s, &rays[i], &h);
+        hits[i].t = h.prim == PB2_INVALID_PRIM ? rays[i].tmax : h.t;
+        hits[i].prim = h.prim;
+        hits[i].u = h.u;
+        hits[i].v = h.v;
+    }
+}
+
+void or_trace_any(const or_scene* s, const pb2_ray* rays, uint32_t n, uint32_t* occluded, int threads) {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads > 0 ? threads : 1)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        ray_pre p;
+        ray_prepare(&rays[i], &p);
+        occluded[i] = (uint32_t)any_tris(s, &p, NULL, NULL);
+    }
+}
+
+int or_closest_triangle(const or_scene* s, const pb2_ray* ray, pb2_hit* hit) {
+    ray_pre p;
+    ray_prepare(ray, &p);
+    or_hit_rec h;
+    h.t = ray->tmax; h.prim = PB2_INVALID_PRIM; h.u = h.v = 0.0f; h.front = 0;
+    closest_tris(s, &p, &h, NULL, NULL);
+    hit->t = h.t; hit->prim = h.prim; hit->u = h.u; hit->v = h.v;
+    return h.prim != PB2_INVALID_PRIM;
+}
+
+int or_any_triangle(const or_scene* s, const pb2_ray* ray) {
+    ray_pre p;
+    ray_prepare(ray, &p);
+    return any_tris(s, &p, NULL, NULL);
+}
+
+const float* or_triangle_vertices(const or_scene* s, uint32_t prim) { return s->tri + 9 * (size_t)prim; }
+
+void or_trace_counters(const or_scene* s, const pb2_ray* rays, uint32_t n, int closest, uint64_t* node_visits,
+                       uint64_t* tri_tests) {
+    uint64_t nv = 0, nt = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        ray_pre p;
+        ray_prepare(&rays[i], &p);
+        if (closest) {
+            or_hit_rec h;
+            h.t = rays[i].tmax; h.prim = PB2_INVALID_PRIM;
+            closest_tris(s, &p, &h, &nv, &nt);
+        } else {
+            any_tris(s, &p, &nv, &nt);
+        }
+    }
+    *node_visits = nv;
+    *tri_tests = nt;
+}
+
+/* ---- binned SAH BVH over triangle centroids --------------------------------------------------- */
+typedef struct build_ctx {
+    const float* tri;
+    float* cen;       /* 3 per triangle */
+    float* tbmin;     /* 3 per triangle */
+    float* tbmax;
+    uint32_t* order;
+    or_node* nodes;
+    uint32_t nnodes;
+} build_ctx;
+
+static float area_of(const float* mn, const float* mx) {
+    const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    if (dx < 0.0f) return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+#define OR_BINS 16
+static void build_rec(build_ctx* c, uint32_t node, uint32_t first, uint32_t count) {
+    or_node* n = &c->nodes[node];
+    float mn[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, mx[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+    float cmn[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, cmx[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+    for (uint32_t i = first; i < first + count; ++i) {
+        const uint32_t t = c->order[i];
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], c->tbmin[3 * t + k]);
+            mx[k] = fmaxf(mx[k], c->tbmax[3 * t + k]);
+            cmn[k] = fminf(cmn[k], c->cen[3 * t + k]);
+            cmx[k] = fmaxf(cmx[k], c->cen[3 * t + k]);
+        }
+    }
+    memcpy(n->bmin, mn, 12);
+    memcpy(n->bmax, mx, 12);
+    if (count <= 4) {
+        n->first = first; n->count = count;
+        return;
+    }
+    int best_axis = -1, best_split = 0;
+    float best_cost = FLT_MAX;
+    for (int axis = 0; axis < 3; ++axis) {
+        const float ext = cmx[axis] - cmn[axis];
+        if (!(ext > 0.0f)) continue;
+        uint32_t bcnt[OR_BINS] = { 0 };
+        float bmn[OR_BINS][3], bmx[OR_BINS][3];
+        for (int b = 0; b < OR_BINS; ++b)
+            for (int k = 0; k < 3; ++k) { bmn[b][k] = FLT_MAX; bmx[b][k] = -FLT_MAX; }
+        const float scale = (float)OR_BINS / ext;
+        for (uint32_t i = first; i < first + count; ++i) {
+            const uint32_t t = c->order[i];
+            int b = (int)((c->cen[3 * t + axis] - cmn[axis]) * scale);
+            if (b >= OR_BINS) b = OR_BINS - 1;
+            if (b < 0) b = 0;
+            bcnt[b]++;
+            for (int k = 0; k < 3; ++k) {
+                bmn[b][k] = fminf(bmn[b][k], c->tbmin[3 * t + k]);
+                bmx[b][k] = fmaxf(bmx[b][k], c->tbmax[3 * t + k]);
+            }
+        }
+        float lmn[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, lmx[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+        float larea[OR_BINS];
+        uint32_t lcnt[OR_BINS];
+        uint32_t acc = 0;
+        for (int b = 0; b < OR_BINS - 1; ++b) {
+            for (int k = 0; k < 3; ++k) { lmn[k] = fminf(lmn[k], bmn[b][k]); lmx[k] = fmaxf(lmx[k], bmx[b][k]); }
+            acc += bcnt[b];
+            larea[b] = area_of(lmn, lmx);
+            lcnt[b] = acc;
+        }
+        float rmn[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, rmx[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+        uint32_t racc = 0;
+        for (int b = OR_BINS - 1; b > 0; --b) {
+            for (int k = 0; k < 3; ++k) { rmn[k] = fminf(rmn[k], bmn[b][k]); rmx[k] = fmaxf(rmx[k], bmx[b][k]); }
+            racc += bcnt[b];
+            const uint32_t l = lcnt[b - 1];
+            if (l == 0 || racc == 0) continue;
+            const float cost = larea[b - 1] * (float)l + area_of(rmn, rmx) * (float)racc;
+            if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = b; }
+        }
+    }
+    uint32_t mid;
+    if (best_axis < 0) {
+        mid = first + count / 2; /* all centroids equal: median split by index */
+    } else {
+        const float ext = cmx[best_axis] - cmn[best_axis];
+        const float scale = (float)OR_BINS / ext;
+        uint32_t i = first, j = first + count;
+        while (i < j) {
+            const uint32_t t = c->order[i];
+            int b = (int)((c->cen[3 * t + best_axis] - cmn[best_axis]) * scale);
+            if (b >= OR_BINS) b = OR_BINS - 1;
+            if (b < 0) b = 0;
+            if (b < best_split) ++i;
+            else { --j; const uint32_t tmp = c->order[i]; c->order[i] = c->order[j]; c->order[j] = tmp; }
+        }
+        mid = i;
+        if (mid == first || mid == first + count) mid = first + count / 2;
+    }
+    const uint32_t left = c->nnodes;
+    c->nnodes += 2;
+    n = &c->nodes[node];
+    n->first = left;
+    n->count = 0;
+    build_rec(c, left, first, mid - first);
+    build_rec(c, left + 1, mid, first + count - mid);
+}
+
+static void build_bvh(or_scene* s) {
+    build_ctx c;
+    const uint32_t nt = s->ntri;
+    c.tri = s->tri;
+    c.cen = (float*)malloc(sizeof(float) * 3 * nt);
+    c.tbmin = (float*)malloc(sizeof(float) * 3 * nt);
+    c.tbmax = (float*)malloc(sizeof(float) * 3 * nt);
+    c.order = (uint32_t*)malloc(sizeof(uint32_t) * nt);
+    c.nodes = (or_node*)malloc(sizeof(or_node) * (2 * (size_t)nt + 1));
+    c.nnodes = 1;
+    for (uint32_t i = 0; i < nt; ++i) {
+        const float* t = s->tri + 9 * (size_t)i;
+        for (int k = 0; k < 3; ++k) {
+            const float a = t[k], b = t[3 + k], d = t[6 + k];
+            c.tbmin[3 * i + k] = fminf(a, fminf(b, d));
+            c.tbmax[3 * i + k] = fmaxf(a, fmaxf(b, d));
+            c.cen[3 * i + k] = 0.5f * (c.tbmin[3 * i + k] + c.tbmax[3 * i + k]);
+        }
+        c.order[i] = i;
+    }
+    build_rec(&c, 0, 0, nt);
+    free(c.cen);
+    free(c.tbmin);
+    free(c.tbmax);
+    s->nodes = c.nodes;
+    s->nnodes = c.nnodes;
+    s->order = c.order;
+}
+
+or_scene* or_scene_create(const pb2_scene* d, int use_bvh) {
+    or_scene* s = (or_scene*)calloc(1, sizeof(or_scene));
+    uint64_t nt = 0;
+    for (uint32_t m = 0; m < d->mesh_count; ++m) nt += d->meshes[m].tri_count;
+    s->ntri = (uint32_t)nt;
+    s->tri = (float*)malloc(sizeof(float) * 9 * (nt ? nt : 1));
+    s->tri_mat = (uint32_t*)malloc(sizeof(uint32_t) * (nt ? nt : 1));
+    uint64_t k = 0;
+    for (uint32_t m = 0; m < d->mesh_count; ++m) {
+        const pb2_mesh* mesh = &d->meshes[m];
+        for (uint32_t i = 0; i < mesh->tri_count; ++i, ++k) {
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t vi = mesh->indices[3 * i + j];
+                for (int a = 0; a < 3; ++a) s->tri[9 * k + 3 * j + a] = mesh->vertices[3 * vi + a] + mesh->translation[a];
+            }
+            s->tri_mat[k] = mesh->material;
+        }
+    }
+    s->nplane = d->plane_count;
+    s->planes = (pb2_plane*)malloc(sizeof(pb2_plane) * (d->plane_count ? d->plane_count : 1));
+    s->plane_light = (uint32_t*)calloc(d->plane_count ? d->plane_count : 1, sizeof(uint32_t));
+    s->plane_cdf = (float*)calloc(d->plane_count ? d->plane_count : 1, sizeof(float));
+    s->plane_pdf = (float*)calloc(d->plane_count ? d->plane_count : 1, sizeof(float));
+    if (d->plane_count) memcpy(s->planes, d->planes, sizeof(pb2_plane) * d->plane_count);
+    s->nlight = d->area_light_count;
+    s->lights = (or_light*)calloc(d->area_light_count ? d->area_light_count : 1, sizeof(or_light));
+    for (uint32_t l = 0; l < d->area_light_count; ++l) {
+        const pb2_area_light* al = &d->area_lights[l];
+        or_light* L = &s->lights[l];
+        L->radiance = mksp(al->radiance[0], al->radiance[1], al->radiance[2]);
+        L->first_plane = al->first_plane;
+        L->plane_count = al->plane_count;
+        L->translation = ld3(al->translation);
+        /* BasicShapes.cpp:76-94: running area -> cdf, per-plane area -> pdf, both / total */
+        float total = 0.0f;
+        for (uint32_t i = 0; i < al->plane_count; ++i) {
+            const pb2_plane* pl = &d->planes[al->first_plane + i];
+            const float area = sqrt_safe(len2_3(cross3(ld3(pl->u), ld3(pl->v))));
+            total = total + area;
+            s->plane_cdf[al->first_plane + i] = total;
+            s->plane_pdf[al->first_plane + i] = area;
+            s->plane_light[al->first_plane + i] = l;
+        }
+        for (uint32_t i = 0; i < al->plane_count; ++i) {
+            s->plane_cdf[al->first_plane + i] = s->plane_cdf[al->first_plane + i] / total;
+            s->plane_pdf[al->first_plane + i] = s->plane_pdf[al->first_plane + i] / total;
+        }
+        L->area = total;
+        L->inverse_area = 1.0f / total;
+    }
+    s->nmat = d->material_count;
+    s->mats = (pb2_material*)malloc(sizeof(pb2_material) * (d->material_count ? d->material_count : 1));
+    s->alpha = (float*)malloc(sizeof(float) * 2 * (d->material_count ? d->material_count : 1));
+    if (d->material_count) memcpy(s->mats, d->materials, sizeof(pb2_material) * d->material_count);
+    for (uint32_t m = 0; m < d->material_count; ++m) {
+        const pb2_material* mt = &d->materials[m];
+        if (mt->type == PB2_SURFACE_CONDUCTOR) {
+            s->alpha[2 * m] = mt->roughness[0];
+            s->alpha[2 * m + 1] = mt->roughness[0];
+        } else if (mt->type == PB2_SURFACE_PLASTIC) {
+            s->alpha[2 * m] = or_remap_roughness(mt->roughness[0]);
+            s->alpha[2 * m + 1] = s->alpha[2 * m];
+        } else {
+            s->alpha[2 * m] = or_remap_roughness(mt->roughness[0]);
+            s->alpha[2 * m + 1] = or_remap_roughness(mt->roughness[1]);
+        }
+    }
+    s->env = mksp(d->env_radiance[0], d->env_radiance[1], d->env_radiance[2]);
+    if (use_bvh && s->ntri > 0) build_bvh(s);
+    return s;
+}
+
+void or_scene_destroy(or_scene* s) {
+    if (!s) return;
+    free(s->tri); free(s->tri_mat); free(s->planes); free(s->plane_light); free(s->plane_cdf);
+    free(s->plane_pdf); free(s->lights); free(s->mats); free(s->alpha); free(s->nodes); free(s->order);
+    free(s);
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * Surface geometry at a hit
+ * ---------------------------------------------------------------------------------------------- */
+enum { KIND_SURFACE = 0, KIND_AREA_LIGHT = 1, KIND_MISSING = 2 };
+
+typedef struct surf_info {
+    int kind;
+    float t;
+    v3 T, B, N, Ng; /* local frame == world frame (translation-only instances) */
+    int front;
+    uint32_t material;
+    uint32_t light; /* area light index */
+} surf_info;
+
+/* piperEmbreeTrace (Src/BuiltinComponent/Tracer/Embree/Embree.cpp:267-355) with
+ * calcTriangleMeshSurface (Tracer/Embree/Kernel.cpp:170-192) and planeSurface
+ * (BasicShapes/Kernel.cpp:101-111). */
+static void trace_surface(const or_scene* s, v3 o, v3 d, float tmin, float tmax, surf_info* si, uint64_t* nrays) {
+    pb2_ray r;
+    r.org[0] = o.x; r.org[1] = o.y; r.org[2] = o.z;
+    r.dir[0] = d.x; r.dir[1] = d.y; r.dir[2] = d.z;
+    r.tmin = tmin; r.tmax = tmax;
+    or_hit_rec h;
+    closest_one(s, &r, &h);
+    if (nrays) (*nrays)++;
+    if (h.prim == PB2_INVALID_PRIM) {
+        si->kind = KIND_MISSING;
+        return;
+    }
+    si->t = h.t;
+    if (h.prim & PB2_PLANE_FLAG) {
+        const uint32_t pi = h.prim & ~PB2_PLANE_FLAG;
+        const pb2_plane* pl = &s->planes[pi];
+        si->kind = KIND_AREA_LIGHT;
+        si->light = s->plane_light[pi];
+        si->front = h.front;
+        const v3 n = ld3(pl->normal);
+        si->Ng = h.front ? neg3(n) : n;
+        si->N = si->Ng;
+        si->T = ld3(pl->tangent);
+        si->B = cross3(si->N, si->T);
+        return;
+    }
+    const float* tri = s->tri + 9 * (size_t)h.prim;
+    const v3 p0 = ld3(tri), p1 = ld3(tri + 3), p2 = ld3(tri + 6);
+    const v3 ng = normalize3(cross3(sub3(p1, p0), sub3(p2, p0)));
+    const int front = dot3(d, ng) < 0.0f;
+    si->kind = KIND_SURFACE;
+    si->front = front;
+    si->material = s->tri_mat[h.prim];
+    si->N = si->Ng = front ? ng : neg3(ng);
+    const v3 e1 = mk3(1.0f, 0.0f, 0.0f), e2 = mk3(0.0f, 1.0f, 0.0f);
+    if (fabsf(dot3(si->N, e1)) < fabsf(dot3(si->N, e2)))
+        si->T = cross3(si->N, e1);
+    else
+        si->T = cross3(si->N, e2);
+    si->B = cross3(si->N, si->T);
+}
+
+static int occluded(const or_scene* s, v3 o, v3 d, float tmin, float tmax, uint64_t* nrays) {
+    pb2_ray r;
+    r.org[0] = o.x; r.org[1] = o.y; r.org[2] = o.z;
+    r.dir[0] = d.x; r.dir[1] = d.y; r.dir[2] = d.z;
+    r.tmin = tmin; r.tmax = tmax;
+    ray_pre p;
+    ray_prepare(&r, &p);
+    if (nrays) (*nrays)++;
+    return any_tris(s, &p, NULL, NULL);
+}
+
+/* SurfaceIntersectionInfo::local2Shading / shading2Local (Src/Kernel/Protocol.hpp:55-66) */
+static inline v3 to_shading(const surf_info* si, v3 v) { return mk3(dot3(si->T, v), dot3(si->B, v), dot3(si->N, v)); }
+static inline v3 to_local(const surf_info* si, v3 v) {
+    return mk3(si->T.x * v.x + si->B.x * v.y + si->N.x * v.z, si->T.y * v.x + si->B.y * v.y + si->N.y * v.z,
+               si->T.z * v.x + si->B.z * v.y + si->N.z * v.z);
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * BxDFs (Src/BuiltinComponent/Surface/Classic/Kernel.cpp)
+ * ---------------------------------------------------------------------------------------------- */
+enum {
+    PART_R = 1, PART_T = 2, PART_DIFFUSE = 4, PART_SPECULAR = 8, PART_GLOSSY = 16, PART_ALL = 31,
+    PART_NO_SPECULAR = 31 ^ 8
+};
+/* match (Protocol.hpp:143-145) */
+static inline int part_match(int provide, int require) { return (provide & require) == provide; }
+
+typedef struct bsdf_sample { v3 wi; spec f; float pdf; int part; } bsdf_sample;
+
+enum { LOBE_LAMBERT, LOBE_OREN_NAYAR, LOBE_MF_REFL, LOBE_FRESNEL_SPEC, LOBE_MF_TRANS, LOBE_MIRROR, LOBE_BLEND };
+enum { FRESNEL_DIELECTRIC, FRESNEL_SCHLICK };
+
+typedef struct lobe {
+    int type;
+    int part;
+    spec color;   /* reflection / transmission */
+    spec color2;  /* FresnelBlend specular, Schlick F0 */
+    float a, b;   /* Oren-Nayar A, B */
+    float ax, ay; /* microfacet alphas */
+    float eta_i, eta_t;
+    float eta, correct;
+    int fresnel;
+} lobe;
+
+typedef struct bsdf {
+    int n;
+    lobe l[3];
+    int no_specular;
+    int mirror; /* Mirror surface: sample only, evaluate/pdf are the black body's (Classic.cpp:163-166) */
+} bsdf;
+
+/* FresnelDielectric (Kernel.cpp:271-286) */
+static float fresnel_dielectric(float eta_i, float eta_t, float cos_i) {
+    cos_i = fmaxf(0.0f, fminf(1.0f, fabsf(cos_i)));
+    const float sin_i = sqrt_safe(1.0f - cos_i * cos_i);
+    const float sin_t = eta_i / eta_t * sin_i;
+    if (sin_t >= 1.0f) return 1.0f;
+    const float cos_t = sqrt_safe(1.0f - sin_t * sin_t);
+    const float p1 = eta_t * cos_i, p2 = eta_i * cos_t;
+    const float par = (p1 - p2) / (p1 + p2);
+    const float p3 = eta_i * cos_i, p4 = eta_t * cos_t;
+    const float perp = (p3 - p4) / (p3 + p4);
+    return 0.5f * (par * par + perp * perp);
+}
+
+static spec lobe_fresnel(const lobe* L, float c) {
+    if (L->fresnel == FRESNEL_SCHLICK) {
+        /* extension: Schlick's approximation F0 + (1 - F0)(1 - cos)^5 */
+        const float m = 1.0f - fminf(1.0f, fabsf(c));
+        const float m5 = (m * m) * (m * m) * m;
+        return mksp(L->color2.r + (1.0f - L->color2.r) * m5, L->color2.g + (1.0f - L->color2.g) * m5,
+                    L->color2.b + (1.0f - L->color2.b) * m5);
+    }
+    const float f = fresnel_dielectric(L->eta_i, L->eta_t, c);
+    return mksp(f, f, f);
+}
+
+/* MicrofacetDistribution (Kernel.cpp:289-382) */
+static float mf_lambda(float ax, float ay, v3 w) {
+    const float cos2 = w.z * w.z;
+    const float sin2 = fmaxf(0.0f, 1.0f - cos2);
+    const float tan2 = sin2 / cos2;
+    if (isinf(tan2)) return 0.0f;
+    const float sin_t = sqrtf(sin2);
+    const float cos_phi = sin_t == 0.0f ? 1.0f : fminf(1.0f, fmaxf(-1.0f, w.x / sin_t));
+    const float p1 = cos_phi * ax;
+    const float sin_phi = sin_t == 0.0f ? 0.0f : fminf(1.0f, fmaxf(-1.0f, w.y / sin_t));
+    const float p2 = sin_phi * ay;
+    const float sqr = (p1 * p1 + p2 * p2) * tan2;
+    return (-1.0f + sqrtf(1.0f + sqr)) * 0.5f;
+}
+
+static float mf_d(float ax, float ay, v3 wh) {
+    const float cos2 = wh.z * wh.z;
+    const float sin2 = fmaxf(0.0f, 1.0f - cos2);
+    const float tan2 = sin2 / cos2;
+    if (isinf(tan2)) return 0.0f;
+    const float sin_t = sqrtf(sin2);
+    const float cos_phi = sin_t == 0.0f ? 1.0f : fminf(1.0f, fmaxf(-1.0f, wh.x / sin_t));
+    const float p1 = cos_phi / ax;
+    const float sin_phi = sin_t == 0.0f ? 0.0f : fminf(1.0f, fmaxf(-1.0f, wh.y / sin_t));
+    const float p2 = sin_phi / ay;
+    const float e = cos2 * (1.0f + (p1 * p1 + p2 * p2) * tan2);
+    return K_INV_PI / (ax * ay * e * e);
+}
+
+static void mf_sample11(float cos_theta, float u1, float u2, float* sx, float* sy) {
+    if (cos_theta > 1.0f - 1e-5f) {
+        const float r = sqrtf(u1 / (1.0f - u1));
+        const float phi = K_TWO_PI * u2;
+        float s, c;
+        pb2_sincosf(phi, &s, &c);
+        *sx = r * c;
+        *sy = r * s;
+        return;
+    }
+    const float sin_t = sqrt_safe(1.0f - cos_theta * cos_theta);
+    const float tan_t = sin_t / cos_theta;
+    const float tan2 = tan_t * tan_t;
+    const float g1 = 2.0f / (1.0f + sqrtf(1.0f + tan2));
+    const float a = 2.0f * u1 / g1 - 1.0f;
+    const float a2 = a * a;
+    const float v = fminf(1e10f, 1.0f / (a2 - 1.0f));
+    const float d = sqrt_safe(tan2 * v * v - (a2 - tan2) * v);
+    const float p = tan_t * v;
+    const float p1 = p - d;
+    const float p2 = p + d;
+    const float x = (a < 0.0f || p2 > 1.0f / tan_t) ? p1 : p2;
+    const float s = u2 > 0.5f ? 1.0f : -1.0f;
+    const float nu2 = (u2 > 0.5f ? 2.0f : -2.0f) * (u2 - 0.5f);
+    const float z = (nu2 * (nu2 * (nu2 * 0.27385f - 0.73369f) + 0.46341f)) /
+                    (nu2 * (nu2 * (nu2 * 0.093073f + 0.309420f) - 1.000000f) + 0.597999f);
+    *sx = x;
+    *sy = s * z * sqrtf(1.0f + x * x);
+}
+
+static v3 mf_sample_wh(float ax, float ay, v3 wi, float u1, float u2) {
+    const v3 st = normalize3(mk3(ax * wi.x, ay * wi.y, wi.z));
+    float sx, sy;
+    mf_sample11(st.z, u1, u2, &sx, &sy);
+    const float sin_t = sqrt_safe(1.0f - st.z * st.z);
+    const float cos_phi = sin_t == 0.0f ? 1.0f : fminf(1.0f, fmaxf(-1.0f, st.x / sin_t));
+    const float sin_phi = sin_t == 0.0f ? 0.0f : fminf(1.0f, fmaxf(-1.0f, st.y / sin_t));
+    const float rx = cos_phi * sx - sin_phi * sy;
+    const float ry = sin_phi * sx + cos_phi * sy;
+    return normalize3(mk3(-rx * ax, -ry * ay, 1.0f));
+}
+
+/* halfVector (Transform.hpp:279-282) */
+static inline v3 half_vector(v3 a, v3 b) { return normalize3(mk3(a.x + b.x, a.y + b.y, a.z + b.z)); }
+/* reflect (Transform.hpp:405-408) */
+static inline v3 reflect3(v3 wo, v3 n) { return sub3(mul3s(n, 2.0f * dot3(wo, n)), wo); }
+/* refract (Transform.hpp:410-421) */
+static int refract3(v3 wi, v3 n, float eta, v3* wt) {
+    const float cos_i = dot3(n, wi);
+    const float sin2_i = fmaxf(0.0f, 1.0f - cos_i * cos_i);
+    const float sin2_t = eta * eta * sin2_i;
+    if (sin2_t >= 1.0f) return 0;
+    const float cos_t = sqrt_safe(1.0f - sin2_t);
+    *wt = normalize3(sub3(mul3s(n, eta * cos_i - cos_t), mul3s(wi, eta)));
+    return 1;
+}
+
+/* sampleConcentricDisk / sampleCosineHemisphere (Src/Kernel/Sampling.hpp:31-50) */
+static v3 sample_cosine_hemisphere(float u1, float u2) {
+    u1 = 2.0f * u1 - 1.0f;
+    u2 = 2.0f * u2 - 1.0f;
+    const float au1 = fabsf(u1), au2 = fabsf(u2);
+    float cx, cy;
+    if (fminf(au1, au2) < 1e-4f) {
+        cx = 0.0f; cy = 0.0f;
+    } else {
+        const float rad = au1 > au2 ? u1 : u2;
+        const float theta = au1 > au2 ? K_QUARTER_PI * (u2 / u1) : K_HALF_PI - K_QUARTER_PI * (u1 / u2);
+        float s, c;
+        pb2_sincosf(theta, &s, &c);
+        cx = c * rad; cy = s * rad;
+    }
+    const float z = sqrt_safe(1.0f - (cx * cx + cy * cy));
+    return mk3(cx, cy, z);
+}
+
+static spec lobe_eval(const lobe* L, v3 wo, v3 wi) {
+    switch (L->type) {
+        case LOBE_LAMBERT: /* Kernel.cpp:89-91 */
+            return sp_muls(L->color, K_INV_PI);
+        case LOBE_OREN_NAYAR: { /* Kernel.cpp:111-139 */
+            const float sin_i = sqrt_safe(1.0f - wi.z * wi.z);
+            const float sin_o = sqrt_safe(1.0f - wo.z * wo.z);
+            if (sin_i < 1e-4f || sin_o < 1e-4f) return SP_ZERO;
+            const float cos_phi_i = sin_i == 0.0f ? 1.0f : fminf(1.0f, fmaxf(-1.0f, wi.x / sin_i));
+            const float sin_phi_i = sin_i == 0.0f ? 0.0f : fminf(1.0f, fmaxf(-1.0f, wi.y / sin_i));
+            const float cos_phi_o = sin_o == 0.0f ? 1.0f : fminf(1.0f, fmaxf(-1.0f, wo.x / sin_o));
+            const float sin_phi_o = sin_o == 0.0f ? 0.0f : fminf(1.0f, fmaxf(-1.0f, wo.y / sin_o));
+            const float max_cos = fmaxf(0.0f, cos_phi_i * cos_phi_o + sin_phi_i * sin_phi_o);
+            float sin_alpha, tan_beta;
+            if (fabsf(wi.z) > fabsf(wo.z)) { sin_alpha = sin_o; tan_beta = sin_i / fabsf(wi.z); }
+            else { sin_alpha = sin_i; tan_beta = sin_o / fabsf(wo.z); }
+            return sp_muls(L->color, K_INV_PI * (L->a + L->b * max_cos * sin_alpha * tan_beta));
+        }
+        case LOBE_MF_REFL: { /* Kernel.cpp:397-404 */
+            const v3 wh = half_vector(wo, wi);
+            const spec F = lobe_fresnel(L, dot3(wi, wh));
+            const float q = mf_d(L->ax, L->ay, wh) /
+                            (4.0f * (1.0f + mf_lambda(L->ax, L->ay, wo) + mf_lambda(L->ax, L->ay, wi)) * fabsf(wo.z * wi.z));
+            return sp_mul(L->color, mksp(F.r * q, F.g * q, F.b * q));
+        }
+        case LOBE_MF_TRANS: { /* Kernel.cpp:553-573 */
+            if (wi.z >= 0.0f) return SP_ZERO;
+            v3 wh = normalize3(add3(wo, mul3s(wi, L->eta)));
+            if (wh.z < 0.0f) wh = neg3(wh);
+            if (dot3(wo, wh) * dot3(wi, wh) > 0.0f) return SP_ZERO;
+            const float f = fresnel_dielectric(L->eta_i, L->eta_t, dot3(wo, wh));
+            const float sd = dot3(wo, wh) + L->eta * dot3(wi, wh);
+            const float num = (1.0f - f) * mf_d(L->ax, L->ay, wh) * fabsf(dot3(wi, wh)) * fabsf(dot3(wo, wh)) * L->correct;
+            const float den = (1.0f + mf_lambda(L->ax, L->ay, wo) + mf_lambda(L->ax, L->ay, wi)) * wo.z * wi.z * (sd * sd);
+            return sp_muls(L->color, fabsf(num / den));
+        }
+        case LOBE_BLEND: { /* FresnelBlend::evaluate (Kernel.cpp:706-722) */
+            const spec nrs = sp_add(L->color2, mksp(-1.0f, -1.0f, -1.0f));
+            const float pi5 = 1.0f - 0.5f * fabsf(wi.z), po5 = 1.0f - 0.5f * fabsf(wo.z);
+            const float pw_i = (pi5 * pi5) * (pi5 * pi5) * pi5, pw_o = (po5 * po5) * (po5 * po5) * po5;
+            const float k = -28.f / (23.f * K_PI) * (1.0f - pw_i) * (1.0f - pw_o);
+            const spec diffuse = sp_muls(sp_mul(L->color, nrs), k);
+            const v3 wh = half_vector(wo, wi);
+            const float cm1 = dot3(wi, wh) - 1.0f;
+            const float p5 = (cm1 * cm1) * (cm1 * cm1) * cm1;
+            const spec schlick = sp_add(L->color2, sp_muls(nrs, p5));
+            const float denom = 4.0f * fmaxf(fabsf(wi.z), fabsf(wo.z)) * fabsf(dot3(wi, wh));
+            const spec specular = sp_muls(schlick, mf_d(L->ax, L->ay, wh) / denom);
+            return sp_add(diffuse, specular);
+        }
+        default: /* specular lobes: delta, evaluate = 0 */
+            return SP_ZERO;
+    }
+}
+
+static float lobe_pdf(const lobe* L, v3 wo, v3 wi) {
+    switch (L->type) {
+        case LOBE_LAMBERT:
+        case LOBE_OREN_NAYAR: /* DefaultBxDFHelper::pdf (Kernel.cpp:76-78) */
+            return wi.z > 0.0f ? fabsf(wi.z) * K_INV_PI : 0.0f;
+        case LOBE_MF_REFL: { /* Kernel.cpp:405-412 */
+            if (wi.z <= 0.0f) return 0.0f;
+            const v3 wh = half_vector(wo, wi);
+            const float p1 = 1.0f + mf_lambda(L->ax, L->ay, wo);
+            const float p2 = mf_lambda(L->ax, L->ay, wh);
+            return fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+        }
+        case LOBE_MF_TRANS: { /* Kernel.cpp:574-586 */
+            if (wi.z >= 0.0f) return 0.0f;
+            const v3 wh = normalize3(add3(wo, mul3s(wi, L->eta)));
+            if (dot3(wo, wh) * dot3(wi, wh) > 0.0f) return 0.0f;
+            const float sd = dot3(wo, wh) + L->eta * dot3(wi, wh);
+            const float q = L->eta / sd;
+            const float delta = fabsf((q * q) * dot3(wi, wh));
+            return mf_d(L->ax, L->ay, wh) * fabsf(dot3(wo, wh)) * delta /
+                   ((1.0f + mf_lambda(L->ax, L->ay, wo)) * fabsf(wo.z));
+        }
+        case LOBE_BLEND: { /* Kernel.cpp:723-732 */
+            if (wi.z <= 0.0f) return 0.0f;
+            const v3 wh = half_vector(wo, wi);
+            return 0.5f * (fabsf(wi.z) * K_INV_PI +
+                           mf_d(L->ax, L->ay, wh) /
+                               (4.0f * fabsf(wo.z) * (1.0f + mf_lambda(L->ax, L->ay, wo) + mf_lambda(L->ax, L->ay, wh))));
+        }
+        default:
+            return 0.0f;
+    }
+}
+
+/* Per-lobe sample; leaves res->pdf untouched when it rejects (the caller preset it to 0). */
+static void lobe_sample(const lobe* L, float u1, float u2, v3 wo, bsdf_sample* res) {
+    switch (L->type) {
+        case LOBE_LAMBERT:
+        case LOBE_OREN_NAYAR: /* DefaultBxDFHelper::sample (Kernel.cpp:68-74) */
+            res->wi = sample_cosine_hemisphere(u1, u2);
+            res->f = lobe_eval(L, wo, res->wi);
+            res->pdf = lobe_pdf(L, wo, res->wi);
+            res->part = L->part;
+            return;
+        case LOBE_MF_REFL: { /* Kernel.cpp:413-432 */
+            if (wo.z == 0.0f) return;
+            const v3 wh = mf_sample_wh(L->ax, L->ay, wo, u1, u2);
+            if (dot3(wo, wh) < 0.0f) return;
+            res->wi = reflect3(wo, wh);
+            if (res->wi.z <= 0.0f) return;
+            const float p1 = 1.0f + mf_lambda(L->ax, L->ay, wo);
+            const spec F = lobe_fresnel(L, dot3(res->wi, wh));
+            const float q = mf_d(L->ax, L->ay, wh) / (4.0f * (p1 + mf_lambda(L->ax, L->ay, res->wi)) * fabsf(wo.z * res->wi.z));
+            res->f = sp_mul(L->color, mksp(F.r * q, F.g * q, F.b * q));
+            res->part = L->part;
+            const float p2 = mf_lambda(L->ax, L->ay, wh);
+            res->pdf = fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+            return;
+        }
+        case LOBE_FRESNEL_SPEC: { /* FresnelSpecular::sample (Kernel.cpp:519-536) */
+            const float f = fresnel_dielectric(L->eta_i, L->eta_t, wo.z);
+            if (u1 < f) {
+                res->wi = mk3(-wo.x, -wo.y, wo.z);
+                res->part = PART_R | PART_SPECULAR;
+                res->pdf = f;
+                res->f = sp_muls(L->color, f / fabsf(res->wi.z));
+            } else {
+                v3 wt;
+                if (!refract3(wo, mk3(0.0f, 0.0f, 1.0f), L->eta, &wt)) return;
+                res->wi = wt;
+                res->part = PART_T | PART_SPECULAR;
+                res->pdf = 1.0f - f;
+                res->f = sp_muls(L->color2, L->correct * res->pdf / fabsf(res->wi.z));
+            }
+            return;
+        }
+        case LOBE_MF_TRANS: { /* Kernel.cpp:587-599 */
+            if (wo.z == 0.0f) return;
+            const v3 wh = mf_sample_wh(L->ax, L->ay, wo, u1, u2);
+            if (dot3(wo, wh) < 0.0f) return;
+            v3 wt;
+            if (!refract3(wo, wh, L->eta, &wt)) return;
+            res->wi = wt;
+            res->part = L->part;
+            res->f = lobe_eval(L, wo, wt);
+            res->pdf = lobe_pdf(L, wo, wt);
+            return;
+        }
+        case LOBE_BLEND: { /* FresnelBlend::sample (Kernel.cpp:733-747) */
+            if (u1 < 0.5f) {
+                u1 = fminf(2.0f * u1, 1.0f);
+                res->wi = sample_cosine_hemisphere(u1, u2);
+            } else {
+                u1 = fminf(2.0f * (u1 - 0.5f), 1.0f);
+                const v3 wh = mf_sample_wh(L->ax, L->ay, wo, u1, u2);
+                res->wi = reflect3(wo, wh);
+                if (res->wi.z <= 0.0f) return;
+            }
+            res->part = L->part;
+            res->pdf = lobe_pdf(L, wo, res->wi);
+            res->f = lobe_eval(L, wo, res->wi);
+            return;
+        }
+        default:
+            return;
+    }
+}
+
+/* Surface init (matteInit :249-268, plasticInit :441-470, glassInit :613-656, mirrorInit :668-677,
+ * substrateInit :755-778, blackBodyInit :45-48).  Lobe order = the KERNEL_FUNCTION_GROUP order. */
+static void bsdf_init(const or_scene* s, uint32_t mat, int front, bsdf* b) {
+    const pb2_material* m = &s->mats[mat];
+    const spec c0 = mksp(m->color0[0], m->color0[1], m->color0[2]);
+    const spec c1 = mksp(m->color1[0], m->color1[1], m->color1[2]);
+    const float ax = s->alpha[2 * mat], ay = s->alpha[2 * mat + 1];
+    memset(b, 0, sizeof(*b));
+    switch (m->type) {
+        case PB2_SURFACE_MATTE: {
+            lobe* L = &b->l[b->n++];
+            L->part = PART_DIFFUSE | PART_R;
+            L->color = c0;
+            if (m->roughness[0] > 0.0f) {
+                L->type = LOBE_OREN_NAYAR;
+                const float sigma = m->roughness[0] * K_PI;
+                const float sigma2 = sigma * sigma;
+                L->a = 1.0f - (sigma2 / (2.0f * (sigma2 + 0.33f)));
+                L->b = 0.45f * sigma2 / (sigma2 + 0.09f);
+            } else {
+                L->type = LOBE_LAMBERT;
+            }
+            b->no_specular = 1;
+            break;
+        }
+        case PB2_SURFACE_PLASTIC: {
+            if (sp_valid(c0)) {
+                lobe* L = &b->l[b->n++];
+                L->type = LOBE_LAMBERT; L->part = PART_DIFFUSE | PART_R; L->color = c0;
+            }
+            if (sp_valid(c1)) {
+                lobe* L = &b->l[b->n++];
+                L->type = LOBE_MF_REFL; L->part = PART_GLOSSY | PART_R; L->color = c1;
+                L->fresnel = FRESNEL_DIELECTRIC;
+                L->eta_i = front ? 1.0f : 1.46f;
+                L->eta_t = front ? 1.46f : 1.0f;
+                L->ax = ax; L->ay = ax;
+            }
+            b->no_specular = 1;
+            break;
+        }
+        case PB2_SURFACE_CONDUCTOR: {
+            lobe* L = &b->l[b->n++];
+            L->type = LOBE_MF_REFL; L->part = PART_GLOSSY | PART_R;
+            L->color = mksp(1.0f, 1.0f, 1.0f);
+            L->color2 = c1;
+            L->fresnel = FRESNEL_SCHLICK;
+            L->ax = ax; L->ay = ay;
+            b->no_specular = 1;
+            break;
+        }
+        case PB2_SURFACE_GLASS: {
+            if (!sp_valid(c0) && !sp_valid(c1)) { b->no_specular = 0; break; }
+            const float eta_i = front ? 1.0f : 1.5f, eta_t = front ? 1.5f : 1.0f;
+            if (m->roughness[0] == 0.0f && m->roughness[1] == 0.0f) {
+                lobe* L = &b->l[b->n++];
+                L->type = LOBE_FRESNEL_SPEC; L->part = PART_R | PART_T | PART_SPECULAR;
+                L->color = c0; L->color2 = c1;
+                L->eta_i = eta_i; L->eta_t = eta_t;
+                L->eta = eta_i / eta_t;
+                L->correct = L->eta * L->eta; /* TransportMode::Radiance */
+                b->no_specular = 0;
+            } else {
+                if (sp_valid(c0)) {
+                    lobe* L = &b->l[b->n++];
+                    L->type = LOBE_MF_REFL; L->part = PART_GLOSSY | PART_R; L->color = c0;
+                    L->fresnel = FRESNEL_DIELECTRIC; L->eta_i = eta_i; L->eta_t = eta_t; L->ax = ax; L->ay = ay;
+                }
+                if (sp_valid(c1)) {
+                    lobe* L = &b->l[b->n++];
+                    L->type = LOBE_MF_TRANS; L->part = PART_GLOSSY | PART_T; L->color = c1;
+                    L->eta_i = eta_i; L->eta_t = eta_t; L->ax = ax; L->ay = ay;
+                    L->eta = eta_t / eta_i;
+                    L->correct = 1.0f; /* TransportMode::Radiance */
+                }
+                b->no_specular = 1;
+            }
+            break;
+        }
+        case PB2_SURFACE_MIRROR: {
+            lobe* L = &b->l[b->n++];
+            L->type = LOBE_MIRROR; L->part = PART_R | PART_SPECULAR; L->color = c0;
+            b->mirror = 1;
+            b->no_specular = 0;
+            break;
+        }
+        case PB2_SURFACE_SUBSTRATE: {
+            if (!sp_valid(c0) && !sp_valid(c1)) { b->no_specular = 0; break; }
+            lobe* L = &b->l[b->n++];
+            L->type = LOBE_BLEND; L->part = PART_GLOSSY | PART_R; L->color = c0; L->color2 = c1;
+            L->ax = ax; L->ay = ay;
+            b->no_specular = 1;
+            break;
+        }
+        default: /* black body */
+            b->no_specular = 0;
+            break;
+    }
+}
+
+static uint32_t bsdf_count(const bsdf* b, int require) {
+    uint32_t c = 0;
+    for (int i = 0; i < b->n; ++i) c += part_match(b->l[i].part, require);
+    return c;
+}
+
+/* sample() of KERNEL_FUNCTION_GROUP (Kernel.cpp:186-206) */
+static void bsdf_sample_fn(const bsdf* b, float u1, float u2, v3 wo, v3 ng, int require, bsdf_sample* out) {
+    out->pdf = 0.0f;
+    if (b->mirror) { /* mirrorSample (Kernel.cpp:680-692) */
+        const int part = PART_R | PART_SPECULAR;
+        if (part_match(part, require)) {
+            out->wi = mk3(-wo.x, -wo.y, wo.z);
+            out->f = sp_divs(b->l[0].color, fabsf(out->wi.z));
+            out->part = part;
+            out->pdf = 1.0f;
+        }
+        return;
+    }
+    const uint32_t count = bsdf_count(b, require);
+    if (count == 0) return;
+    uint32_t sel = (uint32_t)floorf(u1 * (float)count);
+    if (sel > count - 1) sel = count - 1;
+    u1 = u1 * (float)count - (float)sel;
+    int chosen = -1;
+    for (int i = 0, k = 0; i < b->n; ++i) {
+        if (!part_match(b->l[i].part, require)) continue;
+        if ((uint32_t)k == sel) { chosen = i; break; }
+        ++k;
+    }
+    lobe_sample(&b->l[chosen], u1, u2, wo, out);
+    if (out->pdf <= 0.0f) return;
+    if (!(out->part & PART_SPECULAR)) {
+        const int addition = (dot3(wo, ng) * dot3(out->wi, ng)) > 0.0f ? PART_R : PART_T;
+        for (int i = 0; i < b->n; ++i) { /* evaluateN (:168-176) */
+            if (i == chosen || !part_match(b->l[i].part, require)) continue;
+            if (addition & b->l[i].part) out->f = sp_add(out->f, lobe_eval(&b->l[i], wo, out->wi));
+        }
+        for (int i = 0; i < b->n; ++i) { /* pdfN (:158-166) */
+            if (i == chosen || !part_match(b->l[i].part, require)) continue;
+            out->pdf = out->pdf + lobe_pdf(&b->l[i], wo, out->wi);
+        }
+    }
+    if (count > 1) out->pdf = out->pdf / (float)count;
+}
+
+/* PREFIX##Evaluate (Kernel.cpp:217-224) */
+static spec bsdf_eval(const bsdf* b, v3 wo, v3 wi, v3 ng, int require) {
+    if (b->mirror) return SP_ZERO;
+    const int addition = (dot3(wo, ng) * dot3(wi, ng)) > 0.0f ? PART_R : PART_T;
+    spec f = SP_ZERO;
+    for (int i = 0; i < b->n; ++i)
+        if (part_match(b->l[i].part, require) && (addition & b->l[i].part)) f = sp_add(f, lobe_eval(&b->l[i], wo, wi));
+    return f;
+}
+
+/* PREFIX##Pdf (Kernel.cpp:226-236) */
+static float bsdf_pdf(const bsdf* b, v3 wo, v3 wi, int require) {
+    if (b->mirror) return 0.0f;
+    const uint32_t count = bsdf_count(b, require);
+    if (count == 0) return 0.0f;
+    float pdf = 0.0f;
+    for (int i = 0; i < b->n; ++i)
+        if (part_match(b->l[i].part, require)) pdf = pdf + lobe_pdf(&b->l[i], wo, wi);
+    if (count > 1) pdf = pdf / (float)count;
+    return pdf;
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * Lights (Src/BuiltinComponent/Light/...)
+ * ---------------------------------------------------------------------------------------------- */
+typedef struct light_sample { v3 dir; spec rad; float pdf; float distance; } light_sample;
+
+/* select() (Src/Kernel/Sampling.hpp:52-63): note u is remapped with cdf[r] itself. */
+static uint32_t cdf_select(const float* cdf, const float* pdf, uint32_t size, float* u) {
+    uint32_t l = 0, r = size;
+    while (l < r) {
+        const uint32_t mid = (l + r) >> 1;
+        if (*u >= cdf[mid]) l = mid + 1;
+        else r = mid;
+    }
+    *u = (*u - cdf[r]) / pdf[r];
+    return r;
+}
+
+/* diffuseSample (AreaLight/Kernel.cpp:24-41) over planeSample (BasicShapes/Kernel.cpp:113-134) */
+static void area_sample(const or_scene* s, uint32_t li, v3 hit, float u1, float u2, light_sample* ls) {
+    const or_light* L = &s->lights[li];
+    const uint32_t idx = cdf_select(s->plane_cdf + L->first_plane, s->plane_pdf + L->first_plane, L->plane_count, &u1);
+    const pb2_plane* pl = &s->planes[L->first_plane + idx];
+    const v3 lp = add3(add3(ld3(pl->origin), mul3s(ld3(pl->u), u1)), mul3s(ld3(pl->v), u2));
+    const v3 src = add3(lp, L->translation);
+    v3 n = ld3(pl->normal);
+    if (dot3(sub3(hit, src), n) <= 0.0f) n = neg3(n);
+    float pdf = L->inverse_area;
+    const v3 delta = sub3(src, hit);
+    if (pdf == 0.0f || dot3(delta, n) >= 0.0f) {
+        ls->pdf = 0.0f;
+        return;
+    }
+    ls->rad = L->radiance;
+    const float dis2 = len2_3(delta);
+    ls->distance = sqrtf(dis2);
+    ls->dir = div3s(delta, ls->distance);
+    ls->pdf = pdf * dis2 / fabsf(dot3(n, ls->dir));
+}
+
+/* SESample (BasicLight/Kernel.cpp:61-73): phi covers [0, pi] only, as in the reference. */
+static void env_sample(const or_scene* s, float u1, float u2, light_sample* ls) {
+    ls->rad = s->env;
+    const float theta = u1 * K_PI, phi = u2 * K_PI;
+    float st, ct, sp, cp;
+    pb2_sincosf(theta, &st, &ct);
+    pb2_sincosf(phi, &sp, &cp);
+    ls->dir = mk3(st * cp, st * sp, ct);
+    ls->pdf = st == 0.0f ? 0.0f : 1.0f / ((2.0f * K_SQR_PI) * st);
+    ls->distance = 1e5f;
+}
+
+/* SEPdf (BasicLight/Kernel.cpp:80-89) */
+static float env_pdf(v3 dir) {
+    const float theta = pb2_acosf(fmaxf(-1.0f, fminf(1.0f, dir.z)));
+    const float st = pb2_sinf(theta);
+    return st == 0.0f ? 0.0f : 1.0f / ((2.0f * K_SQR_PI) * st);
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * Integrator (Src/BuiltinComponent/Integrator/PathTracing/Kernel.cpp:23-193)
+ * ---------------------------------------------------------------------------------------------- */
+typedef struct path_ctx {
+    const or_scene* s;
+    uint64_t index;
+    uint32_t dim;
+    int overflow;
+    uint64_t closest_rays, shadow_rays;
+} path_ctx;
+
+/* piperSample (Tracer/Embree/Kernel.cpp:37-45); the mt19937_64 tail past dimension 1023 is not
+ * reproduced (settings that could reach it are rejected up front). */
+static inline float next_sample(path_ctx* c) {
+    if (c->dim >= PB2_SOBOL_DIMS) { c->overflow = 1; return 0.5f; }
+    return or_sobol_sample(c->index, c->dim++);
+}
+
+/* The two uniform numbers of piperSurfaceSample / piperLightSample are the two `piperSample(context)`
+ * arguments of one call (Tracer/Embree/Kernel.cpp:117, 145); the compiler evaluates them right to left,
+ * so u2 takes the lower dimension. */
+static inline void next_pair(path_ctx* c, float* u1, float* u2) {
+    *u2 = next_sample(c);
+    *u1 = next_sample(c);
+}
+
+static inline float power_heuristic(float a, float b) {
+    const float sp1 = a * a;
+    const float sp2 = b * b;
+    return sp1 / (sp1 + sp2);
+}
+
+static spec mis(path_ctx* c, v3 hit, const bsdf* b, v3 wo, const surf_info* si, v3 ng_sh) {
+    const or_scene* s = c->s;
+    /* uniformSelect (BasicLight/Kernel.cpp:91-98): lights[0] = environment, then the area lights */
+    const uint32_t count = 1 + s->nlight;
+    const float u = next_sample(c);
+    uint32_t sel = (uint32_t)floorf(u * (float)count);
+    if (sel > count - 1) sel = count - 1;
+    const float sel_pdf = 1.0f / (float)count;
+    const int delta = 0;
+    if (sel_pdf <= 0.0f) return SP_ZERO;
+
+    spec part_a = SP_ZERO;
+    {
+        light_sample ls;
+        float u1, u2;
+        next_pair(c, &u1, &u2);
+        if (sel == 0) env_sample(s, u1, u2, &ls);
+        else area_sample(s, sel - 1, hit, u1, u2, &ls);
+        if (ls.pdf > 0.0f && sp_valid(ls.rad)) {
+            const v3 wi = to_shading(si, ls.dir);
+            const spec f = bsdf_eval(b, wo, wi, ng_sh, PART_NO_SPECULAR);
+            if (sp_valid(f)) {
+                if (!occluded(s, hit, ls.dir, fminf(1e-3f, ls.distance), ls.distance, &c->shadow_rays)) {
+                    float w = fabsf(wi.z) / ls.pdf;
+                    if (!delta) {
+                        const float bp = bsdf_pdf(b, wo, wi, PART_NO_SPECULAR);
+                        w = w * power_heuristic(ls.pdf, bp);
+                    }
+                    part_a = sp_muls(sp_mul(f, ls.rad), w);
+                }
+            }
+        }
+    }
+    spec part_b = SP_ZERO;
+    if (!delta) {
+        bsdf_sample bs;
+        float u1, u2;
+        next_pair(c, &u1, &u2);
+        bsdf_sample_fn(b, u1, u2, wo, ng_sh, PART_NO_SPECULAR, &bs);
+        if (bs.pdf > 0.0f && sp_valid(bs.f)) {
+            float weight = fabsf(bs.wi.z) / bs.pdf;
+            const v3 dir = to_local(si, bs.wi);
+            surf_info hs;
+            trace_surface(s, hit, dir, 1e-3f, 1e5f, &hs, &c->closest_rays);
+            const int is_sel_light = hs.kind == KIND_AREA_LIGHT && sel != 0 && hs.light == sel - 1;
+            if (is_sel_light || hs.kind == KIND_MISSING) {
+                spec rad;
+                float pdf;
+                if (hs.kind == KIND_MISSING) {
+                    rad = s->env;
+                    pdf = sp_valid(rad) ? env_pdf(dir) : 0.0f;
+                } else {
+                    const or_light* L = &s->lights[hs.light];
+                    /* diffuseEvaluate / diffusePdf (AreaLight/Kernel.cpp:43-55) */
+                    rad = dot3(hs.N, dir) < 0.0f ? L->radiance : SP_ZERO;
+                    pdf = hs.t * hs.t / (fabsf(dot3(hs.N, dir)) * L->area);
+                }
+                if (sp_valid(rad) && pdf > 0.0f) {
+                    weight = weight * power_heuristic(bs.pdf, pdf);
+                    part_b = sp_muls(sp_mul(rad, bs.f), weight);
+                }
+            }
+        }
+    }
+    return sp_divs(sp_add(part_a, part_b), sel_pdf);
+}
+
+static spec trace_path(path_ctx* c, const pb2_render_settings* st, v3 o, v3 d, uint32_t* depth_out) {
+    const or_scene* s = c->s;
+    spec pf = mksp(1.0f, 1.0f, 1.0f);
+    spec sample = SP_ZERO;
+    int specular = 1;
+    uint32_t depth = 0;
+    for (;;) {
+        surf_info si;
+        trace_surface(s, o, d, 1e-3f, 1e5f, &si, &c->closest_rays);
+        if (specular && (si.kind == KIND_AREA_LIGHT || si.kind == KIND_MISSING)) {
+            spec rad;
+            if (si.kind == KIND_AREA_LIGHT) {
+                const v3 delta = mul3s(d, si.t);
+                const v3 wi = normalize3(delta);
+                rad = dot3(si.N, wi) < 0.0f ? s->lights[si.light].radiance : SP_ZERO;
+            } else {
+                rad = s->env;
+            }
+            sample = sp_add(sample, sp_mul(pf, rad));
+        }
+        if (si.kind == KIND_AREA_LIGHT) {
+            --depth;
+            o = add3(o, mul3s(d, si.t + 0.001f));
+            continue;
+        }
+        if (si.kind == KIND_MISSING || depth >= st->max_depth) break;
+
+        const v3 wo = to_shading(&si, neg3(d));
+        const v3 ng_sh = to_shading(&si, si.Ng);
+        bsdf b;
+        bsdf_init(s, si.material, si.front, &b);
+        const v3 hit = add3(o, mul3s(d, si.t));
+        if (b.no_specular) sample = sp_add(sample, sp_mul(pf, mis(c, hit, &b, wo, &si, ng_sh)));
+        bsdf_sample ss;
+        float u1, u2;
+        next_pair(c, &u1, &u2);
+        bsdf_sample_fn(&b, u1, u2, wo, ng_sh, PART_ALL, &ss);
+        if (!(ss.pdf > 0.0f && sp_valid(ss.f))) break;
+        pf = sp_muls(sp_mul(pf, ss.f), fabsf(ss.wi.z) / ss.pdf);
+        if (depth > st->min_rr_depth) {
+            const float p = fmaxf(0.05f, 1.0f - fmaxf(pf.r, fmaxf(pf.g, pf.b)));
+            if (next_sample(c) < p) break;
+            pf = sp_divs(pf, 1.0f - p);
+        }
+        d = to_local(&si, ss.wi);
+        o = add3(hit, mul3s(si.Ng, (ss.part & PART_R) ? 0.001f : -0.001f));
+        specular = (ss.part & PART_SPECULAR) != 0;
+        ++depth;
+    }
+    *depth_out = depth;
+    return sample;
+}
+
+/* accumulate + filters (Src/BuiltinComponent/RenderDriver/FixedSampler/Kernel.cpp:30-69) */
+static float filter_weight(const pb2_render_settings* st, float dx, float dy) {
+    switch (st->filter) {
+        case PB2_FILTER_TRIANGLE:
+            return fmaxf(0.0f, 1.0f - fabsf(dx)) * fmaxf(0.0f, 1.0f - fabsf(dy));
+        case PB2_FILTER_GAUSSIAN: {
+            const float neg_alpha = -st->gaussian_alpha;
+            const float sub = expf(-st->gaussian_alpha); /* host: FixedSampler.cpp:43 */
+            const float wx = fmaxf(pb2_expf(neg_alpha * dx * dx) - sub, 0.0f);
+            const float wy = fmaxf(pb2_expf(neg_alpha * dy * dy) - sub, 0.0f);
+            return wx * wy;
+        }
+        default:
+            return 1.0f;
+    }
+}
+
+static void splat(const pb2_render_settings* st, float* rgbw, float px, float py, spec v) {
+    const int32_t bx = (int32_t)(px - 0.5f), by = (int32_t)(py - 0.5f);
+    const int32_t xs[4] = { bx, bx + 1, bx, bx + 1 };
+    const int32_t ys[4] = { by, by, by + 1, by + 1 };
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t x = (uint32_t)xs[k], y = (uint32_t)ys[k];
+        if (!(x < st->width && y < st->height)) continue;
+        const float w = filter_weight(st, px - ((float)x + 0.5f), py - ((float)y + 0.5f));
+        float* p = rgbw + 4 * ((size_t)x + (size_t)y * st->width);
+        p[0] += v.r * w;
+        p[1] += v.g * w;
+        p[2] += v.b * w;
+        p[3] += w;
+    }
+}
+
+int or_render(const or_scene* s, const pb2_render_settings* st, const pb2_rect* rect, uint32_t sample_begin,
+              uint32_t sample_count, float* rgbw, float* sample_out, int threads) {
+    if (st->scramble) return -1;
+    if (5u + 8u * (uint64_t)st->max_depth > PB2_SOBOL_DIMS) return -2;
+    pb2_ndc_transform tr;
+    pb2_rect full;
+    const float dev_aspect = st->camera.sensor_size[0] / st->camera.sensor_size[1];
+    or_calc_render_rect(st->width, st->height, dev_aspect, st->fit_mode, &tr, &full);
+    const uint32_t mx = full.width > full.height ? full.width : full.height;
+    const uint32_t log2res = (uint32_t)ceil(log2((double)mx));
+    const uint32_t res = 1u << log2res;
+    const size_t nsamp = (size_t)rect->width * rect->height * sample_count;
+    float* out = sample_out ? sample_out : (float*)malloc(sizeof(float) * 5 * (nsamp ? nsamp : 1));
+    int overflow = 0;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1) reduction(| : overflow)
+    for (int64_t row = 0; row < (int64_t)rect->height; ++row) {
+        for (uint32_t col = 0; col < rect->width; ++col) {
+            for (uint32_t k = 0; k < sample_count; ++k) {
+                /* piperMain (Tracer/Embree/Kernel.cpp:47-99) */
+                const uint32_t sx = rect->left + col - full.left;
+                const uint32_t sy = rect->top + (uint32_t)row - full.top;
+                const uint32_t sidx = sample_begin + k;
+                path_ctx c;
+                memset(&c, 0, sizeof(c));
+                c.s = s;
+                c.dim = 5;
+                float off[2];
+                or_sobol_start(res, log2res, sx, sy, sidx, &c.index, off);
+                const float px = off[0] + (float)(full.left + sx);
+                const float py = off[1] + (float)(full.top + sy);
+                const float ndc_x = tr.ox + tr.sx * px / (float)st->width;
+                const float ndc_y = tr.oy + tr.sy * py / (float)st->height;
+                const float u1 = or_sobol_sample(c.index, 3);
+                const float u2 = or_sobol_sample(c.index, 4);
+                pb2_ray ray;
+                or_camera_ray(&st->camera, ndc_x, ndc_y, u1, u2, &ray);
+                uint32_t depth;
+                const spec v = trace_path(&c, st, ld3(ray.org), ld3(ray.dir), &depth);
+                overflow |= c.overflow;
+                float* o = out + 5 * (((size_t)row * rect->width + col) * sample_count + k);
+                o[0] = px; o[1] = py; o[2] = v.r; o[3] = v.g; o[4] = v.b;
+            }
+        }
+    }
+    if (rgbw) {
+        for (size_t i = 0; i < nsamp; ++i) {
+            const float* o = out + 5 * i;
+            splat(st, rgbw, o[0], o[1], mksp(o[2], o[3], o[4]));
+        }
+    }
+    if (!sample_out) free(out);
+    return overflow ? -3 : 0;
+}

@@ -1,0 +1,201 @@
+"""Python host API over the C ABI, mirroring the reference's tracer interface for this path.
+
+* :class:`Accel`     -- ``Tracer::buildAcceleration`` + the trace queries Embree answers
+  (``rtcIntersect1`` / ``rtcOccluded1``, Src/BuiltinComponent/Tracer/Embree/Embree.cpp:267-391), batched.
+* :class:`Pipeline`  -- ``Tracer::buildPipeline`` -> ``Pipeline::prepare`` -> ``TraceLauncher::launch``
+  (Src/Interface/BuiltinComponent/Tracer.hpp:100-159) and the FixedSampler film resolve
+  (Src/BuiltinComponent/RenderDriver/FixedSampler/FixedSampler.cpp:68-133).
+
+Device memory and streams come from torch (plumbing only); all compute is in libpiper2_b200.so.
+Errors raise :class:`piper2_b200.capi.PB2Error` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise capi.PB2Error("piper2_b200 needs a CUDA device")
+    return torch
+
+
+def _stream():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Accel:
+    """Acceleration structure over a scene's meshes and area-light planes."""
+
+    def __init__(self, scene_data):
+        torch = _torch()
+        torch.cuda.init()
+        self._sc, self._keep = scene_data.to_ctypes()
+        h = C.c_void_p()
+        capi.check(capi.lib().pb2_accel_create(C.byref(self._sc), _stream(), C.byref(h)))
+        self.h = h
+
+    def info(self) -> capi.AccelInfo:
+        i = capi.AccelInfo()
+        capi.check(capi.lib().pb2_accel_get_info(self.h, C.byref(i)))
+        return i
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().pb2_accel_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_counting(self, enable: bool):
+        capi.check(capi.lib().pb2_accel_set_counting(self.h, 1 if enable else 0))
+
+    def counters(self):
+        nv, nt = C.c_uint64(), C.c_uint64()
+        capi.check(capi.lib().pb2_accel_get_counters(self.h, C.byref(nv), C.byref(nt), _stream()))
+        return nv.value, nt.value
+
+    # ---- device-pointer calls (torch tensors) ----
+    def trace_closest_dev(self, rays_dev, n, hits_dev):
+        capi.check(capi.lib().pb2_trace_closest(self.h, C.c_void_p(rays_dev), n, C.c_void_p(hits_dev), _stream()))
+
+    def trace_any_dev(self, rays_dev, n, occ_dev):
+        capi.check(capi.lib().pb2_trace_any(self.h, C.c_void_p(rays_dev), n, C.c_void_p(occ_dev), _stream()))
+
+    # ---- host arrays in / out (numpy RAY_DTYPE) ----
+    def trace_closest(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=capi.RAY_DTYPE)
+        hits = np.zeros(len(rays), dtype=capi.HIT_DTYPE)
+        capi.check(capi.lib().pb2_trace_closest_host(self.h, rays.ctypes.data_as(C.c_void_p), len(rays),
+                                                     hits.ctypes.data_as(C.c_void_p), _stream()))
+        return hits
+
+    def trace_any(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=capi.RAY_DTYPE)
+        occ = np.zeros(len(rays), dtype=np.uint32)
+        capi.check(capi.lib().pb2_trace_any_host(self.h, rays.ctypes.data_as(C.c_void_p), len(rays),
+                                                 occ.ctypes.data_as(C.c_void_p), _stream()))
+        return occ
+
+
+class Pipeline:
+    """A render pipeline for one scene and one set of render settings."""
+
+    def __init__(self, scene_data, settings=None):
+        torch = _torch()
+        torch.cuda.init()
+        self.settings = settings if settings is not None else scene_data.settings
+        self._sc, self._keep = scene_data.to_ctypes()
+        h = C.c_void_p()
+        capi.check(capi.lib().pb2_pipeline_create(C.byref(self._sc), C.byref(self.settings), _stream(), C.byref(h)))
+        self.h = h
+        self.rect = capi.Rect()
+        self.ndc = capi.NDCTransform()
+        capi.check(capi.lib().pb2_pipeline_get_rect(self.h, C.byref(self.rect), C.byref(self.ndc)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().pb2_pipeline_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def new_film(self):
+        torch = _torch()
+        return torch.zeros((self.settings.height, self.settings.width, 4), dtype=torch.float32, device="cuda")
+
+    def launch(self, film, rect=None, sample_begin=0, sample_count=None, sample_out=None):
+        """TraceLauncher::launch: adds the samples of `rect` to `film` (device tensor H x W x 4)."""
+        rect = rect or self.rect
+        if sample_count is None:
+            sample_count = self.settings.samples_per_pixel
+        capi.check(capi.lib().pb2_pipeline_launch(
+            self.h, C.byref(rect), sample_begin, sample_count, C.c_void_p(film.data_ptr()),
+            C.c_void_p(sample_out.data_ptr()) if sample_out is not None else None, _stream()))
+
+    def render(self, samples=False, rect=None, sample_begin=0, sample_count=None):
+        """Full render; returns (film RGBW numpy H x W x 4, per-sample numpy rows x cols x spp x 5 or None)."""
+        torch = _torch()
+        rect = rect or self.rect
+        if sample_count is None:
+            sample_count = self.settings.samples_per_pixel
+        film = self.new_film()
+        out = None
+        if samples:
+            out = torch.zeros((rect.height, rect.width, sample_count, 5), dtype=torch.float32, device="cuda")
+        self.launch(film, rect, sample_begin, sample_count, out)
+        torch.cuda.synchronize()
+        return film.cpu().numpy(), (out.cpu().numpy() if out is not None else None)
+
+    def resolve(self, film):
+        torch = _torch()
+        rgb = torch.empty((self.settings.height, self.settings.width, 3), dtype=torch.float32, device="cuda")
+        capi.check(capi.lib().pb2_film_resolve(C.c_void_p(film.data_ptr()), self.settings.width * self.settings.height,
+                                               C.c_void_p(rgb.data_ptr()), _stream()))
+        return rgb
+
+    def camera_rays(self, sample=0, rect=None):
+        torch = _torch()
+        rect = rect or self.rect
+        n = rect.width * rect.height
+        rays = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+        pts = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+        capi.check(capi.lib().pb2_pipeline_camera_rays(self.h, C.byref(rect), sample, C.c_void_p(rays.data_ptr()),
+                                                       C.c_void_p(pts.data_ptr()), _stream()))
+        torch.cuda.synchronize()
+        return rays.cpu().numpy(), pts.cpu().numpy()
+
+    def stats(self) -> capi.LaunchStats:
+        s = capi.LaunchStats()
+        capi.check(capi.lib().pb2_pipeline_get_stats(self.h, C.byref(s), _stream()))
+        return s
+
+
+def sobol_generate(index: np.ndarray, dim: np.ndarray) -> np.ndarray:
+    torch = _torch()
+    idx = torch.from_numpy(np.ascontiguousarray(index, dtype=np.uint64).view(np.int64)).cuda()
+    dm = torch.from_numpy(np.ascontiguousarray(dim, dtype=np.uint32).view(np.int32)).cuda()
+    out = torch.empty(len(index), dtype=torch.float32, device="cuda")
+    capi.check(capi.lib().pb2_sobol_generate(C.c_void_p(idx.data_ptr()), C.c_void_p(dm.data_ptr()), len(index),
+                                             C.c_void_p(out.data_ptr()), _stream()))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def sobol_start(log2res: int, pixel_sample: np.ndarray):
+    torch = _torch()
+    ps = torch.from_numpy(np.ascontiguousarray(pixel_sample, dtype=np.uint32).view(np.int32).reshape(-1)).cuda()
+    n = len(pixel_sample)
+    idx = torch.empty(n, dtype=torch.int64, device="cuda")
+    off = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    capi.check(capi.lib().pb2_sobol_start(log2res, C.c_void_p(ps.data_ptr()), n, C.c_void_p(idx.data_ptr()),
+                                          C.c_void_p(off.data_ptr()), _stream()))
+    torch.cuda.synchronize()
+    return idx.cpu().numpy().view(np.uint64), off.cpu().numpy()

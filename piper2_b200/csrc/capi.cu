@@ -1,0 +1,340 @@
+// capi.cu -- the C ABI (include/piper2_b200.h): error handling, host-side component helpers, the
+// acceleration structure and the batch trace calls.  The render pipeline lives in render.cu.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pb2_internal.h"
+#include "sobol_tables_decl.h"
+
+namespace pb2 {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) + ")");
+    return err == cudaErrorMemoryAllocation ? PB2_ERR_OUT_OF_MEMORY : PB2_ERR_CUDA;
+}
+
+}  // namespace pb2
+
+using namespace pb2;
+
+#define PB2_CUDA(call, what)                                  \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, (what));  \
+    } while (0)
+
+extern "C" {
+
+const char* pb2_last_error(void) { return g_last_error.c_str(); }
+
+int pb2_abi_version(void) { return PB2_ABI_VERSION; }
+
+int pb2_set_device(int device) {
+    PB2_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    return PB2_OK;
+}
+
+/* Plane from Origin/U/V (Src/BuiltinComponent/Geometry/BasicShapes/BasicShapes.cpp:70-89). */
+int pb2_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out) {
+    if (!origin || !u || !v || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_plane_make: null argument");
+    const float d0 = u[1] * v[2] - u[2] * v[1];
+    const float d1 = u[2] * v[0] - u[0] * v[2];
+    const float d2 = u[0] * v[1] - u[1] * v[0];
+    const float area = std::sqrt(std::fmax(d0 * d0 + d1 * d1 + d2 * d2, 0.0f));
+    const float ul = std::sqrt(std::fmax(u[0] * u[0] + u[1] * u[1] + u[2] * u[2], 0.0f));
+    const float a0 = std::fabs(d0), a1 = std::fabs(d1), a2 = std::fabs(d2);
+    uint32_t sel;
+    if (a0 >= a1 && a0 >= a2) sel = 0;
+    else sel = (a1 >= a0 && a1 >= a2) ? 1 : 2;
+    for (int k = 0; k < 3; ++k) {
+        out->origin[k] = origin[k];
+        out->u[k] = u[k];
+        out->v[k] = v[k];
+        out->tangent[k] = u[k] / ul;
+    }
+    out->normal[0] = d0 / area;
+    out->normal[1] = d1 / area;
+    out->normal[2] = d2 / area;
+    out->max_det_comp = sel;
+    return PB2_OK;
+}
+
+/* PerspectiveCamera config -> payload (Src/BuiltinComponent/Sensor/PerspectiveCamera/PerspectiveCamera.cpp:39-44) */
+int pb2_camera_from_config(const float position[3], const float look_at[3], const float up[3],
+                           const float sensor_size_mm[2], float focal_length_mm, float fstop, pb2_camera* out) {
+    if (!position || !look_at || !up || !sensor_size_mm || !out)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_camera_from_config: null argument");
+    const float ul = std::sqrt(std::fmax(up[0] * up[0] + up[1] * up[1] + up[2] * up[2], 0.0f));
+    for (int k = 0; k < 3; ++k) {
+        out->position[k] = position[k];
+        out->look_at[k] = look_at[k];
+        out->up[k] = up[k] / ul;
+    }
+    out->sensor_size[0] = sensor_size_mm[0] * 1e-3f;
+    out->sensor_size[1] = sensor_size_mm[1] * 1e-3f;
+    out->focal_length = focal_length_mm * 1e-3f;
+    out->aperture_radius = out->focal_length / (2.0f * fstop);
+    return PB2_OK;
+}
+
+/* calcRenderRECT (Src/Interface/BuiltinComponent/Sensor.hpp:38-75) */
+int pb2_calc_render_rect(uint32_t width, uint32_t height, float device_aspect, uint32_t fit_mode,
+                         pb2_ndc_transform* tr, pb2_rect* rect) {
+    if (!tr || !rect || width == 0 || height == 0 || !(device_aspect > 0.0f))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_calc_render_rect: invalid argument");
+    const float iar = (float)width / (float)height;
+    const float iiar = 1.0f / iar;
+    const float idar = 1.0f / device_aspect;
+    if (fit_mode == PB2_FIT_FILL) {
+        *rect = { 0, 0, width, height };
+        if (iar > device_aspect) *tr = { 0.0f, (idar - iiar) * 0.5f * device_aspect, 1.0f, iiar * device_aspect };
+        else *tr = { (device_aspect - iar) * 0.5f * idar, 0.0f, iar * idar, 1.0f };
+    } else {
+        if (iar > device_aspect) {
+            *tr = { -(iar - device_aspect) * 0.5f * idar, 0.0f, iar * idar, 1.0f };
+            rect->left = (uint32_t)std::floor(std::fmax(0.0f, (float)width * (iar - device_aspect) * 0.5f * iiar));
+            rect->top = 0;
+            const uint32_t r = (uint32_t)std::ceil((float)width * (iar + device_aspect) * 0.5f * iiar);
+            rect->width = (width < r ? width : r) - rect->left;
+            rect->height = height;
+        } else {
+            *tr = { 0.0f, -(iiar - idar) * 0.5f * device_aspect, 1.0f, device_aspect * iiar };
+            rect->left = 0;
+            rect->top = (uint32_t)std::floor(std::fmax(0.0f, (float)height * (iiar - idar) * 0.5f * iar));
+            rect->width = width;
+            rect->height = (uint32_t)std::ceil((float)height * (iiar + idar) * 0.5f * iar) - rect->top;
+        }
+    }
+    return PB2_OK;
+}
+
+const char* pb2_sobol_table_digest(void) { return pb2_sobol_table_sha256(); }
+
+/* ---- acceleration structure ------------------------------------------------------------------ */
+
+int pb2_accel_create(const pb2_scene* scene, void* stream_ptr, pb2_accel** out) {
+    if (!scene || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: null argument");
+    *out = nullptr;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    uint64_t n64 = 0;
+    for (uint32_t m = 0; m < scene->mesh_count; ++m) {
+        const pb2_mesh& mesh = scene->meshes[m];
+        if (mesh.tri_count && (!mesh.vertices || !mesh.indices))
+            return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: mesh without vertices or indices");
+        if (mesh.material >= scene->material_count && scene->material_count)
+            return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: mesh material out of range");
+        for (uint64_t i = 0; i < 3ull * mesh.tri_count; ++i)
+            if (mesh.indices[i] >= mesh.vert_count)
+                return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: vertex index out of range");
+        n64 += mesh.tri_count;
+    }
+    if (n64 >= 0x80000000ull) return fail(PB2_ERR_NOT_SUPPORTED, "pb2_accel_create: more than 2^31 triangles");
+    for (uint32_t l = 0; l < scene->area_light_count; ++l) {
+        const pb2_area_light& al = scene->area_lights[l];
+        if ((uint64_t)al.first_plane + al.plane_count > scene->plane_count || al.plane_count == 0)
+            return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: area light plane range out of bounds");
+    }
+    const uint32_t n = (uint32_t)n64;
+    std::vector<TriSlot> host(n);
+    std::vector<uint32_t> prim_mat(n ? n : 1, 0);
+    uint32_t k = 0;
+    for (uint32_t m = 0; m < scene->mesh_count; ++m) {
+        const pb2_mesh& mesh = scene->meshes[m];
+        for (uint32_t i = 0; i < mesh.tri_count; ++i, ++k) {
+            float v[9];
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t vi = mesh.indices[3 * i + j];
+                for (int a = 0; a < 3; ++a) v[3 * j + a] = mesh.vertices[3 * vi + a] + mesh.translation[a];
+            }
+            uint32_t id = k;
+            float w;
+            std::memcpy(&w, &id, 4);
+            host[k].v0 = make_float4(v[0], v[1], v[2], w);
+            host[k].v1 = make_float4(v[3], v[4], v[5], 0.0f);
+            host[k].v2 = make_float4(v[6], v[7], v[8], 0.0f);
+            prim_mat[k] = mesh.material;
+        }
+    }
+    std::vector<DevPlane> planes(scene->plane_count);
+    for (uint32_t l = 0; l < scene->area_light_count; ++l) {
+        const pb2_area_light& al = scene->area_lights[l];
+        for (uint32_t i = 0; i < al.plane_count; ++i) {
+            DevPlane& d = planes[al.first_plane + i];
+            static_assert(sizeof(pb2_plane) == 64, "pb2_plane");
+            std::memcpy(&d, &scene->planes[al.first_plane + i], sizeof(pb2_plane));
+            for (int a = 0; a < 3; ++a) d.translation[a] = al.translation[a];
+            d.light = l;
+        }
+    }
+    auto* acc = new pb2_accel();
+    auto cleanup = [&](int code) {
+        pb2_accel_destroy(acc);
+        return code;
+    };
+    cudaGetDevice(&acc->device);
+    TriSlot* d_in = nullptr;
+    void* scratch = nullptr;
+    const size_t node_cap = n ? n : 1;
+    cudaError_t e;
+    if ((e = cudaMalloc(&acc->nodes, sizeof(WideNode) * node_cap))) return cleanup(cuda_fail(e, "cudaMalloc nodes"));
+    if ((e = cudaMalloc(&acc->tris, sizeof(TriSlot) * (n ? n : 1)))) return cleanup(cuda_fail(e, "cudaMalloc tris"));
+    if ((e = cudaMalloc(&acc->prim_material, sizeof(uint32_t) * (n ? n : 1))))
+        return cleanup(cuda_fail(e, "cudaMalloc prim_material"));
+    if ((e = cudaMalloc(&acc->planes, sizeof(DevPlane) * (planes.size() ? planes.size() : 1))))
+        return cleanup(cuda_fail(e, "cudaMalloc planes"));
+    if ((e = cudaMalloc(&acc->work, sizeof(uint32_t) * 8))) return cleanup(cuda_fail(e, "cudaMalloc work"));
+    if ((e = cudaMalloc(&acc->counters, sizeof(unsigned long long) * 4)))
+        return cleanup(cuda_fail(e, "cudaMalloc counters"));
+    if ((e = cudaMalloc(&acc->error_flag, sizeof(uint32_t)))) return cleanup(cuda_fail(e, "cudaMalloc flag"));
+    if ((e = cudaMemsetAsync(acc->error_flag, 0, sizeof(uint32_t), stream))) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMemsetAsync(acc->counters, 0, sizeof(unsigned long long) * 4, stream)))
+        return cleanup(cuda_fail(e, "memset"));
+    if (!planes.empty() && (e = cudaMemcpyAsync(acc->planes, planes.data(), sizeof(DevPlane) * planes.size(),
+                                                cudaMemcpyHostToDevice, stream)))
+        return cleanup(cuda_fail(e, "upload planes"));
+    if ((e = cudaMemcpyAsync(acc->prim_material, prim_mat.data(), sizeof(uint32_t) * prim_mat.size(),
+                             cudaMemcpyHostToDevice, stream)))
+        return cleanup(cuda_fail(e, "upload materials"));
+    BuildResult br{ 0, 0.0f };
+    if (n) {
+        const size_t sb = build_scratch_bytes(n);
+        if ((e = cudaMalloc(&d_in, sizeof(TriSlot) * n))) return cleanup(cuda_fail(e, "cudaMalloc build input"));
+        if ((e = cudaMalloc(&scratch, sb))) {
+            cudaFree(d_in);
+            return cleanup(cuda_fail(e, "cudaMalloc build scratch"));
+        }
+        e = cudaMemcpyAsync(d_in, host.data(), sizeof(TriSlot) * n, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = build_wide_bvh(d_in, n, acc->nodes, acc->tris, scratch, sb, stream, &br);
+        cudaStreamSynchronize(stream);
+        cudaFree(d_in);
+        cudaFree(scratch);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "BVH build"));
+    }
+    if ((e = cudaStreamSynchronize(stream))) return cleanup(cuda_fail(e, "accel build sync"));
+    acc->view.nodes = acc->nodes;
+    acc->view.tris = acc->tris;
+    acc->view.planes = acc->planes;
+    acc->view.node_count = br.node_count;
+    acc->view.tri_count = n;
+    acc->view.plane_count = (uint32_t)planes.size();
+    acc->view.root_is_leaf = n <= 1;
+    acc->info.triangle_count = n;
+    acc->info.node_count = br.node_count;
+    acc->info.leaf_triangle_slots = n;
+    acc->info.plane_count = (uint32_t)planes.size();
+    acc->info.device_bytes = sizeof(WideNode) * node_cap + sizeof(TriSlot) * (uint64_t)(n ? n : 1) +
+                             sizeof(uint32_t) * (uint64_t)(n ? n : 1) + sizeof(DevPlane) * planes.size();
+    acc->info.build_ms = br.ms;
+    *out = acc;
+    return PB2_OK;
+}
+
+int pb2_accel_destroy(pb2_accel* acc) {
+    if (!acc) return PB2_OK;
+    cudaFree(acc->nodes);
+    cudaFree(acc->tris);
+    cudaFree(acc->planes);
+    cudaFree(acc->prim_material);
+    cudaFree(acc->work);
+    cudaFree(acc->counters);
+    cudaFree(acc->error_flag);
+    cudaFree(acc->stage);
+    delete acc;
+    return PB2_OK;
+}
+
+int pb2_accel_get_info(const pb2_accel* acc, pb2_accel_info* info) {
+    if (!acc || !info) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_get_info: null argument");
+    *info = acc->info;
+    return PB2_OK;
+}
+
+int pb2_accel_set_counting(pb2_accel* acc, int enable) {
+    if (!acc) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_set_counting: null accel");
+    acc->counting = enable != 0;
+    return PB2_OK;
+}
+
+int pb2_accel_get_counters(const pb2_accel* acc, uint64_t* node_visits, uint64_t* tri_tests, void* stream_ptr) {
+    if (!acc || !node_visits || !tri_tests) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_get_counters: null");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    unsigned long long c[2];
+    uint32_t flag = 0;
+    PB2_CUDA(cudaMemcpyAsync(c, acc->counters, sizeof(c), cudaMemcpyDeviceToHost, stream), "read counters");
+    PB2_CUDA(cudaMemcpyAsync(&flag, acc->error_flag, sizeof(flag), cudaMemcpyDeviceToHost, stream), "read flag");
+    PB2_CUDA(cudaStreamSynchronize(stream), "sync");
+    *node_visits = c[0];
+    *tri_tests = c[1];
+    if (flag) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow in an earlier trace call");
+    return PB2_OK;
+}
+
+static int trace_dev(const pb2_accel* acc, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occ, bool closest,
+                     cudaStream_t stream) {
+    if (acc->counting) PB2_CUDA(cudaMemsetAsync(acc->counters, 0, sizeof(unsigned long long) * 2, stream), "memset");
+    PB2_CUDA(launch_trace_api(acc->view, rays, n, hits, occ, closest, acc->counting, acc->work, acc->counters,
+                              acc->error_flag, stream),
+             closest ? "trace_closest launch" : "trace_any launch");
+    return PB2_OK;
+}
+
+int pb2_trace_closest(const pb2_accel* acc, const pb2_ray* rays, uint32_t n, pb2_hit* hits, void* stream) {
+    if (!acc || (n && (!rays || !hits))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_trace_closest: null argument");
+    return trace_dev(acc, rays, n, hits, nullptr, true, static_cast<cudaStream_t>(stream));
+}
+
+int pb2_trace_any(const pb2_accel* acc, const pb2_ray* rays, uint32_t n, uint32_t* occluded, void* stream) {
+    if (!acc || (n && (!rays || !occluded))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_trace_any: null argument");
+    return trace_dev(acc, rays, n, nullptr, occluded, false, static_cast<cudaStream_t>(stream));
+}
+
+static int ensure_stage(pb2_accel* acc, size_t bytes) {
+    if (acc->stage_bytes >= bytes) return PB2_OK;
+    cudaFree(acc->stage);
+    acc->stage = nullptr;
+    acc->stage_bytes = 0;
+    PB2_CUDA(cudaMalloc(&acc->stage, bytes), "cudaMalloc staging");
+    acc->stage_bytes = bytes;
+    return PB2_OK;
+}
+
+static int trace_host(const pb2_accel* cacc, const pb2_ray* rays, uint32_t n, void* out, bool closest,
+                      cudaStream_t stream) {
+    auto* acc = const_cast<pb2_accel*>(cacc);
+    const size_t rb = sizeof(pb2_ray) * (size_t)n;
+    const size_t ob = (closest ? sizeof(pb2_hit) : sizeof(uint32_t)) * (size_t)n;
+    int rc = ensure_stage(acc, rb + ob + 256);
+    if (rc) return rc;
+    auto* d_rays = static_cast<pb2_ray*>(acc->stage);
+    void* d_out = static_cast<char*>(acc->stage) + ((rb + 255) / 256) * 256;
+    PB2_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, stream), "upload rays");
+    rc = trace_dev(acc, d_rays, n, closest ? static_cast<pb2_hit*>(d_out) : nullptr,
+                   closest ? nullptr : static_cast<uint32_t*>(d_out), closest, stream);
+    if (rc) return rc;
+    PB2_CUDA(cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, stream), "download results");
+    PB2_CUDA(cudaStreamSynchronize(stream), "trace sync");
+    return PB2_OK;
+}
+
+int pb2_trace_closest_host(const pb2_accel* acc, const pb2_ray* rays, uint32_t n, pb2_hit* hits, void* stream) {
+    if (!acc || (n && (!rays || !hits))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_trace_closest_host: null");
+    return trace_host(acc, rays, n, hits, true, static_cast<cudaStream_t>(stream));
+}
+
+int pb2_trace_any_host(const pb2_accel* acc, const pb2_ray* rays, uint32_t n, uint32_t* occluded, void* stream) {
+    if (!acc || (n && (!rays || !occluded))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_trace_any_host: null");
+    return trace_host(acc, rays, n, occluded, false, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

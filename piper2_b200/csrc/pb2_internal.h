@@ -1,0 +1,38 @@
+// pb2_internal.h -- declarations shared between the library's translation units (not installed).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/piper2_b200.h"
+#include "pb2_bvh.h"
+
+namespace pb2 {
+
+// thread-local last error (pb2_last_error)
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what);
+
+cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
+                             bool closest, bool count, uint32_t* work, unsigned long long* counters,
+                             uint32_t* error_flag, cudaStream_t stream);
+
+}  // namespace pb2
+
+struct pb2_accel {
+    int device = 0;
+    pb2::WideNode* nodes = nullptr;
+    pb2::TriSlot* tris = nullptr;
+    pb2::DevPlane* planes = nullptr;
+    uint32_t* prim_material = nullptr;  // material of each global primitive
+    uint32_t* work = nullptr;           // work counters of the trace kernels
+    unsigned long long* counters = nullptr;
+    uint32_t* error_flag = nullptr;
+    bool counting = false;
+    pb2::BvhView view{};
+    pb2_accel_info info{};
+    // staging buffers of the *_host trace calls
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+};

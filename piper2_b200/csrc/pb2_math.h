@@ -1,0 +1,149 @@
+/*
+ * pb2_math.h -- elementary functions with one definition on the host and on sm_100a.
+ *
+ * The render path calls cos/sin (camera lens disk, cosine hemisphere, GGX slope sampling, environment
+ * sampling), acos (environment pdf) and exp (Gaussian film filter).  The reference calls the C library
+ * (Src/Kernel/PhysicalQuantitySI.hpp:162-175, Src/Kernel/Sampling.hpp:24-43,
+ * Src/BuiltinComponent/RenderDriver/FixedSampler/Kernel.cpp:65-69).  CUDA's and glibc's versions of
+ * those functions can differ in the last bit, which would let a single path diverge between the GPU
+ * and the CPU oracle.  These functions are written once here, from textbook methods, using only IEEE
+ * add/mul/div/sqrt and explicitly fused multiply-adds, so a host build with -ffp-contract=off and a
+ * device build give bit-identical results:
+ *
+ *   sin/cos : Cody-Waite reduction by pi/2 (three-part constant, fused), then the Taylor series of sin
+ *             (to x^9) and cos (to x^10) on |r| <= pi/4 -- truncation error < 3e-9 relative.
+ *   exp     : reduction by ln 2 (two-part constant), Taylor series to r^7 on |r| <= ln2/2, then an
+ *             exact power-of-two scale.
+ *   acos    : the binomial (arcsine) series on |x| <= 1/2, and acos(x) = 2 asin(sqrt((1-x)/2)) above.
+ *
+ * Accuracy is checked against the C library in the CPU tests and against CUDA's own functions in the
+ * GPU tests (a few ulp).
+ */
+#pragma once
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define PB2_HD static __host__ __device__ __forceinline__
+#else
+#define PB2_HD static inline
+#endif
+
+#if defined(__CUDA_ARCH__)
+#define PB2_FMA(a, b, c) __fmaf_rn((a), (b), (c))
+#define PB2_RINT(x) rintf(x)
+#else
+#define PB2_FMA(a, b, c) fmaf((a), (b), (c))
+#define PB2_RINT(x) rintf(x)
+#endif
+
+/* pi/2 split into three floats: hi = nearest float, mid/lo = successive remainders. */
+#define PB2_PIO2_HI 1.57079637050628662109375f
+#define PB2_PIO2_MID (-4.37113882867379289e-08f)
+#define PB2_PIO2_LO (-1.71512451000588187e-15f)
+#define PB2_TWO_OVER_PI 0.636619772367581343076f
+
+PB2_HD float pb2_ldexp_int(float x, int k) {
+    /* x * 2^k for k in [-252, 254] using exact power-of-two factors. */
+    while (k > 127) { x = x * 1.7014118346046923e38f; k -= 127; }
+    while (k < -126) { x = x * 1.1754943508222875e-38f; k += 126; }
+    union { uint32_t u; float f; } s;
+    s.u = (uint32_t)(k + 127) << 23;
+    return x * s.f;
+}
+
+PB2_HD void pb2_sincosf(float x, float* s_out, float* c_out) {
+    const float q = PB2_RINT(x * PB2_TWO_OVER_PI);
+    float r = PB2_FMA(-q, PB2_PIO2_HI, x);
+    r = PB2_FMA(-q, PB2_PIO2_MID, r);
+    r = PB2_FMA(-q, PB2_PIO2_LO, r);
+    const float r2 = r * r;
+    /* sin(r) = r + r^3 (-1/6 + r^2 (1/120 + r^2 (-1/5040 + r^2 / 362880))) */
+    float ps = PB2_FMA(r2, 2.75573192239858906526e-6f, -1.98412698412698412698e-4f);
+    ps = PB2_FMA(r2, ps, 8.33333333333333333333e-3f);
+    ps = PB2_FMA(r2, ps, -1.66666666666666666667e-1f);
+    const float s = PB2_FMA(r * r2, ps, r);
+    /* cos(r) = 1 + r^2 (-1/2 + r^2 (1/24 + r^2 (-1/720 + r^2 (1/40320 - r^2/3628800)))) */
+    float pc = PB2_FMA(r2, -2.75573192239858906526e-7f, 2.48015873015873015873e-5f);
+    pc = PB2_FMA(r2, pc, -1.38888888888888888889e-3f);
+    pc = PB2_FMA(r2, pc, 4.16666666666666666667e-2f);
+    pc = PB2_FMA(r2, pc, -0.5f);
+    const float c = PB2_FMA(r2, pc, 1.0f);
+    const int quadrant = ((int)q) & 3;
+    float so, co;
+    switch (quadrant) {
+        case 0: so = s; co = c; break;
+        case 1: so = c; co = -s; break;
+        case 2: so = -s; co = -c; break;
+        default: so = -c; co = s; break;
+    }
+    *s_out = so;
+    *c_out = co;
+}
+
+PB2_HD float pb2_sinf(float x) {
+    float s, c;
+    pb2_sincosf(x, &s, &c);
+    return s;
+}
+
+PB2_HD float pb2_cosf(float x) {
+    float s, c;
+    pb2_sincosf(x, &s, &c);
+    return c;
+}
+
+#define PB2_LN2_HI 0.693145751953125f
+#define PB2_LN2_LO 1.42860676533018705e-06f
+#define PB2_LOG2E 1.44269504088896340736f
+
+PB2_HD float pb2_expf(float x) {
+    if (x != x) return x;
+    if (x > 88.72283935546875f) return INFINITY;
+    if (x < -103.97208404541015625f) return 0.0f;
+    const float k = PB2_RINT(x * PB2_LOG2E);
+    float r = PB2_FMA(-k, PB2_LN2_HI, x);
+    r = PB2_FMA(-k, PB2_LN2_LO, r);
+    /* e^r = sum r^n / n!, n <= 7 */
+    float p = PB2_FMA(r, 1.98412698412698412698e-4f, 1.38888888888888888889e-3f);
+    p = PB2_FMA(r, p, 8.33333333333333333333e-3f);
+    p = PB2_FMA(r, p, 4.16666666666666666667e-2f);
+    p = PB2_FMA(r, p, 1.66666666666666666667e-1f);
+    p = PB2_FMA(r, p, 0.5f);
+    p = PB2_FMA(r, p, 1.0f);
+    p = PB2_FMA(r, p, 1.0f);
+    return pb2_ldexp_int(p, (int)k);
+}
+
+/* asin on |x| <= 1/2 by the binomial series x + sum_{n=1..11} c_n x^(2n+1),
+ * c_n = (2n)! / (4^n (n!)^2 (2n+1)); the first omitted term is below 4e-10 relative. */
+PB2_HD float pb2_asin_small(float x) {
+    const float z = x * x;
+    float p = 7.31252587359884544810e-03f;     /* c_11 = 88179/12058624 */
+    p = PB2_FMA(z, p, 8.39033580961681506316e-03f); /* c_10 = 46189/5505024 */
+    p = PB2_FMA(z, p, 9.76160952919407839956e-03f); /* c_9  = 12155/1245184 */
+    p = PB2_FMA(z, p, 1.15518008961397050660e-02f); /* c_8  = 6435/557056 */
+    p = PB2_FMA(z, p, 1.39648437500000006939e-02f); /* c_7  = 143/10240 */
+    p = PB2_FMA(z, p, 1.73527644230769238776e-02f); /* c_6  = 231/13312 */
+    p = PB2_FMA(z, p, 2.23721590909090918553e-02f); /* c_5  = 63/2816 */
+    p = PB2_FMA(z, p, 3.03819444444444440590e-02f); /* c_4  = 35/1152 */
+    p = PB2_FMA(z, p, 4.46428571428571438484e-02f); /* c_3  = 5/112 */
+    p = PB2_FMA(z, p, 7.49999999999999972244e-02f); /* c_2  = 3/40 */
+    p = PB2_FMA(z, p, 1.66666666666666657415e-01f); /* c_1  = 1/6 */
+    return PB2_FMA(x * z, p, x);
+}
+
+PB2_HD float pb2_acosf(float x) {
+    const float pio2 = 1.57079632679489661923f;
+    const float pi = 3.14159265358979323846f;
+    const float a = fabsf(x);
+    float r;
+    if (a <= 0.5f) {
+        r = pio2 - pb2_asin_small(x);
+    } else {
+        const float h = sqrtf((1.0f - a) * 0.5f);
+        const float t = 2.0f * pb2_asin_small(h);
+        r = x > 0.0f ? t : pi - t;
+    }
+    return r;
+}

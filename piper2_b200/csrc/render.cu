@@ -1,0 +1,1047 @@
+// render.cu -- the render pipeline: Sobol sampler, camera, wavefront path tracer, film.
+//
+// One launch renders `sample_count` samples of every pixel of a rectangle.  Each (pixel, sample) is a
+// path with SoA state in device memory.  A bounce is a fixed sequence of kernels over index queues:
+//   extend (closest hit of every active path) -> classify (emission, area-light pass-through, miss,
+//   depth limit; surface hits go to one queue per material type) -> shade<material> (NEE light
+//   sample + shadow ray, MIS BSDF sample + ray, continuation sample, Russian roulette) -> shadow
+//   (any hit) and MIS (closest hit) traces -> finish (adds the MIS estimate, re-queues or splats).
+// All per-path arithmetic is the reference's (PathTracing/Kernel.cpp:23-193) in its operation order,
+// so each path's radiance equals the CPU oracle's bit for bit; only the film sums, which use
+// atomics in any order (as the reference's CAS loop does), differ in rounding.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pb2_internal.h"
+#include "shading.cuh"
+#include "traverse.cuh"
+
+#define PB2_SOBOL_STORAGE static __device__ const
+#include "sobol_tables.h"
+
+namespace pb2 {
+
+__device__ __forceinline__ float sobol_sample(uint64_t index, uint32_t dim) {
+    uint32_t v = 0;
+    for (uint32_t i = dim * PB2_SOBOL_MATRIX_SIZE; index; index >>= 1, i++)
+        if (index & 1) v ^= __ldg(&pb2_sobol_matrices32[i]);
+    return (float)v * 0x1p-32f;
+}
+
+__device__ __forceinline__ uint64_t sobol_interval_to_index(uint32_t m, uint32_t sample, uint32_t px, uint32_t py) {
+    if (m == 0) return 0;
+    const uint32_t m2 = m << 1;
+    uint64_t index = (uint64_t)sample << m2;
+    uint64_t delta = 0;
+    for (int c = 0; sample; sample >>= 1, ++c)
+        if (sample & 1) delta ^= __ldg(&pb2_vdc_sobol_matrices[m - 1][c]);
+    uint64_t b = (((uint64_t)px << m) | py) ^ delta;
+    for (int c = 0; b; b >>= 1, ++c)
+        if (b & 1) index ^= __ldg(&pb2_vdc_sobol_matrices_inv[m - 1][c]);
+    return index;
+}
+
+__global__ void k_sobol_generate(const uint64_t* __restrict__ idx, const uint32_t* __restrict__ dim, uint32_t n,
+                                 float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = dim[i] < PB2_SOBOL_DIMS ? sobol_sample(idx[i], dim[i]) : 0.0f;
+}
+
+__global__ void k_sobol_start(uint32_t log2res, const uint32_t* __restrict__ pxs, uint32_t n, uint64_t* __restrict__ idx,
+                              float* __restrict__ off) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t px = pxs[3 * i], py = pxs[3 * i + 1], s = pxs[3 * i + 2];
+    const uint64_t id = sobol_interval_to_index(log2res, s, px, py);
+    const float res = (float)(1u << log2res);
+    idx[i] = id;
+    off[2 * i] = fminf(fmaxf(sobol_sample(id, 0) * res - (float)px, 0.0f), 1.0f);
+    off[2 * i + 1] = fminf(fmaxf(sobol_sample(id, 1) * res - (float)py, 0.0f), 1.0f);
+}
+
+// ---- pipeline state ------------------------------------------------------------------------------
+
+struct DevLight {
+    float radiance[3];
+    uint32_t first_plane, plane_count;
+    float area, inverse_area;
+    float translation[3];
+};
+
+constexpr int kNumSurfaceTypes = 7;
+
+// Counter slots in Paths::counts
+enum : int {
+    C_EXT_CUR = 0, C_EXT_NEXT = 1, C_SHADOW = 2, C_MIS = 3, C_SHADED = 4, C_SURF0 = 5,  // 5..11 per type
+    C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24, C_COUNT = 32
+};
+
+struct Paths {
+    float4* o;       // ray origin
+    float4* d;       // ray direction
+    float4* pf;      // throughput rgb, w = specular flag (0/1)
+    float4* rad;     // radiance rgb
+    unsigned long long* sidx;
+    uint32_t* dim;
+    uint32_t* depth;
+    float2* point;
+    float4* hit;     // t, prim, u, v (prim = PB2_INVALID_PRIM on a miss)
+    uint32_t* hit_slot;
+    // pending next-event estimation and MIS-BSDF sample of the current vertex
+    float4* mis_pf;    // pf at the vertex, w = 1 / select pdf... stored as the pdf itself
+    float4* nee;       // candidate light contribution (f * rad * w), w = 1 if a shadow ray was queued
+    float4* sh_o;      // shadow ray origin, w = tmin
+    float4* sh_d;      // shadow ray direction, w = tmax
+    float4* mr_o;      // MIS ray origin
+    float4* mr_d;      // MIS ray direction
+    float4* mr_f;      // sampled f, w = |wi.z| / pdf
+    float2* mr_pdf;    // x = bsdf pdf, y = selected light (as uint bits; 0 = environment)
+    uint32_t* flags;   // bit0 = has MIS, bit1 = continue, bit2 = MIS ray queued
+    uint32_t* occ;
+    float4* mhit;
+    // queues
+    uint32_t* ext[2];
+    uint32_t* surf[kNumSurfaceTypes];
+    uint32_t* shadow_q;
+    uint32_t* mis_q;
+    uint32_t* shaded_q;
+    uint32_t* counts;  // C_COUNT entries
+};
+
+struct LaunchParams {
+    pb2_rect rect;        // launch rectangle
+    pb2_rect full;        // full render rectangle
+    pb2_ndc_transform ndc;
+    uint32_t width, height;
+    uint32_t log2res;
+    uint32_t sample_begin, sample_count;
+    uint32_t max_depth, min_rr_depth;
+    uint32_t filter;
+    float gauss_neg_alpha, gauss_sub;
+    pb2_camera cam;
+    uint32_t num_lights;  // area lights
+    float env[3];
+    uint32_t path_count;
+};
+
+struct SceneView {
+    const DevMaterial* materials;
+    const uint32_t* prim_material;
+    const DevLight* lights;
+    const float* plane_cdf;
+    const float* plane_pdf;
+    BvhView bvh;
+};
+
+// ---- helpers ----------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t warp_push(uint32_t* counter) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t v) {
+    const unsigned mask = __activemask();
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    if ((int)(threadIdx.x & 31u) == __ffs(mask) - 1) atomicAdd(counter, (unsigned long long)v);
+}
+
+// The pixel/sample of path p: p = ((row * rect.width) + col) * sample_count + k
+__device__ __forceinline__ void path_coords(const LaunchParams& lp, uint32_t p, uint32_t& sx, uint32_t& sy,
+                                            uint32_t& s) {
+    const uint32_t k = p % lp.sample_count;
+    const uint32_t pix = p / lp.sample_count;
+    const uint32_t col = pix % lp.rect.width, row = pix / lp.rect.width;
+    sx = lp.rect.left + col - lp.full.left;
+    sy = lp.rect.top + row - lp.full.top;
+    s = lp.sample_begin + k;
+}
+
+// PerspectiveCamera rayGen (Src/BuiltinComponent/Sensor/PerspectiveCamera/Kernel.cpp:22-48)
+__device__ __forceinline__ void camera_ray(const pb2_camera& cam, float ndc_x, float ndc_y, float u1, float u2, v3& org,
+                                           v3& dir) {
+    const v3 base = mk3(cam.position[0], cam.position[1], cam.position[2]);
+    const v3 look = mk3(cam.look_at[0], cam.look_at[1], cam.look_at[2]);
+    const v3 forward = normalize3(sub3(look, base));
+    const v3 right = cross3(forward, mk3(cam.up[0], cam.up[1], cam.up[2]));
+    const v3 up = cross3(right, forward);
+    const v3 film_hit = add3(add3(base, mul3s(right, cam.sensor_size[0] * (0.5f - ndc_x))),
+                             mul3s(up, cam.sensor_size[1] * (ndc_y - 0.5f)));
+    const float focal_distance = dot3(sub3(look, base), forward);
+    const float film_distance = 1.0f / (1.0f / cam.focal_length - 1.0f / focal_distance);
+    const v3 lens_center = add3(base, mul3s(forward, film_distance));
+    const float ang = u1 * kTwoPi;
+    const float rad = sqrt_safe(u2);
+    float s, c;
+    pb2_sincosf(ang, &s, &c);
+    const float lx = rad * c, ly = rad * s;
+    const v3 lens_hit = add3(add3(lens_center, mul3s(right, cam.aperture_radius * lx)), mul3s(up, cam.aperture_radius * ly));
+    const v3 d = sub3(lens_center, film_hit);
+    const v3 focus_hit = add3(lens_center, mul3s(d, focal_distance / dot3(d, forward)));
+    org = lens_hit;
+    dir = normalize3(sub3(focus_hit, lens_hit));
+}
+
+// piperMain's sample set-up (Src/BuiltinComponent/Tracer/Embree/Kernel.cpp:47-90)
+__device__ __forceinline__ void primary_ray(const LaunchParams& lp, uint32_t sx, uint32_t sy, uint32_t s,
+                                            uint64_t& index, float& px, float& py, v3& org, v3& dir) {
+    const float res = (float)(1u << lp.log2res);
+    index = sobol_interval_to_index(lp.log2res, s, sx, sy);
+    const float offx = fminf(fmaxf(sobol_sample(index, 0) * res - (float)sx, 0.0f), 1.0f);
+    const float offy = fminf(fmaxf(sobol_sample(index, 1) * res - (float)sy, 0.0f), 1.0f);
+    px = offx + (float)(lp.full.left + sx);
+    py = offy + (float)(lp.full.top + sy);
+    const float ndc_x = lp.ndc.ox + lp.ndc.sx * px / (float)lp.width;
+    const float ndc_y = lp.ndc.oy + lp.ndc.sy * py / (float)lp.height;
+    const float u1 = sobol_sample(index, 3);
+    const float u2 = sobol_sample(index, 4);
+    camera_ray(lp.cam, ndc_x, ndc_y, u1, u2, org, dir);
+}
+
+__global__ void k_camera_rays(LaunchParams lp, uint32_t sample, float4* __restrict__ rays, float2* __restrict__ points) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= lp.rect.width * lp.rect.height) return;
+    const uint32_t col = i % lp.rect.width, row = i / lp.rect.width;
+    const uint32_t sx = lp.rect.left + col - lp.full.left, sy = lp.rect.top + row - lp.full.top;
+    uint64_t index;
+    float px, py;
+    v3 o, d;
+    primary_ray(lp, sx, sy, sample, index, px, py, o, d);
+    rays[2 * i] = make_float4(o.x, o.y, o.z, 1e-3f);
+    rays[2 * i + 1] = make_float4(d.x, d.y, d.z, 1e5f);
+    points[i] = make_float2(px, py);
+}
+
+__global__ void k_generate(LaunchParams lp, Paths ps) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= lp.path_count) return;
+    uint32_t sx, sy, s;
+    path_coords(lp, p, sx, sy, s);
+    uint64_t index;
+    float px, py;
+    v3 o, d;
+    primary_ray(lp, sx, sy, s, index, px, py, o, d);
+    ps.o[p] = make_float4(o.x, o.y, o.z, 0.0f);
+    ps.d[p] = make_float4(d.x, d.y, d.z, 0.0f);
+    ps.pf[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ps.sidx[p] = index;
+    ps.dim[p] = 5;
+    ps.depth[p] = 0;
+    ps.point[p] = make_float2(px, py);
+    ps.ext[0][p] = p;
+}
+
+// ---- traversal over queues -----------------------------------------------------------------------
+
+constexpr int kQThreads = 128;
+constexpr int kQRefill = 8;
+constexpr int kQSteps = 8;
+
+enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
+
+template <int kKind>
+__global__ void __launch_bounds__(kQThreads) k_trace_queue(BvhView bvh, Paths ps, const uint32_t* __restrict__ queue,
+                                                           const uint32_t* __restrict__ count_ptr, uint32_t* work,
+                                                           unsigned long long* stat) {
+    constexpr bool kClosest = kKind != Q_SHADOW;
+    const uint32_t n = *count_ptr;
+    Traverser<kClosest, false> tr;
+    bool active = false;
+    uint32_t slot = 0;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint32_t rays = 0;
+    for (;;) {
+        const unsigned inactive = __ballot_sync(0xFFFFFFFFu, !active);
+        if (__popc(inactive) >= kQRefill) {
+            const int leader = __ffs(inactive) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(work, (uint32_t)__popc(inactive));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (!active) {
+                const uint32_t idx = base + __popc(inactive & lt_mask);
+                if (idx < n) {
+                    slot = queue[idx];
+                    float4 a, b;
+                    if (kKind == Q_EXTEND) {
+                        a = ps.o[slot]; b = ps.d[slot];
+                        a.w = 1e-3f; b.w = 1e5f;
+                    } else if (kKind == Q_MIS) {
+                        a = ps.mr_o[slot]; b = ps.mr_d[slot];
+                        a.w = 1e-3f; b.w = 1e5f;
+                    } else {
+                        a = ps.sh_o[slot]; b = ps.sh_d[slot];
+                    }
+                    tr.init(bvh, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w);
+                    active = true;
+                    ++rays;
+                }
+            }
+            if (__ballot_sync(0xFFFFFFFFu, active) == 0u) break;
+        }
+        if (active) {
+            for (int it = 0; it < kQSteps && !tr.done; ++it) tr.step(bvh);
+            if (tr.done) {
+                if (kClosest) {
+                    bool front;
+                    tr.finish_planes(bvh, front);
+                    const float4 h = make_float4(tr.tbest, __uint_as_float(tr.best_prim), tr.bu, tr.bv);
+                    if (kKind == Q_EXTEND) {
+                        ps.hit[slot] = h;
+                        ps.hit_slot[slot] = tr.best_slot;
+                    } else {
+                        ps.mhit[slot] = h;
+                    }
+                } else {
+                    ps.occ[slot] = tr.best_prim != kInvalidPrim ? 1u : 0u;
+                }
+                if (tr.overflow) atomicOr(&ps.counts[C_ERROR], 1u);
+                active = false;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) rays += __shfl_xor_sync(0xFFFFFFFFu, rays, o);
+    if (lane == 0 && rays) atomicAdd(stat, (unsigned long long)rays);
+}
+
+// ---- film -------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ float filter_weight(const LaunchParams& lp, float dx, float dy) {
+    if (lp.filter == PB2_FILTER_TRIANGLE) return fmaxf(0.0f, 1.0f - fabsf(dx)) * fmaxf(0.0f, 1.0f - fabsf(dy));
+    if (lp.filter == PB2_FILTER_GAUSSIAN) {
+        const float wx = fmaxf(pb2_expf(lp.gauss_neg_alpha * dx * dx) - lp.gauss_sub, 0.0f);
+        const float wy = fmaxf(pb2_expf(lp.gauss_neg_alpha * dy * dy) - lp.gauss_sub, 0.0f);
+        return wx * wy;
+    }
+    return 1.0f;
+}
+
+// accumulate (Src/BuiltinComponent/RenderDriver/FixedSampler/Kernel.cpp:30-52)
+__device__ __forceinline__ void splat(const LaunchParams& lp, float4* film, float px, float py, spec v) {
+    const int32_t bx = (int32_t)(px - 0.5f), by = (int32_t)(py - 0.5f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t x = (uint32_t)(bx + (k & 1)), y = (uint32_t)(by + (k >> 1));
+        if (!(x < lp.width && y < lp.height)) continue;
+        const float w = filter_weight(lp, px - ((float)x + 0.5f), py - ((float)y + 0.5f));
+        atomicAdd(&film[(size_t)x + (size_t)y * lp.width], make_float4(v.r * w, v.g * w, v.b * w, w));
+    }
+}
+
+__device__ __forceinline__ void terminate_path(const LaunchParams& lp, const Paths& ps, uint32_t slot, float4* film,
+                                               float* sample_out) {
+    const float4 r = ps.rad[slot];
+    const float2 pt = ps.point[slot];
+    if (film) splat(lp, film, pt.x, pt.y, mksp(r.x, r.y, r.z));
+    if (sample_out) {
+        float* o = sample_out + 5 * (size_t)slot;
+        o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
+    }
+}
+
+// ---- classify extend results (PathTracing/Kernel.cpp:116-149) ------------------------------------
+
+__global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur, float4* film, float* sample_out) {
+    const uint32_t n = ps.counts[C_EXT_CUR];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ps.ext[cur][i];
+        const float4 h = ps.hit[slot];
+        const uint32_t prim = __float_as_uint(h.y);
+        const float4 o4 = ps.o[slot], d4 = ps.d[slot];
+        const float4 pf4 = ps.pf[slot];
+        const bool specular = pf4.w != 0.0f;
+        const bool missing = prim == kInvalidPrim;
+        const bool area = !missing && (prim & kPlaneFlag);
+        spec sample = mksp(ps.rad[slot].x, ps.rad[slot].y, ps.rad[slot].z);
+        const spec pf = mksp(pf4.x, pf4.y, pf4.z);
+        const v3 d = mk3(d4.x, d4.y, d4.z);
+        if (specular && (area || missing)) {
+            spec rad;
+            if (area) {
+                const DevPlane& pl = sv.bvh.planes[prim & ~kPlaneFlag];
+                // planeSurface: N faces the ray (face from the renormalised direction, Embree.cpp:573-577)
+                const v3 dn = normalize3(d);
+                const v3 nrm = mk3(pl.normal[0], pl.normal[1], pl.normal[2]);
+                const bool front = dot3(dn, nrm) > 0.0f;
+                const v3 N = front ? neg3(nrm) : nrm;
+                const v3 wi = normalize3(mul3s(d, h.x));
+                const DevLight& L = sv.lights[pl.light];
+                rad = dot3(N, wi) < 0.0f ? mksp(L.radiance[0], L.radiance[1], L.radiance[2]) : sp_zero();
+            } else {
+                rad = mksp(lp.env[0], lp.env[1], lp.env[2]);
+            }
+            sample = sp_add(sample, sp_mul(pf, rad));
+            ps.rad[slot] = make_float4(sample.r, sample.g, sample.b, 0.0f);
+        }
+        if (area) {
+            // pass through the light, one bounce credited back (the uint32 depth may wrap)
+            ps.depth[slot] = ps.depth[slot] - 1u;
+            const v3 o = add3(mk3(o4.x, o4.y, o4.z), mul3s(d, h.x + 0.001f));
+            ps.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+            ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
+            continue;
+        }
+        if (missing || ps.depth[slot] >= lp.max_depth) {
+            terminate_path(lp, ps, slot, film, sample_out);
+            continue;
+        }
+        const uint32_t type = sv.materials[sv.prim_material[prim]].type;
+        ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
+    }
+}
+
+// ---- shading (PathTracing/Kernel.cpp:23-107, 150-190) ---------------------------------------------
+
+struct SampleCursor {
+    uint64_t index;
+    uint32_t dim;
+    __device__ __forceinline__ float next() {
+        if (dim >= PB2_SOBOL_DIMS) return 0.5f;  // unreachable: the pipeline rejects depths that could get here
+        return sobol_sample(index, dim++);
+    }
+    // the two piperSample() arguments of one call are evaluated right to left (u2 first)
+    __device__ __forceinline__ void pair(float& u1, float& u2) {
+        u2 = next();
+        u1 = next();
+    }
+};
+
+// select() of Src/Kernel/Sampling.hpp:52-63 (u remapped with cdf[r] itself)
+__device__ __forceinline__ uint32_t cdf_select(const float* cdf, const float* pdf, uint32_t size, float& u) {
+    uint32_t l = 0, r = size;
+    while (l < r) {
+        const uint32_t mid = (l + r) >> 1;
+        if (u >= cdf[mid]) l = mid + 1;
+        else r = mid;
+    }
+    u = (u - cdf[r]) / pdf[r];
+    return r;
+}
+
+struct LightSample {
+    v3 dir;
+    spec rad;
+    float pdf, distance;
+};
+
+// diffuseSample over planeSample (AreaLight/Kernel.cpp:24-41, BasicShapes/Kernel.cpp:113-134)
+__device__ __forceinline__ void area_sample(const SceneView& sv, uint32_t li, v3 hit, float u1, float u2, LightSample& ls) {
+    const DevLight& L = sv.lights[li];
+    const uint32_t idx = cdf_select(sv.plane_cdf + L.first_plane, sv.plane_pdf + L.first_plane, L.plane_count, u1);
+    const DevPlane& pl = sv.bvh.planes[L.first_plane + idx];
+    const v3 lp = add3(add3(mk3(pl.origin[0], pl.origin[1], pl.origin[2]), mul3s(mk3(pl.u[0], pl.u[1], pl.u[2]), u1)),
+                       mul3s(mk3(pl.v[0], pl.v[1], pl.v[2]), u2));
+    const v3 src = add3(lp, mk3(L.translation[0], L.translation[1], L.translation[2]));
+    v3 n = mk3(pl.normal[0], pl.normal[1], pl.normal[2]);
+    if (dot3(sub3(hit, src), n) <= 0.0f) n = neg3(n);
+    const float pdf = L.inverse_area;
+    const v3 delta = sub3(src, hit);
+    if (pdf == 0.0f || dot3(delta, n) >= 0.0f) {
+        ls.pdf = 0.0f;
+        return;
+    }
+    ls.rad = mksp(L.radiance[0], L.radiance[1], L.radiance[2]);
+    const float dis2 = len2_3(delta);
+    ls.distance = sqrtf(dis2);
+    ls.dir = div3s(delta, ls.distance);
+    ls.pdf = pdf * dis2 / fabsf(dot3(n, ls.dir));
+}
+
+// SESample (BasicLight/Kernel.cpp:61-73)
+__device__ __forceinline__ void env_sample(const LaunchParams& lp, float u1, float u2, LightSample& ls) {
+    ls.rad = mksp(lp.env[0], lp.env[1], lp.env[2]);
+    const float theta = u1 * kPi, phi = u2 * kPi;
+    float st, ct, sp, cp;
+    pb2_sincosf(theta, &st, &ct);
+    pb2_sincosf(phi, &sp, &cp);
+    ls.dir = mk3(st * cp, st * sp, ct);
+    ls.pdf = st == 0.0f ? 0.0f : 1.0f / ((2.0f * kSqrPi) * st);
+    ls.distance = 1e5f;
+}
+
+// SEPdf (BasicLight/Kernel.cpp:80-89)
+__device__ __forceinline__ float env_pdf(v3 dir) {
+    const float theta = pb2_acosf(fmaxf(-1.0f, fminf(1.0f, dir.z)));
+    const float st = pb2_sinf(theta);
+    return st == 0.0f ? 0.0f : 1.0f / ((2.0f * kSqrPi) * st);
+}
+
+struct Frame {
+    v3 T, B, N, Ng;
+};
+__device__ __forceinline__ v3 to_shading(const Frame& f, v3 v) { return mk3(dot3(f.T, v), dot3(f.B, v), dot3(f.N, v)); }
+__device__ __forceinline__ v3 to_local(const Frame& f, v3 v) {
+    return mk3(f.T.x * v.x + f.B.x * v.y + f.N.x * v.z, f.T.y * v.x + f.B.y * v.y + f.N.y * v.z,
+               f.T.z * v.x + f.B.z * v.y + f.N.z * v.z);
+}
+
+template <int kType>
+__global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
+    const uint32_t n = ps.counts[C_SURF0 + kType];
+    uint32_t vertices = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ps.surf[kType][i];
+        ++vertices;
+        const float4 h = ps.hit[slot];
+        const uint32_t prim = __float_as_uint(h.y);
+        const float4 o4 = ps.o[slot], d4 = ps.d[slot], pf4 = ps.pf[slot];
+        const v3 o = mk3(o4.x, o4.y, o4.z), d = mk3(d4.x, d4.y, d4.z);
+        spec pf = mksp(pf4.x, pf4.y, pf4.z);
+        uint32_t depth = ps.depth[slot];
+        SampleCursor sc{ ps.sidx[slot], ps.dim[slot] };
+        // calcTriangleMeshSurface (Tracer/Embree/Kernel.cpp:170-192) with face from Embree.cpp:336
+        const uint32_t hs = ps.hit_slot[slot];
+        const float4* t4 = reinterpret_cast<const float4*>(sv.bvh.tris + hs);
+        const float4 a = t4[0], b = t4[1], c = t4[2];
+        const v3 p0 = mk3(a.x, a.y, a.z), p1 = mk3(b.x, b.y, b.z), p2 = mk3(c.x, c.y, c.z);
+        const v3 ng = normalize3(cross3(sub3(p1, p0), sub3(p2, p0)));
+        const bool front = dot3(d, ng) < 0.0f;
+        Frame fr;
+        fr.N = fr.Ng = front ? ng : neg3(ng);
+        if (fabsf(dot3(fr.N, mk3(1.0f, 0.0f, 0.0f))) < fabsf(dot3(fr.N, mk3(0.0f, 1.0f, 0.0f))))
+            fr.T = cross3(fr.N, mk3(1.0f, 0.0f, 0.0f));
+        else
+            fr.T = cross3(fr.N, mk3(0.0f, 1.0f, 0.0f));
+        fr.B = cross3(fr.N, fr.T);
+        const v3 wo = to_shading(fr, neg3(d));
+        const v3 ng_sh = to_shading(fr, fr.Ng);
+        Bsdf bsdf;
+        bsdf_init(sv.materials[sv.prim_material[prim]], front, bsdf);
+        const v3 hit = add3(o, mul3s(d, h.x));
+        uint32_t flags = 0;
+        if (bsdf.no_specular) {
+            // multipleImportanceSampling (PathTracing/Kernel.cpp:23-107)
+            flags |= 1u;
+            const uint32_t count = 1u + lp.num_lights;
+            const float u = sc.next();
+            uint32_t sel = (uint32_t)floorf(u * (float)count);
+            if (sel > count - 1) sel = count - 1;
+            const float sel_pdf = 1.0f / (float)count;
+            ps.mis_pf[slot] = make_float4(pf.r, pf.g, pf.b, sel_pdf);
+            float4 nee = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            {
+                LightSample ls;
+                float u1, u2;
+                sc.pair(u1, u2);
+                if (sel == 0) env_sample(lp, u1, u2, ls);
+                else area_sample(sv, sel - 1, hit, u1, u2, ls);
+                if (ls.pdf > 0.0f && sp_valid(ls.rad)) {
+                    const v3 wi = to_shading(fr, ls.dir);
+                    const spec f = bsdf_eval(bsdf, wo, wi, ng_sh, kPartNoSpecular);
+                    if (sp_valid(f)) {
+                        float w = fabsf(wi.z) / ls.pdf;
+                        const float bp = bsdf_pdf(bsdf, wo, wi, kPartNoSpecular);
+                        w = w * power_heuristic(ls.pdf, bp);
+                        const spec cand = sp_muls(sp_mul(f, ls.rad), w);
+                        nee = make_float4(cand.r, cand.g, cand.b, 1.0f);
+                        ps.sh_o[slot] = make_float4(hit.x, hit.y, hit.z, fminf(1e-3f, ls.distance));
+                        ps.sh_d[slot] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.distance);
+                        ps.shadow_q[warp_push(&ps.counts[C_SHADOW])] = slot;
+                    }
+                }
+            }
+            ps.nee[slot] = nee;
+            {
+                BsdfSample bs;
+                float u1, u2;
+                sc.pair(u1, u2);
+                bsdf_sample(bsdf, u1, u2, wo, ng_sh, kPartNoSpecular, bs);
+                if (bs.pdf > 0.0f && sp_valid(bs.f)) {
+                    const float weight = fabsf(bs.wi.z) / bs.pdf;
+                    const v3 dir = to_local(fr, bs.wi);
+                    ps.mr_o[slot] = make_float4(hit.x, hit.y, hit.z, 0.0f);
+                    ps.mr_d[slot] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+                    ps.mr_f[slot] = make_float4(bs.f.r, bs.f.g, bs.f.b, weight);
+                    ps.mr_pdf[slot] = make_float2(bs.pdf, __uint_as_float(sel));
+                    ps.mis_q[warp_push(&ps.counts[C_MIS])] = slot;
+                    flags |= 4u;
+                }
+            }
+        }
+        // continuation (PathTracing/Kernel.cpp:164-190)
+        BsdfSample ss;
+        float u1, u2;
+        sc.pair(u1, u2);
+        bsdf_sample(bsdf, u1, u2, wo, ng_sh, kPartAll, ss);
+        bool cont = ss.pdf > 0.0f && sp_valid(ss.f);
+        if (cont) {
+            pf = sp_muls(sp_mul(pf, ss.f), fabsf(ss.wi.z) / ss.pdf);
+            if (depth > lp.min_rr_depth) {
+                const float p = fmaxf(0.05f, 1.0f - fmaxf(pf.r, fmaxf(pf.g, pf.b)));
+                if (sc.next() < p) cont = false;
+                else pf = sp_divs(pf, 1.0f - p);
+            }
+        }
+        if (cont) {
+            const v3 nd = to_local(fr, ss.wi);
+            const v3 no = add3(hit, mul3s(fr.Ng, (ss.part & kPartR) ? 0.001f : -0.001f));
+            ps.o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+            ps.d[slot] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+            ps.pf[slot] = make_float4(pf.r, pf.g, pf.b, (ss.part & kPartSpecular) ? 1.0f : 0.0f);
+            ps.depth[slot] = depth + 1u;
+            flags |= 2u;
+        }
+        ps.dim[slot] = sc.dim;
+        ps.flags[slot] = flags;
+        ps.shaded_q[warp_push(&ps.counts[C_SHADED])] = slot;
+    }
+    if (vertices) warp_count(reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_VERTICES), vertices);
+}
+
+// ---- finish: add the vertex's MIS estimate, then re-queue or splat --------------------------------
+
+__global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur, float4* film, float* sample_out) {
+    const uint32_t n = ps.counts[C_SHADED];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ps.shaded_q[i];
+        const uint32_t flags = ps.flags[slot];
+        if (flags & 1u) {
+            const float4 nee = ps.nee[slot];
+            spec part_a = sp_zero();
+            if (nee.w != 0.0f && ps.occ[slot] == 0u) part_a = mksp(nee.x, nee.y, nee.z);
+            spec part_b = sp_zero();
+            if (flags & 4u) {
+                const float4 mh = ps.mhit[slot];
+                const uint32_t prim = __float_as_uint(mh.y);
+                const float2 mp = ps.mr_pdf[slot];
+                const uint32_t sel = __float_as_uint(mp.y);
+                const float4 md = ps.mr_d[slot];
+                const v3 dir = mk3(md.x, md.y, md.z);
+                const bool missing = prim == kInvalidPrim;
+                bool is_sel_light = false;
+                uint32_t light = 0;
+                if (!missing && (prim & kPlaneFlag)) {
+                    light = sv.bvh.planes[prim & ~kPlaneFlag].light;
+                    is_sel_light = sel != 0 && light == sel - 1;
+                }
+                if (is_sel_light || missing) {
+                    spec rad;
+                    float pdf;
+                    if (missing) {
+                        rad = mksp(lp.env[0], lp.env[1], lp.env[2]);
+                        pdf = sp_valid(rad) ? env_pdf(dir) : 0.0f;
+                    } else {
+                        const DevPlane& pl = sv.bvh.planes[prim & ~kPlaneFlag];
+                        const v3 dn = normalize3(dir);
+                        const v3 nrm = mk3(pl.normal[0], pl.normal[1], pl.normal[2]);
+                        const v3 N = dot3(dn, nrm) > 0.0f ? neg3(nrm) : nrm;
+                        const DevLight& L = sv.lights[light];
+                        rad = dot3(N, dir) < 0.0f ? mksp(L.radiance[0], L.radiance[1], L.radiance[2]) : sp_zero();
+                        pdf = mh.x * mh.x / (fabsf(dot3(N, dir)) * L.area);
+                    }
+                    if (sp_valid(rad) && pdf > 0.0f) {
+                        const float4 mf = ps.mr_f[slot];
+                        const float weight = mf.w * power_heuristic(mp.x, pdf);
+                        part_b = sp_muls(sp_mul(rad, mksp(mf.x, mf.y, mf.z)), weight);
+                    }
+                }
+            }
+            const float4 mpf = ps.mis_pf[slot];
+            const spec mis = sp_divs(sp_add(part_a, part_b), mpf.w);
+            const float4 r = ps.rad[slot];
+            const spec sample = sp_add(mksp(r.x, r.y, r.z), sp_mul(mksp(mpf.x, mpf.y, mpf.z), mis));
+            ps.rad[slot] = make_float4(sample.r, sample.g, sample.b, 0.0f);
+        }
+        if (flags & 2u) ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
+        else terminate_path(lp, ps, slot, film, sample_out);
+    }
+}
+
+// Per-bounce bookkeeping: next extend queue becomes current; clear per-bounce counters.
+__global__ void k_advance(uint32_t* counts) {
+    counts[C_EXT_CUR] = counts[C_EXT_NEXT];
+    counts[C_EXT_NEXT] = 0;
+    counts[C_SHADOW] = 0;
+    counts[C_MIS] = 0;
+    counts[C_SHADED] = 0;
+    for (int t = 0; t < kNumSurfaceTypes; ++t) counts[C_SURF0 + t] = 0;
+}
+
+__global__ void k_resolve(const float4* __restrict__ rgbw, uint32_t n, float* __restrict__ rgb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = rgbw[i];
+    if (v.w != 0.0f) {
+        rgb[3 * i] = v.x / v.w;
+        rgb[3 * i + 1] = v.y / v.w;
+        rgb[3 * i + 2] = v.z / v.w;
+    } else {
+        rgb[3 * i] = rgb[3 * i + 1] = rgb[3 * i + 2] = 0.0f;
+    }
+}
+
+}  // namespace pb2
+
+// ====================================================================================================
+// host side
+// ====================================================================================================
+using namespace pb2;
+
+const char* pb2_sobol_table_sha256() { return PB2_SOBOL_TABLE_SHA256; }
+
+struct pb2_pipeline {
+    pb2_accel* accel = nullptr;
+    pb2_render_settings settings{};
+    pb2_rect full{};
+    pb2_ndc_transform ndc{};
+    uint32_t log2res = 0;
+    DevMaterial* materials = nullptr;
+    DevLight* lights = nullptr;
+    float* plane_cdf = nullptr;
+    float* plane_pdf = nullptr;
+    uint32_t num_lights = 0;
+    float env[3] = { 0, 0, 0 };
+    float gauss_sub = 0.0f;
+    // path state
+    uint32_t capacity = 0;
+    void* state = nullptr;
+    Paths ps{};
+    pb2_launch_stats stats{};
+    int sms = 0;
+};
+
+static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
+    if (pl->capacity >= cap) return PB2_OK;
+    cudaFree(pl->state);
+    pl->state = nullptr;
+    pl->capacity = 0;
+    const size_t c = cap;
+    size_t bytes = 0;
+    auto sz = [&](size_t b) { bytes += ((b + 255) / 256) * 256; };
+    // 14 float4 arrays, sidx, dim, depth, point, hit_slot, mr_pdf, flags, occ, queues (2 + types + 3), counts
+    sz(c * 16 * 14); sz(c * 8); sz(c * 4); sz(c * 4); sz(c * 8); sz(c * 4); sz(c * 8); sz(c * 4); sz(c * 4);
+    for (int q = 0; q < 2 + kNumSurfaceTypes + 3; ++q) sz(c * 4);
+    sz(sizeof(uint32_t) * C_COUNT);
+    cudaError_t e = cudaMalloc(&pl->state, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc path state");
+    char* p = static_cast<char*>(pl->state);
+    auto carve = [&](size_t b) {
+        void* r = p;
+        p += ((b + 255) / 256) * 256;
+        return r;
+    };
+    Paths& s = pl->ps;
+    s.o = (float4*)carve(c * 16); s.d = (float4*)carve(c * 16); s.pf = (float4*)carve(c * 16);
+    s.rad = (float4*)carve(c * 16); s.hit = (float4*)carve(c * 16); s.mis_pf = (float4*)carve(c * 16);
+    s.nee = (float4*)carve(c * 16); s.sh_o = (float4*)carve(c * 16); s.sh_d = (float4*)carve(c * 16);
+    s.mr_o = (float4*)carve(c * 16); s.mr_d = (float4*)carve(c * 16); s.mr_f = (float4*)carve(c * 16);
+    s.mhit = (float4*)carve(c * 16);
+    carve(c * 16);  // spare
+    s.sidx = (unsigned long long*)carve(c * 8);
+    s.dim = (uint32_t*)carve(c * 4);
+    s.depth = (uint32_t*)carve(c * 4);
+    s.point = (float2*)carve(c * 8);
+    s.hit_slot = (uint32_t*)carve(c * 4);
+    s.mr_pdf = (float2*)carve(c * 8);
+    s.flags = (uint32_t*)carve(c * 4);
+    s.occ = (uint32_t*)carve(c * 4);
+    s.ext[0] = (uint32_t*)carve(c * 4);
+    s.ext[1] = (uint32_t*)carve(c * 4);
+    for (int t = 0; t < kNumSurfaceTypes; ++t) s.surf[t] = (uint32_t*)carve(c * 4);
+    s.shadow_q = (uint32_t*)carve(c * 4);
+    s.mis_q = (uint32_t*)carve(c * 4);
+    s.shaded_q = (uint32_t*)carve(c * 4);
+    s.counts = (uint32_t*)carve(sizeof(uint32_t) * C_COUNT);
+    pl->capacity = cap;
+    return PB2_OK;
+}
+
+static float remap_roughness(float roughness) {
+    const float x = std::log(std::fmax(1e-3f, roughness));
+    return std::fmax(1e-3f, 1.62142f + (0.819955f + (0.1734f + (0.0171201f + 0.000640711f * x) * x) * x) * x);
+}
+
+extern "C" {
+
+int pb2_sobol_generate(const uint64_t* idx, const uint32_t* dim, uint32_t n, float* out, void* stream) {
+    if (n == 0) return PB2_OK;
+    if (!idx || !dim || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_sobol_generate: null argument");
+    k_sobol_generate<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(idx, dim, n, out);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "k_sobol_generate");
+}
+
+int pb2_sobol_start(uint32_t log2_resolution, const uint32_t* pixel_sample, uint32_t n, uint64_t* index, float* offset,
+                    void* stream) {
+    if (n == 0) return PB2_OK;
+    if (!pixel_sample || !index || !offset) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_sobol_start: null argument");
+    if (log2_resolution > PB2_SOBOL_VDC_LEVELS) return fail(PB2_ERR_NOT_SUPPORTED, "pb2_sobol_start: resolution > 2^25");
+    k_sobol_start<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(log2_resolution, pixel_sample, n, index,
+                                                                                   offset);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "k_sobol_start");
+}
+
+int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, void* stream_ptr, pb2_pipeline** out) {
+    if (!scene || !st || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_create: null argument");
+    *out = nullptr;
+    if (st->scramble) return fail(PB2_ERR_NOT_SUPPORTED, "Scramble is not implemented by the reference sampler");
+    if (st->width == 0 || st->height == 0) return fail(PB2_ERR_INVALID_ARGUMENT, "empty film");
+    if (st->samples_per_pixel == 0 || (st->samples_per_pixel & (st->samples_per_pixel - 1)))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "samples_per_pixel must be a power of two (the sampler rounds it up)");
+    if (5ull + 8ull * st->max_depth > PB2_SOBOL_DIMS)
+        return fail(PB2_ERR_NOT_SUPPORTED, "max_depth would use Sobol dimensions past 1023 (the reference's "
+                                           "mt19937_64 tail is not reproduced)");
+    if (st->filter > PB2_FILTER_GAUSSIAN) return fail(PB2_ERR_INVALID_ARGUMENT, "unknown filter");
+    for (uint32_t m = 0; m < scene->material_count; ++m)
+        if (scene->materials[m].type > PB2_SURFACE_CONDUCTOR) return fail(PB2_ERR_INVALID_ARGUMENT, "unknown surface type");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    auto* pl = new pb2_pipeline();
+    int rc = pb2_accel_create(scene, stream_ptr, &pl->accel);
+    if (rc) {
+        delete pl;
+        return rc;
+    }
+    pl->settings = *st;
+    rc = pb2_calc_render_rect(st->width, st->height, st->camera.sensor_size[0] / st->camera.sensor_size[1], st->fit_mode,
+                              &pl->ndc, &pl->full);
+    if (rc) {
+        pb2_pipeline_destroy(pl);
+        return rc;
+    }
+    const uint32_t mx = pl->full.width > pl->full.height ? pl->full.width : pl->full.height;
+    pl->log2res = (uint32_t)std::ceil(std::log2((double)mx));
+    if (pl->log2res > PB2_SOBOL_VDC_LEVELS) {
+        pb2_pipeline_destroy(pl);
+        return fail(PB2_ERR_NOT_SUPPORTED, "film larger than 2^25");
+    }
+    pl->gauss_sub = std::exp(-st->gaussian_alpha);
+    // materials
+    std::vector<DevMaterial> mats(scene->material_count ? scene->material_count : 1);
+    for (uint32_t m = 0; m < scene->material_count; ++m) {
+        const pb2_material& s = scene->materials[m];
+        DevMaterial& d = mats[m];
+        std::memset(&d, 0, sizeof(d));
+        d.type = s.type;
+        for (int k = 0; k < 3; ++k) { d.c0[k] = s.color0[k]; d.c1[k] = s.color1[k]; }
+        d.valid0 = s.color0[0] > 0.0f || s.color0[1] > 0.0f || s.color0[2] > 0.0f;
+        d.valid1 = s.color1[0] > 0.0f || s.color1[1] > 0.0f || s.color1[2] > 0.0f;
+        d.roughness0 = s.roughness[0];
+        d.roughness1 = s.roughness[1];
+        if (s.type == PB2_SURFACE_CONDUCTOR) {
+            d.ax = d.ay = s.roughness[0];
+        } else if (s.type == PB2_SURFACE_PLASTIC) {
+            d.ax = d.ay = remap_roughness(s.roughness[0]);
+        } else {
+            d.ax = remap_roughness(s.roughness[0]);
+            d.ay = remap_roughness(s.roughness[1]);
+        }
+        // OrenNayar (Classic/Kernel.cpp:103-109)
+        const float sigma = s.roughness[0] * 3.14159265358979323846f;
+        const float sigma2 = sigma * sigma;
+        d.on_a = 1.0f - (sigma2 / (2.0f * (sigma2 + 0.33f)));
+        d.on_b = 0.45f * sigma2 / (sigma2 + 0.09f);
+    }
+    // lights (AreaLight.cpp, BasicShapes.cpp:76-94)
+    std::vector<DevLight> lights(scene->area_light_count ? scene->area_light_count : 1);
+    std::vector<float> cdf(scene->plane_count ? scene->plane_count : 1, 0.0f), pdf(cdf.size(), 0.0f);
+    for (uint32_t l = 0; l < scene->area_light_count; ++l) {
+        const pb2_area_light& al = scene->area_lights[l];
+        DevLight& L = lights[l];
+        for (int k = 0; k < 3; ++k) { L.radiance[k] = al.radiance[k]; L.translation[k] = al.translation[k]; }
+        L.first_plane = al.first_plane;
+        L.plane_count = al.plane_count;
+        float total = 0.0f;
+        for (uint32_t i = 0; i < al.plane_count; ++i) {
+            const pb2_plane& p = scene->planes[al.first_plane + i];
+            const float d0 = p.u[1] * p.v[2] - p.u[2] * p.v[1];
+            const float d1 = p.u[2] * p.v[0] - p.u[0] * p.v[2];
+            const float d2 = p.u[0] * p.v[1] - p.u[1] * p.v[0];
+            const float area = std::sqrt(std::fmax(d0 * d0 + d1 * d1 + d2 * d2, 0.0f));
+            total = total + area;
+            cdf[al.first_plane + i] = total;
+            pdf[al.first_plane + i] = area;
+        }
+        for (uint32_t i = 0; i < al.plane_count; ++i) {
+            cdf[al.first_plane + i] = cdf[al.first_plane + i] / total;
+            pdf[al.first_plane + i] = pdf[al.first_plane + i] / total;
+        }
+        L.area = total;
+        L.inverse_area = 1.0f / total;
+    }
+    pl->num_lights = scene->area_light_count;
+    for (int k = 0; k < 3; ++k) pl->env[k] = scene->env_radiance[k];
+    cudaError_t e;
+    if ((e = cudaMalloc(&pl->materials, sizeof(DevMaterial) * mats.size())) ||
+        (e = cudaMalloc(&pl->lights, sizeof(DevLight) * lights.size())) ||
+        (e = cudaMalloc(&pl->plane_cdf, sizeof(float) * cdf.size())) ||
+        (e = cudaMalloc(&pl->plane_pdf, sizeof(float) * pdf.size())) ||
+        (e = cudaMemcpyAsync(pl->materials, mats.data(), sizeof(DevMaterial) * mats.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaMemcpyAsync(pl->lights, lights.data(), sizeof(DevLight) * lights.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaMemcpyAsync(pl->plane_cdf, cdf.data(), sizeof(float) * cdf.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaMemcpyAsync(pl->plane_pdf, pdf.data(), sizeof(float) * pdf.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaStreamSynchronize(stream))) {
+        pb2_pipeline_destroy(pl);
+        return cuda_fail(e, "pipeline upload");
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&pl->sms, cudaDevAttrMultiProcessorCount, dev);
+    *out = pl;
+    return PB2_OK;
+}
+
+int pb2_pipeline_destroy(pb2_pipeline* pl) {
+    if (!pl) return PB2_OK;
+    pb2_accel_destroy(pl->accel);
+    cudaFree(pl->materials);
+    cudaFree(pl->lights);
+    cudaFree(pl->plane_cdf);
+    cudaFree(pl->plane_pdf);
+    cudaFree(pl->state);
+    delete pl;
+    return PB2_OK;
+}
+
+int pb2_pipeline_get_rect(const pb2_pipeline* pl, pb2_rect* full, pb2_ndc_transform* ndc) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_get_rect: null pipeline");
+    if (full) *full = pl->full;
+    if (ndc) *ndc = pl->ndc;
+    return PB2_OK;
+}
+
+static LaunchParams make_params(const pb2_pipeline* pl, const pb2_rect& rect, uint32_t sb, uint32_t sc) {
+    LaunchParams lp{};
+    lp.rect = rect;
+    lp.full = pl->full;
+    lp.ndc = pl->ndc;
+    lp.width = pl->settings.width;
+    lp.height = pl->settings.height;
+    lp.log2res = pl->log2res;
+    lp.sample_begin = sb;
+    lp.sample_count = sc;
+    lp.max_depth = pl->settings.max_depth;
+    lp.min_rr_depth = pl->settings.min_rr_depth;
+    lp.filter = pl->settings.filter;
+    lp.gauss_neg_alpha = -pl->settings.gaussian_alpha;
+    lp.gauss_sub = pl->gauss_sub;
+    lp.cam = pl->settings.camera;
+    lp.num_lights = pl->num_lights;
+    for (int k = 0; k < 3; ++k) lp.env[k] = pl->env[k];
+    lp.path_count = rect.width * rect.height * sc;
+    return lp;
+}
+
+static bool rect_inside(const pb2_rect& r, const pb2_rect& full) {
+    return r.width && r.height && r.left >= full.left && r.top >= full.top &&
+           (uint64_t)r.left + r.width <= (uint64_t)full.left + full.width &&
+           (uint64_t)r.top + r.height <= (uint64_t)full.top + full.height;
+}
+
+int pb2_pipeline_camera_rays(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample, pb2_ray* rays, float* points,
+                             void* stream) {
+    if (!pl || !rect || !rays || !points) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_camera_rays: null");
+    if (!rect_inside(*rect, pl->full)) return fail(PB2_ERR_INVALID_ARGUMENT, "rect outside the render rectangle");
+    const LaunchParams lp = make_params(pl, *rect, sample, 1);
+    const uint32_t n = rect->width * rect->height;
+    k_camera_rays<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(lp, sample, reinterpret_cast<float4*>(rays),
+                                                                                   reinterpret_cast<float2*>(points));
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "k_camera_rays");
+}
+
+int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_begin, uint32_t sample_count,
+                        float* rgbw, float* sample_out, void* stream_ptr) {
+    if (!pl || !rect) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_launch: null argument");
+    if (!rect_inside(*rect, pl->full)) return fail(PB2_ERR_INVALID_ARGUMENT, "rect outside the render rectangle");
+    if (sample_count == 0) return PB2_OK;
+    if ((uint64_t)sample_begin + sample_count > (1ull << 31))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "sample range too large");
+    const uint64_t paths = (uint64_t)rect->width * rect->height * sample_count;
+    if (paths > 0x7FFFFFFFull) return fail(PB2_ERR_INVALID_ARGUMENT, "launch has more than 2^31 paths");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    int rc = alloc_paths(pl, (uint32_t)paths);
+    if (rc) return rc;
+    const LaunchParams lp = make_params(pl, *rect, sample_begin, sample_count);
+    SceneView sv;
+    sv.materials = pl->materials;
+    sv.prim_material = pl->accel->prim_material;
+    sv.lights = pl->lights;
+    sv.plane_cdf = pl->plane_cdf;
+    sv.plane_pdf = pl->plane_pdf;
+    sv.bvh = pl->accel->view;
+    Paths ps = pl->ps;
+    float4* film = reinterpret_cast<float4*>(rgbw);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream))) return cuda_fail(e, "memset counts");
+    const uint32_t pc = (uint32_t)paths;
+    if ((e = cudaMemcpyAsync(ps.counts + C_EXT_CUR, &pc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream)))
+        return cuda_fail(e, "set count");
+    k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps);
+    const int grid = pl->sms * 8;
+    uint32_t* work = pl->accel->work;
+    unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
+    unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
+    static int qblocks = 0;
+    if (!qblocks) {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND>, kQThreads, 0);
+        qblocks = pl->sms * (per > 0 ? per : 1);
+    }
+    uint32_t cur = 0;
+    const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
+    for (int bounce = 0;; ++bounce) {
+        uint32_t active = 0;
+        if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaStreamSynchronize(stream)))
+            return cuda_fail(e, "read queue size");
+        if (active == 0) break;
+        if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
+        const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
+        cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
+        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(sv.bvh, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
+                                                                 stats);
+        k_classify<<<grid, 256, 0, stream>>>(lp, sv, ps, cur, film, sample_out);
+        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
+                                                                   sstats);
+        k_trace_queue<Q_MIS><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats);
+        k_finish<<<grid, 256, 0, stream>>>(lp, sv, ps, cur, film, sample_out);
+        k_advance<<<1, 1, 0, stream>>>(ps.counts);
+        if ((e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
+        cur ^= 1u;
+    }
+    uint32_t counts[C_COUNT];
+    if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
+        (e = cudaStreamSynchronize(stream)))
+        return cuda_fail(e, "read stats");
+    unsigned long long v;
+    std::memcpy(&v, counts + C_STAT_CLOSEST, 8);
+    pl->stats.closest_rays += v;
+    std::memcpy(&v, counts + C_STAT_SHADOW, 8);
+    pl->stats.shadow_rays += v;
+    std::memcpy(&v, counts + C_STAT_VERTICES, 8);
+    pl->stats.path_vertices += v;
+    pl->stats.paths += paths;
+    if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+    return PB2_OK;
+}
+
+int pb2_film_resolve(const float* rgbw, uint32_t n, float* rgb, void* stream) {
+    if (n == 0) return PB2_OK;
+    if (!rgbw || !rgb) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_film_resolve: null argument");
+    k_resolve<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<const float4*>(rgbw), n, rgb);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "k_resolve");
+}
+
+int pb2_pipeline_get_stats(const pb2_pipeline* pl, pb2_launch_stats* stats, void*) {
+    if (!pl || !stats) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_get_stats: null argument");
+    *stats = pl->stats;
+    return PB2_OK;
+}
+
+}  // extern "C"

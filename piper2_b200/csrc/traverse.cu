@@ -1,0 +1,123 @@
+// traverse.cu -- persistent closest-hit / any-hit kernels over batches of rays.
+//
+// Each warp keeps 32 rays in flight.  When at least kRefill lanes have finished, the warp fetches
+// that many new rays with one atomic on the work counter and hands them to the idle lanes (warp-level
+// compaction of the active ray set, as in Aila and Laine, HPG 2009, "dynamic fetch").  Lanes run
+// kSteps node visits between refill checks.
+#include "pb2_internal.h"
+#include "traverse.cuh"
+
+namespace pb2 {
+
+constexpr int kTraceThreads = 128;
+constexpr int kRefill = 8;
+constexpr int kSteps = 8;
+
+struct ApiRays {
+    const float4* rays;
+    pb2_hit* hits;
+    uint32_t* occluded;
+    __device__ __forceinline__ void load(uint32_t i, float4& a, float4& b) const {
+        a = __ldg(rays + 2 * i);
+        b = __ldg(rays + 2 * i + 1);
+    }
+};
+
+template <bool kClosest, bool kCount>
+__global__ void __launch_bounds__(kTraceThreads) k_trace_api(BvhView bvh, ApiRays io, uint32_t n, uint32_t* work,
+                                                              unsigned long long* counters, uint32_t* error_flag) {
+    Traverser<kClosest, kCount> tr;
+    bool active = false;
+    uint32_t ray_index = 0;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint32_t nv = 0, nt = 0;
+    for (;;) {
+        const unsigned inactive = __ballot_sync(0xFFFFFFFFu, !active);
+        if (__popc(inactive) >= kRefill) {
+            const int leader = __ffs(inactive) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(work, (uint32_t)__popc(inactive));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (!active) {
+                const uint32_t idx = base + __popc(inactive & lt_mask);
+                if (idx < n) {
+                    float4 a, b;
+                    io.load(idx, a, b);
+                    tr.init(bvh, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w);
+                    ray_index = idx;
+                    active = true;
+                }
+            }
+            if (__ballot_sync(0xFFFFFFFFu, active) == 0u) break;
+        }
+        if (active) {
+            for (int it = 0; it < kSteps && !tr.done; ++it) tr.step(bvh);
+            if (tr.done) {
+                if (kCount) { nv += tr.node_visits; nt += tr.tri_tests; }
+                if (tr.overflow) atomicOr(error_flag, 1u);
+                if (kClosest) {
+                    bool front;
+                    tr.finish_planes(bvh, front);
+                    pb2_hit h;
+                    h.t = tr.tbest;
+                    h.prim = tr.best_prim;
+                    h.u = tr.bu;
+                    h.v = tr.bv;
+                    reinterpret_cast<float4*>(io.hits)[ray_index] =
+                        make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
+                } else {
+                    io.occluded[ray_index] = tr.best_prim != kInvalidPrim ? 1u : 0u;
+                }
+                active = false;
+            }
+        }
+    }
+    if (kCount) {
+        for (int o = 16; o > 0; o >>= 1) {
+            nv += __shfl_xor_sync(0xFFFFFFFFu, nv, o);
+            nt += __shfl_xor_sync(0xFFFFFFFFu, nt, o);
+        }
+        if (lane == 0) {
+            atomicAdd(counters + 0, (unsigned long long)nv);
+            atomicAdd(counters + 1, (unsigned long long)nt);
+        }
+    }
+}
+
+static int persistent_blocks(const void* kernel, int threads) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
+                             bool closest, bool count, uint32_t* work, unsigned long long* counters,
+                             uint32_t* error_flag, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    cudaError_t err = cudaMemsetAsync(work, 0, sizeof(uint32_t), stream);
+    if (err != cudaSuccess) return err;
+    ApiRays io{ reinterpret_cast<const float4*>(rays), hits, occluded };
+    const void* kernel;
+    if (closest) kernel = count ? (const void*)k_trace_api<true, true> : (const void*)k_trace_api<true, false>;
+    else kernel = count ? (const void*)k_trace_api<false, true> : (const void*)k_trace_api<false, false>;
+    static int blocks[4] = { 0, 0, 0, 0 };
+    const int slot = (closest ? 2 : 0) + (count ? 1 : 0);
+    if (!blocks[slot]) blocks[slot] = persistent_blocks(kernel, kTraceThreads);
+    int grid = blocks[slot];
+    const int needed = (int)((n + kTraceThreads - 1) / kTraceThreads);
+    if (grid > needed) grid = needed;
+    if (closest) {
+        if (count) k_trace_api<true, true><<<grid, kTraceThreads, 0, stream>>>(bvh, io, n, work, counters, error_flag);
+        else k_trace_api<true, false><<<grid, kTraceThreads, 0, stream>>>(bvh, io, n, work, counters, error_flag);
+    } else {
+        if (count) k_trace_api<false, true><<<grid, kTraceThreads, 0, stream>>>(bvh, io, n, work, counters, error_flag);
+        else k_trace_api<false, false><<<grid, kTraceThreads, 0, stream>>>(bvh, io, n, work, counters, error_flag);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pb2

@@ -1,0 +1,253 @@
+"""Seeded synthetic workloads: the scenes, ray sets and render settings of the benchmark configurations.
+
+No scene files are read: every configuration is generated from a seed with numpy's PCG64 generator,
+so the same seed gives the same float32 arrays on every machine.
+
+* :func:`cornell_box`        -- the small Cornell-box-style scene (10 + 24 triangles, 0.25 x 0.25
+  ceiling light of radiance (17, 12, 4), Lambertian white/red/green, pinhole 40 degree FOV, 256 x 256,
+  16 spp, max depth 8, NEE + MIS).
+* :func:`triangle_soup` / :func:`soup_rays` -- the traversal stress test: 1M triangles with centroids
+  uniform in [0,1]^3 and lognormal edge lengths (median 0.01, sigma 0.5); 4M closest-hit rays from
+  the bounding sphere towards uniform interior points, 4M any-hit rays of length U[0.1, 1].
+
+Rotations are baked into vertex positions and instance transforms are translation-only, because the
+reference inverts instance transforms with a routine that is only correct for translations
+(Src/Kernel/Transform.hpp:344-362).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+
+f32 = np.float32
+
+
+def plane_make(origin, u, v) -> capi.Plane:
+    """PerPlaneData from Origin/U/V exactly as the Plane geometry builds it
+    (Src/BuiltinComponent/Geometry/BasicShapes/BasicShapes.cpp:70-89), in float32."""
+    o = [f32(x) for x in origin]
+    u = [f32(x) for x in u]
+    v = [f32(x) for x in v]
+    det = [u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]]
+    area = np.sqrt(max(det[0] * det[0] + det[1] * det[1] + det[2] * det[2], f32(0)))
+    n = [d / area for d in det]
+    ul = np.sqrt(max(u[0] * u[0] + u[1] * u[1] + u[2] * u[2], f32(0)))
+    t = [x / ul for x in u]
+    a = [abs(d) for d in det]
+    if a[0] >= a[1] and a[0] >= a[2]:
+        sel = 0
+    else:
+        sel = 1 if (a[1] >= a[0] and a[1] >= a[2]) else 2
+    p = capi.Plane()
+    p.origin[:] = [float(x) for x in o]
+    p.u[:] = [float(x) for x in u]
+    p.v[:] = [float(x) for x in v]
+    p.normal[:] = [float(x) for x in n]
+    p.tangent[:] = [float(x) for x in t]
+    p.max_det_comp = sel
+    return p
+
+
+def camera_from_config(position, look_at, up, sensor_size_mm, focal_length_mm, fstop) -> capi.Camera:
+    """PerspectiveCamera config keys -> camera payload (PerspectiveCamera.cpp:39-44): sizes in mm
+    times 1e-3f, up normalised, aperture radius = focal / (2 FStop)."""
+    cam = capi.Camera()
+    cam.position[:] = [float(f32(x)) for x in position]
+    cam.look_at[:] = [float(f32(x)) for x in look_at]
+    upv = [f32(x) for x in up]
+    ul = np.sqrt(max(upv[0] * upv[0] + upv[1] * upv[1] + upv[2] * upv[2], f32(0)))
+    cam.up[:] = [float(x / ul) for x in upv]
+    cam.sensor_size[:] = [float(f32(sensor_size_mm[0]) * f32(1e-3)), float(f32(sensor_size_mm[1]) * f32(1e-3))]
+    focal = f32(focal_length_mm) * f32(1e-3)
+    cam.focal_length = float(focal)
+    cam.aperture_radius = float(focal / (f32(2.0) * f32(fstop)))
+    return cam
+
+
+@dataclass
+class MeshData:
+    vertices: np.ndarray  # (V, 3) float32
+    indices: np.ndarray   # (T, 3) uint32
+    material: int
+    translation: tuple = (0.0, 0.0, 0.0)
+
+
+@dataclass
+class SceneData:
+    meshes: list = field(default_factory=list)
+    planes: list = field(default_factory=list)        # capi.Plane
+    area_lights: list = field(default_factory=list)   # (radiance, first_plane, plane_count, translation)
+    materials: list = field(default_factory=list)     # capi.Material
+    env_radiance: tuple = (0.0, 0.0, 0.0)
+    settings: capi.RenderSettings | None = None
+    name: str = ""
+
+    @property
+    def triangle_count(self) -> int:
+        return int(sum(m.indices.shape[0] for m in self.meshes))
+
+    def to_ctypes(self):
+        """Returns (capi.Scene, keepalive) -- keep the second value alive while the struct is used."""
+        keep = []
+        meshes = (capi.Mesh * max(1, len(self.meshes)))()
+        for i, m in enumerate(self.meshes):
+            v = np.ascontiguousarray(m.vertices, dtype=np.float32)
+            ix = np.ascontiguousarray(m.indices, dtype=np.uint32)
+            keep += [v, ix]
+            meshes[i].vertices = v.ctypes.data
+            meshes[i].indices = ix.ctypes.data
+            meshes[i].texcoords = None
+            meshes[i].vert_count = v.shape[0]
+            meshes[i].tri_count = ix.shape[0]
+            meshes[i].material = m.material
+            meshes[i].translation[:] = [float(x) for x in m.translation]
+        planes = (capi.Plane * max(1, len(self.planes)))(*self.planes)
+        lights = (capi.AreaLight * max(1, len(self.area_lights)))()
+        for i, (rad, first, count, tr) in enumerate(self.area_lights):
+            lights[i].radiance[:] = [float(x) for x in rad]
+            lights[i].first_plane = first
+            lights[i].plane_count = count
+            lights[i].translation[:] = [float(x) for x in tr]
+        mats = (capi.Material * max(1, len(self.materials)))(*self.materials)
+        sc = capi.Scene()
+        sc.meshes = C.cast(meshes, C.POINTER(capi.Mesh))
+        sc.mesh_count = len(self.meshes)
+        sc.planes = C.cast(planes, C.POINTER(capi.Plane))
+        sc.plane_count = len(self.planes)
+        sc.area_lights = C.cast(lights, C.POINTER(capi.AreaLight))
+        sc.area_light_count = len(self.area_lights)
+        sc.materials = C.cast(mats, C.POINTER(capi.Material))
+        sc.material_count = len(self.materials)
+        sc.env_radiance[:] = [float(x) for x in self.env_radiance]
+        keep += [meshes, planes, lights, mats]
+        return sc, keep
+
+
+def material(kind: str, color0=(0, 0, 0, 0), color1=(0, 0, 0, 0), roughness=(0.0, 0.0)) -> capi.Material:
+    m = capi.Material()
+    m.type = capi.SURFACE[kind]
+    c0 = list(color0) + [0.0] * (4 - len(color0))
+    c1 = list(color1) + [0.0] * (4 - len(color1))
+    m.color0[:] = [float(x) for x in c0]
+    m.color1[:] = [float(x) for x in c1]
+    m.roughness[:] = [float(x) for x in roughness]
+    return m
+
+
+def _quad(p0, p1, p2, p3):
+    v = np.array([p0, p1, p2, p3], dtype=np.float64)
+    ix = np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32)
+    return v, ix
+
+
+def _box(center, size, angle):
+    """Axis-aligned box of `size` rotated about +Y by `angle` (radians), resting on y = center[1]."""
+    sx, sy, sz = size
+    corners = np.array([[x, y, z] for y in (0.0, sy) for z in (-sz / 2, sz / 2) for x in (-sx / 2, sx / 2)])
+    c, s = math.cos(angle), math.sin(angle)
+    rot = np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]])
+    v = corners @ rot.T + np.array(center)
+    # corner index = y*4 + z*2 + x
+    faces = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    ix = []
+    for a, b, cc, d in faces:
+        ix += [[a, b, cc], [a, cc, d]]
+    return v, np.array(ix, dtype=np.uint32)
+
+
+def render_settings(width, height, spp, max_depth, min_rr_depth, camera, filt="box", alpha=2.0,
+                    fit="Fill") -> capi.RenderSettings:
+    st = capi.RenderSettings()
+    st.width, st.height = width, height
+    st.fit_mode = capi.FIT[fit]
+    if spp & (spp - 1):
+        spp = 1 << int(math.ceil(math.log2(spp)))  # ScrambledSobolSampler.cpp:43-50
+    st.samples_per_pixel = spp
+    st.scramble = 0
+    st.max_depth = max_depth
+    st.min_rr_depth = min_rr_depth
+    st.filter = capi.FILTER[filt]
+    st.gaussian_alpha = alpha
+    st.camera = camera
+    return st
+
+
+def cornell_box(seed: int = 0, width: int = 256, height: int = 256, spp: int = 16, max_depth: int = 8,
+                min_rr_depth: int = 3) -> SceneData:
+    rng = np.random.default_rng(seed)
+    a1, a2 = np.deg2rad(rng.uniform(-30.0, 30.0, size=2))
+    white, red, green = 0, 1, 2
+    sd = SceneData(name=f"cornell_box(seed={seed})")
+    sd.materials = [material("Matte", (0.73, 0.73, 0.73, 1.0)),
+                    material("Matte", (0.65, 0.05, 0.05, 1.0)),
+                    material("Matte", (0.12, 0.45, 0.15, 1.0))]
+    room = [
+        (_quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)), white),   # floor
+        (_quad((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0)), white),   # ceiling
+        (_quad((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)), white),   # back wall
+        (_quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1)), red),     # x = 1 wall (left in the image)
+        (_quad((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0)), green),   # x = 0 wall (right in the image)
+    ]
+    for (v, ix), mat in room:
+        sd.meshes.append(MeshData(v.astype(np.float32), ix, mat))
+    for center, size, ang in (((0.68, 0.0, 0.35), (0.28, 0.28, 0.28), a1),
+                              ((0.33, 0.0, 0.65), (0.28, 0.56, 0.28), a2)):
+        v, ix = _box(center, size, ang)
+        sd.meshes.append(MeshData(v.astype(np.float32), ix, white))
+    sd.planes = [plane_make((0.375, 0.999, 0.375), (0.25, 0.0, 0.0), (0.0, 0.0, 0.25))]
+    sd.area_lights = [((17.0, 12.0, 4.0), 0, 1, (0.0, 0.0, 0.0))]
+    sd.env_radiance = (0.0, 0.0, 0.0)  # the pipeline requires one infinite light (Embree.cpp:1185-1188)
+    focal_mm = 35.0
+    sensor_mm = 2.0 * focal_mm * math.tan(math.radians(20.0))  # 40 degree field of view
+    cam = camera_from_config((0.5, 0.5, -1.4), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), (sensor_mm, sensor_mm), focal_mm,
+                             1e30)
+    sd.settings = render_settings(width, height, spp, max_depth, min_rr_depth, cam)
+    return sd
+
+
+def triangle_soup(n_tris: int = 1 << 20, seed: int = 0) -> SceneData:
+    """Traversal stress scene: centroids U[0,1]^3, vertices at lognormal distance (median 0.01,
+    sigma 0.5) from the centroid along random unit directions."""
+    rng = np.random.default_rng(seed)
+    cen = rng.random((n_tris, 1, 3))
+    scale = np.exp(rng.normal(math.log(0.01), 0.5, size=(n_tris, 1, 1)))
+    d = rng.normal(size=(n_tris, 3, 3))
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    v = (cen + scale * d).reshape(-1, 3).astype(np.float32)
+    ix = np.arange(3 * n_tris, dtype=np.uint32).reshape(n_tris, 3)
+    sd = SceneData(name=f"triangle_soup(n={n_tris}, seed={seed})")
+    sd.materials = [material("Matte", (0.5, 0.5, 0.5, 1.0))]
+    sd.meshes = [MeshData(v, ix, 0)]
+    return sd
+
+
+def soup_rays(n_rays: int = 1 << 22, seed: int = 1, kind: str = "closest") -> np.ndarray:
+    """Ray sets of the traversal stress test, as a RAY_DTYPE array.
+
+    closest: origin uniform on the sphere around [0,1]^3 (centre 0.5, radius sqrt(3)/2 + 0.01), direction
+    towards a uniform point of [0,1]^3, t in (0, 1e30).  any: origin uniform in [0,1]^3, uniform
+    direction, t in (0, U[0.1, 1])."""
+    rng = np.random.default_rng(seed)
+    rays = np.zeros(n_rays, dtype=capi.RAY_DTYPE)
+    if kind == "closest":
+        s = rng.normal(size=(n_rays, 3))
+        s /= np.linalg.norm(s, axis=1, keepdims=True)
+        org = 0.5 + (math.sqrt(3.0) / 2 + 0.01) * s
+        tgt = rng.random((n_rays, 3))
+        d = tgt - org
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        rays["tmax"] = 1e30
+    else:
+        org = rng.random((n_rays, 3))
+        d = rng.normal(size=(n_rays, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        rays["tmax"] = rng.uniform(0.1, 1.0, size=n_rays)
+    rays["org"] = org
+    rays["dir"] = d
+    rays["tmin"] = 0.0
+    return rays
