@@ -1,0 +1,343 @@
+"""Benchmark of the traversal stress test (1M triangles; 4M closest-hit + 4M any-hit rays).
+
+A step is one pass of the hot path over one batch: a closest-hit trace of 4M rays and an any-hit trace of
+4M shadow rays against the 8-wide BVH of a 1M-triangle soup (centroids U[0,1]^3, lognormal edges with
+median 0.01 and sigma 0.5; closest-hit rays from the bounding sphere to uniform interior points;
+any-hit rays of length U[0.1, 1]).  Synthetic, seeded data of the configuration's shapes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value   : Mrays/s over both ray sets, inputs resident in HBM, device time (CUDA events) of the K steps,
+          L2 flushed (256 MiB write) before every step; for N > 1 every rank traces its own batch
+          (weak scaling) and the time is the max over ranks.
+e2e     : the same through the host-buffer C-ABI calls (pinned host rays in, hits out, copies timed).
+roofline: the closest-hit kernel's algorithmic bytes per launch (32 B ray + 16 B hit + 80 B per node
+          visit + 36 B per triangle test, visits and tests counted by the counting build of the same
+          traversal on the same BVH) / its CUDA-event duration, against the measured HBM copy peak.
+--impl reference: the CPU port of the path (binned-SAH BVH + the same watertight test; Embree itself is
+          not available here) on all host cores, on a bounded sample of the same ray sets.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N_TRIS = 1 << 20
+N_RAYS = 1 << 22
+METRIC = "Mrays/s (closest-hit + any-hit) on the traversal stress test; reference: CPU tracer on host cores"
+CONFIG = {"workload": "traversal stress test: 1M-triangle soup, 4M closest-hit + 4M any-hit rays",
+          "triangles": N_TRIS, "closest_rays": N_RAYS, "anyhit_rays": N_RAYS, "seed": 0,
+          "l2": "flushed (256 MiB write) before every step"}
+BYTES_RAY, BYTES_HIT, BYTES_NODE, BYTES_TRI = 32, 16, 80, 36
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """DRAM bytes per closest-hit launch from the committed ncu summary (None if absent)."""
+    path = os.path.join(ROOT, "profiles", "trace_closest_soup1M.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from piper2_b200 import api, capi, scenes
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    soup = scenes.triangle_soup(N_TRIS, seed=0)
+    crays = scenes.soup_rays(N_RAYS, seed=1 + 2 * rank, kind="closest")
+    arays = scenes.soup_rays(N_RAYS, seed=2 + 2 * rank, kind="any")
+    acc = api.Accel(soup)
+    info = acc.info()
+    stream = torch.cuda.current_stream()
+    d_c = torch.from_numpy(crays.view(np.float32).reshape(-1, 8)).to(dev)
+    d_a = torch.from_numpy(arays.view(np.float32).reshape(-1, 8)).to(dev)
+    d_hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device=dev)
+    d_occ = torch.empty(N_RAYS, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    # work counters of this traversal on this BVH (for the byte model), outside the timed region
+    acc.set_counting(True)
+    acc.trace_closest_dev(d_c.data_ptr(), N_RAYS, d_hits.data_ptr())
+    nv_c, nt_c = acc.counters()
+    acc.trace_any_dev(d_a.data_ptr(), N_RAYS, d_occ.data_ptr())
+    nv_a, nt_a = acc.counters()
+    acc.set_counting(False)
+
+    def step(ev):
+        flush.zero_()
+        ev[0].record(stream)
+        acc.trace_closest_dev(d_c.data_ptr(), N_RAYS, d_hits.data_ptr())
+        ev[1].record(stream)
+        acc.trace_any_dev(d_a.data_ptr(), N_RAYS, d_occ.data_ptr())
+        ev[2].record(stream)
+
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(3)]  # noqa: E731
+    for _ in range(args.warmup):
+        step(mk())
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [mk() for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for e in evs:
+            step(e)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_closest = [e[0].elapsed_time(e[1]) for e in evs]
+    t_any = [e[1].elapsed_time(e[2]) for e in evs]
+    step_ms = [a + b for a, b in zip(t_closest, t_any)]
+    total_ms = sum(step_ms)
+
+    # end to end: host buffers through the C ABI (copies in the timed region)
+    h_c = torch.from_numpy(crays.view(np.uint8)).pin_memory()
+    h_a = torch.from_numpy(arays.view(np.uint8)).pin_memory()
+    h_hits = torch.empty(N_RAYS * 16, dtype=torch.uint8).pin_memory()
+    h_occ = torch.empty(N_RAYS * 4, dtype=torch.uint8).pin_memory()
+    lib = capi.lib()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def e2e_step():
+        capi.check(lib.pb2_trace_closest_host(acc.h, C.c_void_p(h_c.data_ptr()), N_RAYS, C.c_void_p(h_hits.data_ptr()), sp))
+        capi.check(lib.pb2_trace_any_host(acc.h, C.c_void_p(h_a.data_ptr()), N_RAYS, C.c_void_p(h_occ.data_ptr()), sp))
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+
+    res = torch.tensor([total_ms, sum(e2e_ms), sum(t_closest)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(res, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    total_ms, e2e_total, closest_total = res.tolist()
+    if rank != 0:
+        return
+    rays_all = 2 * N_RAYS * args.steps * world
+    value = rays_all / (total_ms * 1e-3) / 1e6
+    e2e_value = rays_all / (e2e_total * 1e-3) / 1e6
+    # roofline of the closest-hit kernel
+    bytes_per_launch = N_RAYS * (BYTES_RAY + BYTES_HIT) + BYTES_NODE * nv_c + BYTES_TRI * nt_c
+    avg_closest_s = (sum(t_closest) / len(t_closest)) * 1e-3
+    achieved = bytes_per_launch / avg_closest_s / 1e9
+    peak, peak_kind = _peaks()
+    traffic = _profile_traffic()
+    cpu = cpu_baseline(soup, crays, arays, args) if world == 1 else None
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator of the configuration's shapes)",
+        "config": dict(CONFIG, parallelism=f"replicas x{world} (independent ray batches)"),
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 2 * N_RAYS * 32,
+                "d2h_bytes_per_step": N_RAYS * 16 + N_RAYS * 4},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "k_trace_api<closest>",
+                     "bytes_model": {"per_ray": BYTES_RAY + BYTES_HIT, "per_node_visit": BYTES_NODE,
+                                     "per_triangle_test": BYTES_TRI,
+                                     "node_visits_per_ray": round(nv_c / N_RAYS, 3),
+                                     "triangle_tests_per_ray": round(nt_c / N_RAYS, 3)}},
+        "cpu_baseline": cpu,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "detail": {"closest_mrays_s": round(N_RAYS / (sum(t_closest) / args.steps * 1e-3) / 1e6, 2),
+                   "anyhit_mrays_s": round(N_RAYS / (sum(t_any) / args.steps * 1e-3) / 1e6, 2),
+                   "anyhit_node_visits_per_ray": round(nv_a / N_RAYS, 3),
+                   "anyhit_triangle_tests_per_ray": round(nt_a / N_RAYS, 3),
+                   "bvh_nodes": info.node_count, "bvh_build_ms": round(info.build_ms, 3)},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline(soup, crays, arays, args, sample=None):
+    """The CPU port (binned-SAH BVH + watertight test) on all host threads, bounded sample."""
+    import oracle_py
+
+    threads = os.cpu_count() or 1
+    osc = oracle_py.OracleScene(soup, use_bvh=True)
+    n = sample or int(os.environ.get("PB2_CPU_SAMPLE", 1 << 17))
+    t0 = time.perf_counter()
+    osc.trace_closest(crays[:n], threads=threads)
+    osc.trace_any(arays[:n], threads=threads)
+    dt = time.perf_counter() - t0
+    osc.close()
+    return {"value": round(2 * n / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"{n} closest-hit + {n} any-hit rays of the same sets (1M-triangle BVH built beforehand)"}
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    import oracle_py  # noqa: F401
+
+    from piper2_b200 import scenes
+
+    soup = scenes.triangle_soup(N_TRIS, seed=0)
+    crays = scenes.soup_rays(N_RAYS, seed=1, kind="closest")
+    arays = scenes.soup_rays(N_RAYS, seed=2, kind="any")
+    import oracle_py as op
+
+    threads = os.cpu_count() or 1
+    osc = op.OracleScene(soup, use_bvh=True)
+    n = int(os.environ.get("PB2_CPU_SAMPLE", 1 << 16))
+    for i in range(args.warmup):
+        osc.trace_closest(crays[:n // 4], threads=threads)
+    times = []
+    for i in range(args.steps):
+        lo = (i * n) % (N_RAYS - n)
+        t0 = time.perf_counter()
+        osc.trace_closest(crays[lo:lo + n], threads=threads)
+        osc.trace_any(arays[lo:lo + n], threads=threads)
+        times.append(time.perf_counter() - t0)
+    value = 2 * n * args.steps / sum(times) / 1e6
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * sum(times) / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator of the configuration's shapes)",
+        "config": dict(CONFIG, parallelism="host threads"),
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} closest-hit + {n} any-hit rays per step (Embree 3.12.1 is not installed; "
+                                   "the reference's Embree tracer is replaced by its CPU restatement)"},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

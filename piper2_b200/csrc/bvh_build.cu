@@ -352,22 +352,51 @@ size_t cub_bytes(uint32_t n) {
 
 }  // namespace
 
-size_t build_scratch_bytes(uint32_t n) {
+struct ScratchLayout {
+    float4 *lo, *hi, *slo, *shi, *ilo, *ihi;
+    uint64_t *keys, *keys2;
+    uint32_t *vals, *vals2;
+    Internal* nodes;
+    int *iparent, *lparent;
+    uint32_t* flags;
+    Frontier *fa, *fb;
+    int* cbounds;
+    uint32_t* counters;
+    void* cub_tmp;
+    size_t cub_bytes;
+    size_t total;
+};
+
+// Carves the scratch buffer (base may be null to only measure it).
+static ScratchLayout layout(char* base, uint32_t n) {
     const size_t m = n ? n : 1;
-    size_t b = 0;
-    auto add = [&](size_t bytes) { b += ((bytes + 255) / 256) * 256; };
-    add(sizeof(float4) * m * 4);      // lo, hi, slo, shi
-    add(sizeof(float4) * m * 2);      // ilo, ihi
-    add(sizeof(uint64_t) * m * 2);    // keys
-    add(sizeof(uint32_t) * m * 2);    // vals
-    add(sizeof(Internal) * m);
-    add(sizeof(int) * m * 2);         // parents
-    add(sizeof(uint32_t) * m);        // flags
-    add(sizeof(Frontier) * m * 2);    // frontiers
-    add(sizeof(int) * 8 + sizeof(uint32_t) * 8);
-    add(cub_bytes((uint32_t)m));
-    return b;
+    ScratchLayout L;
+    char* p = base;
+    L.lo = carve<float4>(p, m);
+    L.hi = carve<float4>(p, m);
+    L.slo = carve<float4>(p, m);
+    L.shi = carve<float4>(p, m);
+    L.ilo = carve<float4>(p, m);
+    L.ihi = carve<float4>(p, m);
+    L.keys = carve<uint64_t>(p, m);
+    L.keys2 = carve<uint64_t>(p, m);
+    L.vals = carve<uint32_t>(p, m);
+    L.vals2 = carve<uint32_t>(p, m);
+    L.nodes = carve<Internal>(p, m);
+    L.iparent = carve<int>(p, m);
+    L.lparent = carve<int>(p, m);
+    L.flags = carve<uint32_t>(p, m);
+    L.fa = carve<Frontier>(p, m);
+    L.fb = carve<Frontier>(p, m);
+    L.cbounds = carve<int>(p, 8);
+    L.counters = carve<uint32_t>(p, 8);
+    L.cub_bytes = cub_bytes((uint32_t)m);
+    L.cub_tmp = carve<char>(p, L.cub_bytes);
+    L.total = (size_t)(p - base);
+    return L;
 }
+
+size_t build_scratch_bytes(uint32_t n) { return layout(nullptr, n).total; }
 
 cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* wnodes, TriSlot* tris_out, void* scratch,
                            size_t scratch_bytes, cudaStream_t stream, BuildResult* result) {
@@ -377,29 +406,19 @@ cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* wnodes,
     cudaEventCreate(&e1);
     cudaEventRecord(e0, stream);
     const size_t m = n ? n : 1;
-    char* p = static_cast<char*>(scratch);
-    float4* lo = carve<float4>(p, m);
-    float4* hi = carve<float4>(p, m);
-    float4* slo = carve<float4>(p, m);
-    float4* shi = carve<float4>(p, m);
-    float4* ilo = carve<float4>(p, m);
-    float4* ihi = carve<float4>(p, m);
-    uint64_t* keys = carve<uint64_t>(p, m);
-    uint64_t* keys2 = carve<uint64_t>(p, m);
-    uint32_t* vals = carve<uint32_t>(p, m);
-    uint32_t* vals2 = carve<uint32_t>(p, m);
-    Internal* nodes = carve<Internal>(p, m);
-    int* iparent = carve<int>(p, m);
-    int* lparent = carve<int>(p, m);
-    uint32_t* flags = carve<uint32_t>(p, m);
-    Frontier* fa = carve<Frontier>(p, m);
-    Frontier* fb = carve<Frontier>(p, m);
-    int* cbounds = carve<int>(p, 8);
-    uint32_t* counters = carve<uint32_t>(p, 8);
-    const size_t cb = cub_bytes((uint32_t)m);
-    void* cub_tmp = carve<char>(p, cb);
-    if ((size_t)(p - static_cast<char*>(scratch)) > scratch_bytes) return cudaErrorInvalidValue;
-
+    const ScratchLayout L = layout(static_cast<char*>(scratch), n);
+    if (L.total > scratch_bytes) return cudaErrorInvalidValue;
+    float4 *lo = L.lo, *hi = L.hi, *slo = L.slo, *shi = L.shi, *ilo = L.ilo, *ihi = L.ihi;
+    uint64_t *keys = L.keys, *keys2 = L.keys2;
+    uint32_t *vals = L.vals, *vals2 = L.vals2;
+    Internal* nodes = L.nodes;
+    int *iparent = L.iparent, *lparent = L.lparent;
+    uint32_t* flags = L.flags;
+    Frontier *fa = L.fa, *fb = L.fb;
+    int* cbounds = L.cbounds;
+    uint32_t* counters = L.counters;
+    void* cub_tmp = L.cub_tmp;
+    const size_t cb = L.cub_bytes;
     uint32_t node_count = 0;
     if (n == 0) {
         result->node_count = 0;

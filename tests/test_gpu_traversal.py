@@ -126,7 +126,7 @@ def test_planes_and_cornell(oracle):
     with _api().Accel(sd) as acc:
         h = acc.trace_closest(rays)
         _assert_hits_equal(h, o.trace_closest(rays))
-        assert np.any(h["prim"] & capi.PB2_PLANE_FLAG & (h["prim"] != capi.PB2_INVALID_PRIM))
+        assert np.any(((h["prim"] & capi.PB2_PLANE_FLAG) != 0) & (h["prim"] != capi.PB2_INVALID_PRIM))
         assert np.array_equal(acc.trace_any(rays), o.trace_any(rays))
 
 
