@@ -7,8 +7,9 @@
 //      BVHs, Octrees, and k-d Trees", HPG 2012), equal codes ordered by index,
 //   5. bottom-up box refit (the second child to arrive at a node computes its box),
 //   6. top-down collapse into 8-wide nodes, one frontier level per launch: each wide node greedily
-//      opens its largest-area binary descendant until it has 8 children; subtrees of at most 3
-//      triangles become leaves; child boxes are quantised to 8 bits relative to the node box
+//      opens its largest-area binary descendant with more than 3 triangles until it has 8 children,
+//      then, while slots remain, the largest smaller subtrees; subtrees of at most 3 triangles become
+//      leaves; child boxes are quantised to 8 bits relative to the node box
 //      (rounded outward) and children are placed in the slot of the ray octant they are nearest
 //      for (greedy assignment on the projected centroid offsets).
 #include <cub/device/device_radix_sort.cuh>
@@ -228,6 +229,16 @@ __global__ void k_collapse(const Frontier* __restrict__ in, uint32_t count, Fron
                 const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
                 const float area = dx * dy + dy * dz + dz * dx;
                 if (area > best_area) { best_area = area; best = k; }
+            }
+            if (best < 0) {
+                // room left: also open small subtrees (tighter leaves, fewer triangle tests)
+                for (int k = 0; k < nch; ++k) {
+                    if (is_leaf(ch[k])) continue;
+                    const float4 l = ilo[ch[k]], h = ihi[ch[k]];
+                    const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+                    const float area = dx * dy + dy * dz + dz * dx;
+                    if (area > best_area) { best_area = area; best = k; }
+                }
             }
             if (best < 0) break;
             const Internal c = nodes[ch[best]];

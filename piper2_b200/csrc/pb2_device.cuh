@@ -5,9 +5,9 @@
 
 #include "pb2_math.h"
 
-// Non-contracted IEEE operations.  The traversal translation unit is compiled with FMA contraction
-// enabled for the box tests, so every operation whose rounding must match the CPU oracle bit for
-// bit (the watertight triangle test) is spelled with the _rn intrinsics, which nvcc never fuses.
+// Non-contracted IEEE operations.  The library is built with -fmad=false, and the operations whose
+// rounding must match the CPU oracle bit for bit (the watertight triangle test, the plane test) are in
+// addition spelled with the _rn intrinsics, which nvcc never fuses whatever the flags.
 #define RN_MUL(a, b) __fmul_rn((a), (b))
 #define RN_ADD(a, b) __fadd_rn((a), (b))
 #define RN_SUB(a, b) __fsub_rn((a), (b))
@@ -51,6 +51,15 @@ __device__ __forceinline__ void ray_prepare(float ox, float oy, float oz, float 
     p.sz = RN_DIV(1.0f, dkz);
 }
 
+// The paper's double-precision recomputation of U, V, W when one of them is exactly zero (an edge or
+// vertex hit).  Rare, so kept out of line to keep the hot loop small.
+static __device__ __noinline__ void edge_fallback(float Ax, float Ay, float Bx, float By, float Cx, float Cy, float& U,
+                                                  float& V, float& W) {
+    U = __double2float_rn(__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx)));
+    V = __double2float_rn(__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx)));
+    W = __double2float_rn(__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax)));
+}
+
 // Watertight ray/triangle test, identical operation for operation to the CPU oracle.  Returns true
 // and writes t, (u, v) = weights of v1, v2 for a hit with tmin < t < tmax.
 __device__ __forceinline__ bool tri_test(const RayPre& p, float4 a4, float4 b4, float4 c4, float& t_out, float& u_out,
@@ -68,11 +77,7 @@ __device__ __forceinline__ bool tri_test(const RayPre& p, float4 a4, float4 b4, 
     float U = RN_SUB(RN_MUL(Cx, By), RN_MUL(Cy, Bx));
     float V = RN_SUB(RN_MUL(Ax, Cy), RN_MUL(Ay, Cx));
     float W = RN_SUB(RN_MUL(Bx, Ay), RN_MUL(By, Ax));
-    if (U == 0.0f || V == 0.0f || W == 0.0f) {
-        U = __double2float_rn(__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx)));
-        V = __double2float_rn(__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx)));
-        W = __double2float_rn(__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax)));
-    }
+    if (U == 0.0f || V == 0.0f || W == 0.0f) edge_fallback(Ax, Ay, Bx, By, Cx, Cy, U, V, W);
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
     const float det = RN_ADD(RN_ADD(U, V), W);
     if (det == 0.0f) return false;

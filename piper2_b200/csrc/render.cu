@@ -241,18 +241,20 @@ __global__ void k_generate(LaunchParams lp, Paths ps) {
 // ---- traversal over queues -----------------------------------------------------------------------
 
 constexpr int kQThreads = 128;
-constexpr int kQRefill = 8;
-constexpr int kQSteps = 8;
+constexpr int kQRefill = 4;
+constexpr int kQSteps = 4;
 
 enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
 
 template <int kKind>
-__global__ void __launch_bounds__(kQThreads) k_trace_queue(BvhView bvh, Paths ps, const uint32_t* __restrict__ queue,
+__global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(BvhView bvh, Paths ps, const uint32_t* __restrict__ queue,
                                                            const uint32_t* __restrict__ count_ptr, uint32_t* work,
                                                            unsigned long long* stat) {
     constexpr bool kClosest = kKind != Q_SHADOW;
     const uint32_t n = *count_ptr;
-    Traverser<kClosest, false> tr;
+    __shared__ uint2 stack_smem[kSharedStack * kQThreads];
+    Traverser<kClosest, false, kQThreads> tr;
+    tr.bind_stack(stack_smem);
     bool active = false;
     uint32_t slot = 0;
     const unsigned lane = threadIdx.x & 31u;
@@ -287,7 +289,8 @@ __global__ void __launch_bounds__(kQThreads) k_trace_queue(BvhView bvh, Paths ps
             if (__ballot_sync(0xFFFFFFFFu, active) == 0u) break;
         }
         if (active) {
-            for (int it = 0; it < kQSteps && !tr.done; ++it) tr.step(bvh);
+#pragma unroll 1
+            for (int it = 0; it < kQSteps && !tr.done; ++it) tr.iteration(bvh);
             if (tr.done) {
                 if (kClosest) {
                     bool front;

@@ -3,15 +3,16 @@
 // Each warp keeps 32 rays in flight.  When at least kRefill lanes have finished, the warp fetches
 // that many new rays with one atomic on the work counter and hands them to the idle lanes (warp-level
 // compaction of the active ray set, as in Aila and Laine, HPG 2009, "dynamic fetch").  Lanes run
-// kSteps node visits between refill checks.
+// kSteps traversal iterations between refill checks (kSteps and kRefill were tuned on a B200).
 #include "pb2_internal.h"
 #include "traverse.cuh"
 
 namespace pb2 {
 
 constexpr int kTraceThreads = 128;
-constexpr int kRefill = 8;
-constexpr int kSteps = 8;
+constexpr int kRefill = 4;
+constexpr int kSteps = 4;
+constexpr int kMinBlocks = 10;
 
 struct ApiRays {
     const float4* rays;
@@ -24,9 +25,11 @@ struct ApiRays {
 };
 
 template <bool kClosest, bool kCount>
-__global__ void __launch_bounds__(kTraceThreads) k_trace_api(BvhView bvh, ApiRays io, uint32_t n, uint32_t* work,
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_trace_api(BvhView bvh, ApiRays io, uint32_t n, uint32_t* work,
                                                               unsigned long long* counters, uint32_t* error_flag) {
-    Traverser<kClosest, kCount> tr;
+    __shared__ uint2 stack_smem[kSharedStack * kTraceThreads];
+    Traverser<kClosest, kCount, kTraceThreads> tr;
+    tr.bind_stack(stack_smem);
     bool active = false;
     uint32_t ray_index = 0;
     const unsigned lane = threadIdx.x & 31u;
@@ -52,7 +55,9 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_api(BvhView bvh, ApiRay
             if (__ballot_sync(0xFFFFFFFFu, active) == 0u) break;
         }
         if (active) {
-            for (int it = 0; it < kSteps && !tr.done; ++it) tr.step(bvh);
+            // not unrolled: copies of the traversal body would overflow the instruction cache
+#pragma unroll 1
+            for (int it = 0; it < kSteps && !tr.done; ++it) tr.iteration(bvh);
             if (tr.done) {
                 if (kCount) { nv += tr.node_visits; nt += tr.tri_tests; }
                 if (tr.overflow) atomicOr(error_flag, 1u);

@@ -24,11 +24,6 @@ struct TraceResult {
     uint32_t prim;
 };
 
-__device__ __forceinline__ float byte_to_float(uint32_t word, int shift) {
-    // exact float of an 8-bit value: mantissa trick (2^23 + b) - 2^23
-    return __uint_as_float(0x4B000000u | ((word >> shift) & 0xFFu)) - 8388608.0f;
-}
-
 __device__ __forceinline__ float safe_rcp(float d) {
     const float a = fmaxf(fabsf(d), 1e-18f);
     return copysignf(__frcp_rn(a), d);
@@ -71,30 +66,28 @@ __device__ __forceinline__ uint32_t intersect_children(const WideNode* __restric
     const uint32_t fy_lo = iy >= 0.0f ? w4.x : w2.z, fy_hi = iy >= 0.0f ? w4.y : w2.w;
     const uint32_t nz_lo = iz >= 0.0f ? w3.x : w4.z, nz_hi = iz >= 0.0f ? w3.y : w4.w;
     const uint32_t fz_lo = iz >= 0.0f ? w4.z : w3.x, fz_hi = iz >= 0.0f ? w4.w : w3.y;
+    // One child per iteration, not unrolled: the loop body stays small in the instruction cache,
+    // which measured faster than the unrolled form for incoherent rays.
     uint32_t hitmask = 0;
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        const uint32_t meta4 = half ? w1.w : w1.z;
-        const uint32_t nxw = half ? nx_hi : nx_lo, fxw = half ? fx_hi : fx_lo;
-        const uint32_t nyw = half ? ny_hi : ny_lo, fyw = half ? fy_hi : fy_lo;
-        const uint32_t nzw = half ? nz_hi : nz_lo, fzw = half ? fz_hi : fz_lo;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int sh = 8 * j;
-            const uint32_t meta = (meta4 >> sh) & 0xFFu;
-            const float tnx = __fmaf_rn(byte_to_float(nxw, sh), ax, bnx);
-            const float tfx = __fmaf_rn(byte_to_float(fxw, sh), ax, bfx);
-            const float tny = __fmaf_rn(byte_to_float(nyw, sh), ay, bny);
-            const float tfy = __fmaf_rn(byte_to_float(fyw, sh), ay, bfy);
-            const float tnz = __fmaf_rn(byte_to_float(nzw, sh), az, bnz);
-            const float tfz = __fmaf_rn(byte_to_float(fzw, sh), az, bfz);
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, p.tmin));
-            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest));
-            if (meta != 0u && tn <= tf) {
-                const uint32_t inner = ((meta & (meta << 1)) & 0x10u) != 0u;
-                const uint32_t bit_index = inner ? ((meta & 0x1Fu) ^ oct_inv) : (meta & 0x1Fu);
-                hitmask |= (meta >> 5) << bit_index;
-            }
+#pragma unroll 1
+    for (int j = 0; j < 8; ++j) {
+        const bool hi = j >= 4;
+        const uint32_t sel = 0x7540u | (uint32_t)(j & 3);
+        const uint32_t meta = ((hi ? w1.w : w1.z) >> (8 * (j & 3))) & 0xFFu;
+        const float qnx = __uint_as_float(__byte_perm(hi ? nx_hi : nx_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float qfx = __uint_as_float(__byte_perm(hi ? fx_hi : fx_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float qny = __uint_as_float(__byte_perm(hi ? ny_hi : ny_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float qfy = __uint_as_float(__byte_perm(hi ? fy_hi : fy_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float qnz = __uint_as_float(__byte_perm(hi ? nz_hi : nz_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float qfz = __uint_as_float(__byte_perm(hi ? fz_hi : fz_lo, 0x4B000000u, sel)) - 8388608.0f;
+        const float tn = fmaxf(fmaxf(__fmaf_rn(qnx, ax, bnx), __fmaf_rn(qny, ay, bny)),
+                               fmaxf(__fmaf_rn(qnz, az, bnz), p.tmin));
+        const float tf = fminf(fminf(__fmaf_rn(qfx, ax, bfx), __fmaf_rn(qfy, ay, bfy)),
+                               fminf(__fmaf_rn(qfz, az, bfz), tbest));
+        if (meta != 0u && tn <= tf) {
+            const uint32_t inner = ((meta & (meta << 1)) & 0x10u) != 0u;
+            const uint32_t bit_index = inner ? ((meta & 0x1Fu) ^ oct_inv) : (meta & 0x1Fu);
+            hitmask |= (meta >> 5) << bit_index;
         }
     }
     return hitmask;
@@ -139,8 +132,14 @@ __device__ __forceinline__ bool plane_test(const DevPlane& pl, const RayPre& p, 
     return true;
 }
 
-// Per-lane traversal state.  `closest` selects closest-hit vs any-hit semantics.
-template <bool kClosest, bool kCount>
+// Traversal stack: the top kSharedStack entries live in shared memory, transposed so that consecutive
+// lanes touch consecutive words ([depth][thread]); deeper entries spill to a small local array.
+constexpr int kSharedStack = 12;
+constexpr int kLocalStack = 36;
+static_assert(kSharedStack + kLocalStack == kStackSize, "stack depth");
+
+// Per-lane traversal state.  kClosest selects closest-hit vs any-hit semantics.
+template <bool kClosest, bool kCount, int kThreads>
 struct Traverser {
     RayPre p;
     float ix, iy, iz;
@@ -149,11 +148,26 @@ struct Traverser {
     uint32_t best_prim;
     uint32_t best_slot;
     uint2 group;
-    uint2 stack[kStackSize];
+    uint2 tgroup;
+    uint2* sstack;  // this lane's column of the shared stack
+    uint2 lstack[kLocalStack];
     int sp;
     bool done;
     bool overflow;
     uint32_t node_visits, tri_tests;
+
+    __device__ __forceinline__ void bind_stack(uint2* shared_base) { sstack = shared_base + threadIdx.x; }
+
+    __device__ __forceinline__ void push(uint2 g) {
+        if (sp < kSharedStack) sstack[sp * kThreads] = g;
+        else if (sp < kStackSize) lstack[sp - kSharedStack] = g;
+        else { overflow = true; return; }
+        ++sp;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        --sp;
+        return sp < kSharedStack ? sstack[sp * kThreads] : lstack[sp - kSharedStack];
+    }
 
     __device__ __forceinline__ void init(const BvhView& bvh, float ox, float oy, float oz, float tmin, float dx,
                                          float dy, float dz, float tmax) {
@@ -170,12 +184,13 @@ struct Traverser {
         sp = 0;
         overflow = false;
         node_visits = tri_tests = 0;
+        tgroup = make_uint2(0, 0);
         if (bvh.tri_count == 0) {
             group = make_uint2(0, 0);
             done = true;
         } else {
-            // root: one internal "child" at slot 0
-            group = make_uint2(0u, (1u << (24u + (0u ^ oct_inv))) | 1u);
+            // the root as the only internal "child", in slot 0
+            group = make_uint2(0u, (1u << (24u + oct_inv)) | 1u);
             done = false;
         }
     }
@@ -201,8 +216,10 @@ struct Traverser {
         }
     }
 
-    // One traversal iteration: open the next node (and test its triangles).  Sets done at the end.
-    __device__ __forceinline__ void step(const BvhView& bvh) {
+    // One iteration: open the nearest pending internal child (if any), then test the triangles of the
+    // leaves it hit.  (Postponing sparse triangle groups onto the stack, as in Ylitie et al., did not
+    // measure faster on this hardware and is not done.)
+    __device__ __forceinline__ void iteration(const BvhView& bvh) {
         if (group.y > 0x00FFFFFFu) {
             const uint32_t hits = group.y;
             const uint32_t bit = 31u - __clz(hits);
@@ -210,26 +227,26 @@ struct Traverser {
             const uint32_t rel = __popc(hits & 0xFFu & ((1u << slot) - 1u));
             const uint32_t node = group.x + rel;
             group.y &= ~(1u << bit);
-            if (group.y > 0x00FFFFFFu) {
-                if (sp < kStackSize) stack[sp++] = group;
-                else overflow = true;
-            }
+            if (group.y > 0x00FFFFFFu) push(group);
             if (kCount) ++node_visits;
             uint32_t child_base, tri_base, imask;
             const uint32_t hm = intersect_children(bvh.nodes, node, p, ix, iy, iz, oct_inv, kClosest ? tbest : p.tmax,
                                                    child_base, tri_base, imask);
             group = make_uint2(child_base, (hm & 0xFF000000u) | imask);
-            uint32_t tm = hm & 0x00FFFFFFu;
-            while (tm) {
-                const uint32_t b = __ffs(tm) - 1u;
-                tm &= tm - 1u;
-                test_tri(bvh, tri_base + b);
-                if (!kClosest && done) return;
-            }
+            tgroup = make_uint2(tri_base, hm & 0x00FFFFFFu);
+        } else {
+            tgroup = group;
+            group = make_uint2(0, 0);
+        }
+        while (tgroup.y != 0u) {
+            const uint32_t b = __ffs(tgroup.y) - 1u;
+            tgroup.y &= tgroup.y - 1u;
+            test_tri(bvh, tgroup.x + b);
+            if (!kClosest && done) return;
         }
         if (group.y <= 0x00FFFFFFu) {
             if (sp == 0) done = true;
-            else group = stack[--sp];
+            else group = pop();
         }
     }
 
