@@ -236,6 +236,20 @@ int pb2_accel_set_counting(pb2_accel* accel, int enable);
 int pb2_accel_get_counters(const pb2_accel* accel, uint64_t* node_visits, uint64_t* tri_tests,
                            void* stream);
 
+/* Closest hit for callers that cannot allocate device memory (a fixed memory budget owned by their own
+ * allocator, or no room for the implicit device synchronisation of cudaMalloc/cudaFree).  No counterpart
+ * in the reference.  Builds the 8-wide BVH over `triangles_dev` (tri_count * 9 floats: v0, v1, v2 per
+ * triangle, world space; prim = triangle index) and writes the closest hit of each ray to hits_dev,
+ * with every intermediate buffer in one 8 MiB file-scope device array that every GPU loading the library
+ * holds until exit -- at most 16384 triangles (larger inputs return PB2_ERR_INVALID_ARGUMENT).  Hits
+ * equal those of pb2_accel_create + pb2_trace_closest on the same triangles.  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  The BVH build synchronises `stream`; the trace is queued on it.  All calls share the array
+ * and it keeps the last call's contents: calls that overlap on the GPU (other threads or streams) race
+ * and must be serialised by the caller. */
+int pb2_trace_closest_nalloc(const float* triangles_dev, uint32_t tri_count, const pb2_ray* rays_dev, uint32_t n,
+                             pb2_hit* hits_dev, void* stream);
+
 /* ---- render pipeline (Tracer::buildPipeline, Pipeline::prepare, TraceLauncher::launch;
  *      Tracer.hpp:100-119, 153-155; Embree.cpp:978-1304) --------------------------------------- */
 typedef struct pb2_pipeline pb2_pipeline;

@@ -122,6 +122,7 @@ SIGNATURES = [
     ("pb2_trace_any", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_trace_closest_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_trace_any_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pb2_trace_closest_nalloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_accel_set_counting", C.c_int, [C.c_void_p, C.c_int]),
     ("pb2_accel_get_counters", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_void_p]),
     ("pb2_pipeline_create", C.c_int, [C.POINTER(Scene), C.POINTER(RenderSettings), C.c_void_p,

@@ -478,4 +478,57 @@ cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* wnodes,
     return cudaGetLastError();
 }
 
+
+// The same build for callers that cannot allocate: no CUDA events, every buffer supplied by the caller
+// (used by the static-scratch trace entry point in nalloc.cu).
+cudaError_t build_wide_bvh_prealloc(const TriSlot* tris_in, uint32_t n, WideNode* wnodes, TriSlot* tris_out,
+                                    void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* node_count_out) {
+    cudaError_t err;
+    const size_t m = n ? n : 1;
+    const ScratchLayout L = layout(static_cast<char*>(scratch), n);
+    if (L.total > scratch_bytes) return cudaErrorInvalidValue;
+    *node_count_out = 0;
+    if (n == 0) return cudaSuccess;
+    Frontier *fa = L.fa, *fb = L.fb;
+    const int T = 256;
+    const unsigned G = (unsigned)((n + T - 1) / T);
+    const int init_bounds[8] = { INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, 0, 0 };
+    if ((err = cudaMemcpyAsync(L.cbounds, init_bounds, sizeof(init_bounds), cudaMemcpyHostToDevice, stream))) return err;
+    k_tri_bounds<<<G, T, 0, stream>>>(tris_in, n, L.lo, L.hi, L.cbounds);
+    k_morton<<<G, T, 0, stream>>>(L.lo, L.hi, n, L.cbounds, L.keys, L.vals);
+    size_t cbb = L.cub_bytes;
+    if ((err = cub::DeviceRadixSort::SortPairs(L.cub_tmp, cbb, L.keys, L.keys2, L.vals, L.vals2, (int)n, 0, 63, stream)))
+        return err;
+    k_gather_leaves<<<G, T, 0, stream>>>(L.vals2, L.lo, L.hi, n, L.slo, L.shi);
+    if (n > 1) {
+        if ((err = cudaMemsetAsync(L.flags, 0, sizeof(uint32_t) * m, stream))) return err;
+        k_karras<<<(unsigned)((n - 1 + T - 1) / T), T, 0, stream>>>(L.keys2, n, L.nodes, L.iparent, L.lparent);
+        k_refit<<<G, T, 0, stream>>>(L.nodes, L.iparent, L.lparent, L.slo, L.shi, L.ilo, L.ihi, L.flags, n);
+    }
+    const uint32_t init_counters[8] = { 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u };
+    if ((err = cudaMemcpyAsync(L.counters, init_counters, sizeof(init_counters), cudaMemcpyHostToDevice, stream)))
+        return err;
+    const Frontier root{ n > 1 ? 0 : ~0, 0u };
+    if ((err = cudaMemcpyAsync(fa, &root, sizeof(root), cudaMemcpyHostToDevice, stream))) return err;
+    uint32_t count = 1;
+    int guard = 0;
+    while (count > 0) {
+        if ((err = cudaMemsetAsync(L.counters + 2, 0, sizeof(uint32_t), stream))) return err;
+        k_collapse<<<(count + 127) / 128, 128, 0, stream>>>(fa, count, fb, L.counters + 2, L.counters + 0, L.counters + 1,
+                                                           L.nodes, L.slo, L.shi, L.ilo, L.ihi, L.vals2, tris_in, wnodes,
+                                                           tris_out);
+        if ((err = cudaMemcpyAsync(&count, L.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream))) return err;
+        if ((err = cudaStreamSynchronize(stream))) return err;
+        Frontier* t = fa;
+        fa = fb;
+        fb = t;
+        if (++guard > 256) return cudaErrorUnknown;
+    }
+    if ((err = cudaMemcpyAsync(node_count_out, L.counters + 0, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)))
+        return err;
+    if ((err = cudaStreamSynchronize(stream))) return err;
+    return cudaGetLastError();
+}
+
 }  // namespace pb2
+

@@ -60,5 +60,8 @@ struct BuildResult {
 cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* nodes, TriSlot* tris_out, void* scratch,
                            size_t scratch_bytes, cudaStream_t stream, BuildResult* result);
 size_t build_scratch_bytes(uint32_t n);
+// The same build without CUDA events, into caller-supplied buffers only; writes the node count.
+cudaError_t build_wide_bvh_prealloc(const TriSlot* tris_in, uint32_t n, WideNode* nodes, TriSlot* tris_out,
+                                    void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* node_count_out);
 
 }  // namespace pb2
