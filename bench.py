@@ -224,6 +224,7 @@ def run_ours(args):
     peak, peak_kind = _peaks()
     traffic = _profile_traffic()
     cpu = cpu_baseline(soup, crays, arays, args) if world == 1 else None
+    render = render_bench(args) if world == 1 else None
     line = {
         "metric": METRIC,
         "value": round(value, 2),
@@ -249,6 +250,7 @@ def run_ours(args):
                                      "triangle_tests_per_ray": round(nt_c / N_RAYS, 3)}},
         "cpu_baseline": cpu,
         "gpu_launches": 2 * args.steps,
+        "render": render,
         "clocks": clk.summary(),
         "detail": {"closest_mrays_s": round(N_RAYS / (sum(t_closest) / args.steps * 1e-3) / 1e6, 2),
                    "anyhit_mrays_s": round(N_RAYS / (sum(t_any) / args.steps * 1e-3) / 1e6, 2),
@@ -257,6 +259,54 @@ def run_ours(args):
                    "bvh_nodes": info.node_count, "bvh_build_ms": round(info.build_ms, 3)},
     }
     print(json.dumps(line))
+
+
+def render_bench(args):
+    """The render path on the Cornell-box configuration (256 x 256, 16 spp, depth 8, NEE + MIS): device time
+    of full-frame launches, against the reference's own kernels compiled natively (oracle/_ref) on all
+    host cores over a bounded crop."""
+    import torch
+
+    import oracle_py
+
+    from piper2_b200 import api, capi, scenes
+
+    sd = scenes.cornell_box(seed=0)
+    st = sd.settings
+    samples_per_frame = st.width * st.height * st.samples_per_pixel
+    with api.Pipeline(sd) as pl:
+        film = pl.new_film()
+        for _ in range(3):
+            pl.launch(film)
+        torch.cuda.synchronize()
+        s0 = pl.stats()
+        c0, h0 = s0.closest_rays, s0.shadow_rays
+        frames = max(3, args.steps // 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(frames):
+            pl.launch(film)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        s1 = pl.stats()
+        rays = (s1.closest_rays - c0) + (s1.shadow_rays - h0)
+    out = {"workload": "Cornell box 256x256, 16 spp, max depth 8, NEE+MIS (plain BxDF sampling)",
+           "samples_per_s": round(samples_per_frame * frames / (ms * 1e-3), 1),
+           "mrays_per_s": round(rays / (ms * 1e-3) / 1e6, 2), "ms_per_frame": round(ms / frames, 3),
+           "rays_per_sample": round(rays / (samples_per_frame * frames), 3)}
+    if oracle_py.ref_available():
+        crop = capi.Rect(0, 96, 256, 16)
+        rs = oracle_py.RefScene(sd, use_bvh=True)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        rs.render(rect=crop, threads=threads, samples=False)
+        dt = time.perf_counter() - t0
+        n = crop.width * crop.height * st.samples_per_pixel
+        out["cpu_baseline"] = {"value": round(n / dt, 1), "unit": "samples/s", "cores": threads, "kind": "reference",
+                               "sample": "rows 96-111 of the frame (65,536 samples) through the reference's own "
+                                         "kernels compiled natively, CPU BVH in place of Embree"}
+    return out
 
 
 def cpu_baseline(soup, crays, arays, args, sample=None):
