@@ -215,6 +215,11 @@ typedef struct pb2_accel_info {
 int pb2_accel_create(const pb2_scene* scene, void* stream, pb2_accel** out);
 int pb2_accel_destroy(pb2_accel* accel);
 int pb2_accel_get_info(const pb2_accel* accel, pb2_accel_info* info);
+/* Host-side structural check of the built BVH (copies it out of device memory): child and triangle
+ * indices in range, every node and triangle reached exactly once, every triangle inside the dequantised
+ * box of its child slot.  PB2_OK or PB2_ERR_INVALID_ARGUMENT naming the first violation.  No
+ * counterpart in the reference (Embree's BVH is opaque). */
+int pb2_accel_validate(const pb2_accel* accel);
 
 /* Closest hit over triangles and area-light planes (planes reported with prim =
  * PB2_PLANE_FLAG | plane index).  Ties in t resolve to the lowest prim. */
@@ -273,6 +278,45 @@ int pb2_pipeline_get_stats(const pb2_pipeline* pipeline, pb2_launch_stats* stats
  * points_dev the film point (2 floats), in (y, x) order. */
 int pb2_pipeline_camera_rays(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample,
                              pb2_ray* rays_dev, float* points_dev, void* stream);
+
+/* ---- learned path guiding (no counterpart in the reference, which samples BxDFs only) ------------
+ * A 96-64-64-64-64-48 MLP (BF16 tensor-core tiles, FP32 accumulation) maps the encoded hit position,
+ * shading normal and outgoing direction to a mixture of 8 von Mises-Fisher lobes.  Guided pipelines draw
+ * each non-specular continuation direction from 0.5 BxDF + 0.5 mixture (one-sample MIS, pdf = the
+ * mixture of both), which keeps the estimator unbiased; NEE + MIS is unchanged.  The network is trained
+ * online on the radiance samples the integrator produces, with the Monte-Carlo KL divergence and Adam. */
+typedef struct pb2_guide pb2_guide;
+
+uint32_t pb2_guide_param_count(void);
+/* He-uniform weights from `seed`, zero biases, zeroed Adam state. */
+int pb2_guide_create(uint32_t seed, pb2_guide** out);
+int pb2_guide_destroy(pb2_guide* guide);
+/* Flat fp32 parameters: per layer W[out][in] then b[out]; setting them resets the Adam state. */
+int pb2_guide_set_params(pb2_guide* guide, const float* params_host, uint32_t count);
+int pb2_guide_get_params(const pb2_guide* guide, float* params_host, uint32_t count);
+/* features_dev: n rows of 12 floats (position in the unit cube xyz, normal xyz, outgoing dir xyz, unused);
+ * out_dev: n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused). */
+int pb2_guide_forward(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev, void* stream);
+/* records_dev: n rows of 16 floats (position xyz, normal xyz, outgoing xyz, sampled direction xyz, weight =
+ * target / sampling pdf, unused x3).  Gradient of the batch loss into grad_host (pb2_guide_param_count
+ * floats, may be NULL) and the loss; parameters unchanged. */
+int pb2_guide_gradient(pb2_guide* guide, const float* records_dev, uint32_t n, float* grad_host, float* loss_host,
+                       void* stream);
+/* One Adam step (beta1 0.9, beta2 0.99) on the batch. */
+int pb2_guide_train(pb2_guide* guide, const float* records_dev, uint32_t n, float learning_rate, float* loss_host,
+                    void* stream);
+
+typedef struct pb2_guide_settings {
+    float selection_prob;      /* probability of sampling the guide at a non-specular vertex (0.5) */
+    uint32_t record_capacity;  /* training records kept per launch (e.g. 262144) */
+} pb2_guide_settings;
+
+/* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */
+int pb2_pipeline_set_guide(pb2_pipeline* pipeline, pb2_guide* guide, const pb2_guide_settings* settings);
+/* Runs `steps` Adam steps of `batch` records drawn from the records of the launches since the last call,
+ * then clears them.  Writes the last step's loss. */
+int pb2_pipeline_train_guide(pb2_pipeline* pipeline, uint32_t steps, uint32_t batch, float learning_rate,
+                             float* loss_host, void* stream);
 
 #ifdef __cplusplus
 }

@@ -57,6 +57,10 @@ def oracle():
         h.or_render.restype = C.c_int
         h.or_render.argtypes = [C.c_void_p, C.POINTER(capi.RenderSettings), C.POINTER(capi.Rect), C.c_uint32,
                                 C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        h.or_bsdf_sample.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]
+        h.or_bsdf_eval.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
         h.or_calc_render_rect.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_uint32,
                                           C.POINTER(capi.NDCTransform), C.POINTER(capi.Rect)]
         h.or_plane_make.argtypes = [C.POINTER(C.c_float)] * 3 + [C.POINTER(capi.Plane)]
@@ -123,6 +127,29 @@ class OracleScene:
         rays = np.ascontiguousarray(rays)
         oracle().or_trace_counters(self.h, rays.ctypes.data, len(rays), 1 if closest else 0, C.byref(nv), C.byref(nt))
         return nv.value, nt.value
+
+    def bsdf_sample(self, mat, wo, u, front=True):
+        """Material `mat`'s BxDF sampled at n (u1, u2) pairs -> (wi (n,3), f (n,3), pdf (n,))."""
+        u = np.ascontiguousarray(u, dtype=np.float32)
+        n = len(u)
+        wo = np.ascontiguousarray(wo, dtype=np.float32)
+        wi = np.zeros((n, 3), np.float32)
+        f = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        oracle().or_bsdf_sample(self.h, mat, int(front), wo.ctypes.data, n, u.ctypes.data, wi.ctypes.data,
+                                f.ctypes.data, pdf.ctypes.data)
+        return wi, f, pdf
+
+    def bsdf_eval(self, mat, wo, wi, front=True):
+        """Material `mat`'s BxDF value (n,3) and pdf (n,) at directions wi (n,3)."""
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        n = len(wi)
+        wo = np.ascontiguousarray(wo, dtype=np.float32)
+        f = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        oracle().or_bsdf_eval(self.h, mat, int(front), wo.ctypes.data, n, wi.ctypes.data, f.ctypes.data,
+                              pdf.ctypes.data)
+        return f, pdf
 
     def render(self, settings, rect=None, sample_begin=0, sample_count=None, threads=0, samples=True):
         st = settings

@@ -340,7 +340,10 @@ static int plane_test(const pb2_plane* pl, v3 org_local, v3 dir, float tnear, fl
 }
 
 /* Conservative slab test: the far distance is widened by 3 ulp-scale (Ize 2013, "Robust BVH Ray
- * Traversal"), so rounding never culls a box holding the true closest hit. */
+ * Traversal"), so rounding never culls a box holding the true closest hit.  The current best distance
+ * is widened the same way: a triangle's t (watertight test arithmetic) can round a few ulp below the
+ * slab entry of the flat box that holds it, and a box holding a tie at exactly the best t must still
+ * be opened for the lowest-primitive tie rule (coplanar floors and box bottoms). */
 static inline int box_test(const ray_pre* p, const float* bmin, const float* bmax, float tbest, float* tnear_out) {
     const float tx0 = (bmin[0] - p->o.x) * p->id.x, tx1 = (bmax[0] - p->o.x) * p->id.x;
     const float ty0 = (bmin[1] - p->o.y) * p->id.y, ty1 = (bmax[1] - p->o.y) * p->id.y;
@@ -348,7 +351,7 @@ static inline int box_test(const ray_pre* p, const float* bmin, const float* bma
     const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), p->tmin));
     const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.0000004f;
     *tnear_out = tn;
-    return tn <= fminf(tf, tbest);
+    return tn <= fminf(tf, tbest * 1.0000004f);
 }
 
 typedef struct or_hit_rec {
@@ -809,7 +812,10 @@ static inline int part_match(int provide, int require) { return (provide & requi
 
 typedef struct bsdf_sample { v3 wi; spec f; float pdf; int part; } bsdf_sample;
 
-enum { LOBE_LAMBERT, LOBE_OREN_NAYAR, LOBE_MF_REFL, LOBE_FRESNEL_SPEC, LOBE_MF_TRANS, LOBE_MIRROR, LOBE_BLEND };
+/* LOBE_GGX_VNDF: the conductor extension (no reference counterpart), GGX reflection sampled with exact
+ * visible-normal sampling (Heitz 2018, JCGT 7(4), listing 1) and its density G1(wo) D(wh) / (4 wo.z). */
+enum { LOBE_LAMBERT, LOBE_OREN_NAYAR, LOBE_MF_REFL, LOBE_FRESNEL_SPEC, LOBE_MF_TRANS, LOBE_MIRROR, LOBE_BLEND,
+       LOBE_GGX_VNDF };
 enum { FRESNEL_DIELECTRIC, FRESNEL_SCHLICK };
 
 typedef struct lobe {
@@ -930,6 +936,28 @@ static v3 mf_sample_wh(float ax, float ay, v3 wi, float u1, float u2) {
 
 /* halfVector (Transform.hpp:279-282) */
 static inline v3 half_vector(v3 a, v3 b) { return normalize3(mk3(a.x + b.x, a.y + b.y, a.z + b.z)); }
+
+/* Heitz 2018, listing 1: a visible normal of the GGX distribution (ax, ay) seen from wo (wo.z > 0). */
+static v3 ggx_sample_vndf(float ax, float ay, v3 wo, float u1, float u2) {
+    const v3 vh = normalize3(mk3(ax * wo.x, ay * wo.y, wo.z));
+    const float lensq = vh.x * vh.x + vh.y * vh.y;
+    v3 t1 = mk3(1.0f, 0.0f, 0.0f);
+    if (lensq > 0.0f) {
+        const float inv = 1.0f / sqrtf(lensq);
+        t1 = mk3(-vh.y * inv, vh.x * inv, 0.0f);
+    }
+    const v3 t2 = cross3(vh, t1);
+    const float r = sqrtf(u1);
+    float sp, cp;
+    pb2_sincosf(K_TWO_PI * u2, &sp, &cp);
+    const float p1 = r * cp;
+    const float s = 0.5f * (1.0f + vh.z);
+    const float p2 = (1.0f - s) * sqrt_safe(1.0f - p1 * p1) + s * (r * sp);
+    const float pz = sqrt_safe(1.0f - p1 * p1 - p2 * p2);
+    const v3 nh = mk3(p1 * t1.x + p2 * t2.x + pz * vh.x, p1 * t1.y + p2 * t2.y + pz * vh.y,
+                      p1 * t1.z + p2 * t2.z + pz * vh.z);
+    return normalize3(mk3(ax * nh.x, ay * nh.y, fmaxf(0.0f, nh.z)));
+}
 /* reflect (Transform.hpp:405-408) */
 static inline v3 reflect3(v3 wo, v3 n) { return sub3(mul3s(n, 2.0f * dot3(wo, n)), wo); }
 /* refract (Transform.hpp:410-421) */
@@ -987,6 +1015,14 @@ static spec lobe_eval(const lobe* L, v3 wo, v3 wi) {
                             (4.0f * (1.0f + mf_lambda(L->ax, L->ay, wo) + mf_lambda(L->ax, L->ay, wi)) * fabsf(wo.z * wi.z));
             return sp_mul(L->color, mksp(F.r * q, F.g * q, F.b * q));
         }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f || wi.z <= 0.0f) return SP_ZERO;
+            const v3 wh = half_vector(wo, wi);
+            const spec F = lobe_fresnel(L, dot3(wi, wh));
+            const float q = mf_d(L->ax, L->ay, wh) /
+                            (4.0f * (1.0f + mf_lambda(L->ax, L->ay, wo) + mf_lambda(L->ax, L->ay, wi)) * (wo.z * wi.z));
+            return sp_mul(L->color, mksp(F.r * q, F.g * q, F.b * q));
+        }
         case LOBE_MF_TRANS: { /* Kernel.cpp:553-573 */
             if (wi.z >= 0.0f) return SP_ZERO;
             v3 wh = normalize3(add3(wo, mul3s(wi, L->eta)));
@@ -1028,6 +1064,12 @@ static float lobe_pdf(const lobe* L, v3 wo, v3 wi) {
             const float p1 = 1.0f + mf_lambda(L->ax, L->ay, wo);
             const float p2 = mf_lambda(L->ax, L->ay, wh);
             return fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+        }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
+            const v3 wh = half_vector(wo, wi);
+            if (dot3(wo, wh) <= 0.0f) return 0.0f;
+            return mf_d(L->ax, L->ay, wh) / (4.0f * wo.z * (1.0f + mf_lambda(L->ax, L->ay, wo)));
         }
         case LOBE_MF_TRANS: { /* Kernel.cpp:574-586 */
             if (wi.z >= 0.0f) return 0.0f;
@@ -1074,6 +1116,16 @@ static void lobe_sample(const lobe* L, float u1, float u2, v3 wo, bsdf_sample* r
             res->part = L->part;
             const float p2 = mf_lambda(L->ax, L->ay, wh);
             res->pdf = fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+            return;
+        }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f) return;
+            const v3 wh = ggx_sample_vndf(L->ax, L->ay, wo, u1, u2);
+            res->wi = reflect3(wo, wh);
+            if (res->wi.z <= 0.0f) return;
+            res->f = lobe_eval(L, wo, res->wi);
+            res->pdf = lobe_pdf(L, wo, res->wi);
+            res->part = L->part;
             return;
         }
         case LOBE_FRESNEL_SPEC: { /* FresnelSpecular::sample (Kernel.cpp:519-536) */
@@ -1168,7 +1220,7 @@ static void bsdf_init(const or_scene* s, uint32_t mat, int front, bsdf* b) {
         }
         case PB2_SURFACE_CONDUCTOR: {
             lobe* L = &b->l[b->n++];
-            L->type = LOBE_MF_REFL; L->part = PART_GLOSSY | PART_R;
+            L->type = LOBE_GGX_VNDF; L->part = PART_GLOSSY | PART_R;
             L->color = mksp(1.0f, 1.0f, 1.0f);
             L->color2 = c1;
             L->fresnel = FRESNEL_SCHLICK;
@@ -1306,6 +1358,9 @@ static uint32_t cdf_select(const float* cdf, const float* pdf, uint32_t size, fl
         if (*u >= cdf[mid]) l = mid + 1;
         else r = mid;
     }
+    /* u == 1.0f (a Sobol value whose float conversion rounds up to 2^32) makes the reference read one
+     * entry past the end; the library and this restatement use the last entry instead */
+    if (r >= size) r = size - 1;
     *u = (*u - cdf[r]) / pdf[r];
     return r;
 }
@@ -1533,6 +1588,39 @@ static void splat(const pb2_render_settings* st, float* rgbw, float px, float py
         p[1] += v.g * w;
         p[2] += v.b * w;
         p[3] += w;
+    }
+}
+
+/* BxDF of scene material `mat` (shading frame, geometric normal +z) for checks of its sampler:
+ * n samples (u pairs in u[2i], u[2i+1]) -> wi (3n), f (3n), pdf (n; 0 where the sample was rejected). */
+void or_bsdf_sample(const or_scene* s, uint32_t mat, int front, const float wo_in[3], uint32_t n, const float* u,
+                    float* wi, float* f, float* pdf) {
+    bsdf b;
+    bsdf_init(s, mat, front, &b);
+    const v3 wo = mk3(wo_in[0], wo_in[1], wo_in[2]);
+    const v3 ng = mk3(0.0f, 0.0f, 1.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+        bsdf_sample r;
+        memset(&r, 0, sizeof(r));
+        bsdf_sample_fn(&b, u[2 * i], u[2 * i + 1], wo, ng, PART_ALL, &r);
+        wi[3 * i] = r.wi.x; wi[3 * i + 1] = r.wi.y; wi[3 * i + 2] = r.wi.z;
+        f[3 * i] = r.f.r; f[3 * i + 1] = r.f.g; f[3 * i + 2] = r.f.b;
+        pdf[i] = r.pdf;
+    }
+}
+
+/* The same BxDF's value and pdf at n given directions. */
+void or_bsdf_eval(const or_scene* s, uint32_t mat, int front, const float wo_in[3], uint32_t n, const float* wi,
+                  float* f, float* pdf) {
+    bsdf b;
+    bsdf_init(s, mat, front, &b);
+    const v3 wo = mk3(wo_in[0], wo_in[1], wo_in[2]);
+    const v3 ng = mk3(0.0f, 0.0f, 1.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const v3 w = mk3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        const spec v = bsdf_eval(&b, wo, w, ng, PART_ALL);
+        f[3 * i] = v.r; f[3 * i + 1] = v.g; f[3 * i + 2] = v.b;
+        pdf[i] = bsdf_pdf(&b, wo, w, PART_ALL);
     }
 }
 

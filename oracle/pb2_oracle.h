@@ -61,6 +61,11 @@ int or_render(const or_scene* s, const pb2_render_settings* settings, const pb2_
 void or_calc_render_rect(uint32_t width, uint32_t height, float device_aspect, uint32_t fit_mode,
                          pb2_ndc_transform* transform, pb2_rect* rect);
 void or_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out);
+/* BxDF of scene material `mat` in its shading frame (geometric normal +z): sampling and evaluation. */
+void or_bsdf_sample(const or_scene* s, uint32_t mat, int front, const float wo[3], uint32_t n, const float* u,
+                    float* wi, float* f, float* pdf);
+void or_bsdf_eval(const or_scene* s, uint32_t mat, int front, const float wo[3], uint32_t n, const float* wi,
+                  float* f, float* pdf);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,8 @@
 * :class:`Pipeline`  -- ``Tracer::buildPipeline`` -> ``Pipeline::prepare`` -> ``TraceLauncher::launch``
   (Src/Interface/BuiltinComponent/Tracer.hpp:100-159) and the FixedSampler film resolve
   (Src/BuiltinComponent/RenderDriver/FixedSampler/FixedSampler.cpp:68-133).
+* :class:`Guide`     -- the learned path-guiding network (no counterpart in the reference: its
+  PathTracing integrator samples BxDFs only), attached with :meth:`Pipeline.set_guide`.
 
 Device memory and streams come from torch (plumbing only); all compute is in libpiper2_b200.so.
 Errors raise :class:`piper2_b200.capi.PB2Error` with the library's message.
@@ -46,6 +48,10 @@ class Accel:
         i = capi.AccelInfo()
         capi.check(capi.lib().pb2_accel_get_info(self.h, C.byref(i)))
         return i
+
+    def validate(self):
+        """Structural check of the BVH (raises PB2Error naming the first violation)."""
+        capi.check(capi.lib().pb2_accel_validate(self.h))
 
     def close(self):
         if getattr(self, "h", None):
@@ -176,6 +182,99 @@ class Pipeline:
         s = capi.LaunchStats()
         capi.check(capi.lib().pb2_pipeline_get_stats(self.h, C.byref(s), _stream()))
         return s
+
+    def set_guide(self, guide, selection_prob=0.5, record_capacity=1 << 18):
+        """Attach a :class:`Guide` (None detaches); later launches sample and record with it."""
+        self._guide = guide
+        if guide is None:
+            capi.check(capi.lib().pb2_pipeline_set_guide(self.h, None, None))
+            return
+        st = capi.GuideSettings(float(selection_prob), int(record_capacity))
+        capi.check(capi.lib().pb2_pipeline_set_guide(self.h, guide.h, C.byref(st)))
+
+    def train_guide(self, steps, batch=4096, learning_rate=5e-3) -> float:
+        """Adam steps on the records of the launches since the last call; returns the last loss."""
+        loss = C.c_float(0.0)
+        capi.check(capi.lib().pb2_pipeline_train_guide(self.h, steps, batch, learning_rate, C.byref(loss), _stream()))
+        return loss.value
+
+    def render_guided(self, film, spp, spp_per_pass=4, train_steps=16, batch=8192, learning_rate=5e-3,
+                      train_passes=None, rect=None, sample_begin=0):
+        """Progressive guided render: `spp / spp_per_pass` launches into `film`, each followed (for the first
+        `train_passes`, default all) by `train_steps` Adam steps on the records it produced.  Every pass is
+        an unbiased estimate, so the film averages all of them.  Returns the losses."""
+        losses = []
+        passes = max(1, spp // spp_per_pass)
+        for p in range(passes):
+            self.launch(film, rect, sample_begin + p * spp_per_pass, spp_per_pass)
+            if train_steps and (train_passes is None or p < train_passes) and p + 1 < passes:
+                losses.append(self.train_guide(train_steps, batch, learning_rate))
+        return losses
+
+
+class Guide:
+    """Path-guiding MLP (96-64-64-64-64-48, 8 von Mises-Fisher lobes) with Adam state on the device."""
+
+    def __init__(self, seed=1):
+        _torch().cuda.init()
+        h = C.c_void_p()
+        capi.check(capi.lib().pb2_guide_create(seed, C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def param_count() -> int:
+        return int(capi.lib().pb2_guide_param_count())
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().pb2_guide_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), dtype=np.float32)
+        capi.check(capi.lib().pb2_guide_get_params(self.h, out.ctypes.data_as(C.c_void_p), len(out)))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        capi.check(capi.lib().pb2_guide_set_params(self.h, p.ctypes.data_as(C.c_void_p), len(p)))
+
+    def forward(self, features: np.ndarray) -> np.ndarray:
+        """features (n, 12) -> raw outputs (n, 48)."""
+        torch = _torch()
+        f = torch.from_numpy(np.ascontiguousarray(features, dtype=np.float32)).cuda()
+        n = f.shape[0]
+        out = torch.empty((n, 48), dtype=torch.float32, device="cuda")
+        capi.check(capi.lib().pb2_guide_forward(self.h, C.c_void_p(f.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                                _stream()))
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    def gradient(self, records: np.ndarray):
+        """records (n, 16) -> (gradient over the flat parameters, loss)."""
+        torch = _torch()
+        r = torch.from_numpy(np.ascontiguousarray(records, dtype=np.float32)).cuda()
+        g = np.empty(self.param_count(), dtype=np.float32)
+        loss = C.c_float(0.0)
+        capi.check(capi.lib().pb2_guide_gradient(self.h, C.c_void_p(r.data_ptr()), r.shape[0],
+                                                 g.ctypes.data_as(C.c_void_p), C.byref(loss), _stream()))
+        return g, loss.value
+
+    def train(self, records, learning_rate=5e-3) -> float:
+        """One Adam step on a batch; `records` is a (n, 16) numpy array or float32 CUDA tensor."""
+        torch = _torch()
+        r = records if isinstance(records, torch.Tensor) else torch.from_numpy(
+            np.ascontiguousarray(records, dtype=np.float32)).cuda()
+        loss = C.c_float(0.0)
+        capi.check(capi.lib().pb2_guide_train(self.h, C.c_void_p(r.data_ptr()), r.shape[0], learning_rate,
+                                              C.byref(loss), _stream()))
+        return loss.value
 
 
 def sobol_generate(index: np.ndarray, dim: np.ndarray) -> np.ndarray:

@@ -103,6 +103,10 @@ class PB2Error(RuntimeError):
 _lib = None
 
 # (name, restype, argtypes) for every entry point declared in include/piper2_b200.h
+class GuideSettings(C.Structure):
+    _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32)]
+
+
 SIGNATURES = [
     ("pb2_last_error", C.c_char_p, []),
     ("pb2_abi_version", C.c_int, []),
@@ -118,6 +122,7 @@ SIGNATURES = [
     ("pb2_accel_create", C.c_int, [C.POINTER(Scene), C.c_void_p, C.POINTER(C.c_void_p)]),
     ("pb2_accel_destroy", C.c_int, [C.c_void_p]),
     ("pb2_accel_get_info", C.c_int, [C.c_void_p, C.POINTER(AccelInfo)]),
+    ("pb2_accel_validate", C.c_int, [C.c_void_p]),
     ("pb2_trace_closest", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_trace_any", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_trace_closest_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -134,6 +139,18 @@ SIGNATURES = [
     ("pb2_film_resolve", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_pipeline_get_stats", C.c_int, [C.c_void_p, C.POINTER(LaunchStats), C.c_void_p]),
     ("pb2_pipeline_camera_rays", C.c_int, [C.c_void_p, C.POINTER(Rect), C.c_uint32, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]),
+    ("pb2_guide_param_count", C.c_uint32, []),
+    ("pb2_guide_create", C.c_int, [C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("pb2_guide_destroy", C.c_int, [C.c_void_p]),
+    ("pb2_guide_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    ("pb2_guide_get_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    ("pb2_guide_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pb2_guide_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_float),
+                                      C.c_void_p]),
+    ("pb2_guide_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_float), C.c_void_p]),
+    ("pb2_pipeline_set_guide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(GuideSettings)]),
+    ("pb2_pipeline_train_guide", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float),
                                             C.c_void_p]),
 ]
 

@@ -254,6 +254,97 @@ int pb2_accel_destroy(pb2_accel* acc) {
     return PB2_OK;
 }
 
+// Structural check of the built BVH on the host: every internal child index inside the node array and
+// reached exactly once from the root, every leaf triangle range inside the triangle array and every
+// triangle slot covered exactly once, every primitive id present once, and every triangle inside the
+// dequantised box of the child slot that holds it.
+int pb2_accel_validate(const pb2_accel* acc) {
+    if (!acc) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_validate: null accel");
+    const uint32_t nn = acc->view.node_count, nt = acc->view.tri_count;
+    if (nt == 0) return PB2_OK;
+    std::vector<WideNode> nodes(nn);
+    std::vector<TriSlot> tris(nt);
+    cudaError_t e;
+    if ((e = cudaMemcpy(nodes.data(), acc->nodes, sizeof(WideNode) * nn, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(tris.data(), acc->tris, sizeof(TriSlot) * nt, cudaMemcpyDeviceToHost)))
+        return cuda_fail(e, "pb2_accel_validate: download");
+    if (nn == 0) return fail(PB2_ERR_INVALID_ARGUMENT, "BVH has triangles but no nodes");
+    std::vector<uint8_t> node_seen(nn, 0), slot_seen(nt, 0), prim_seen(nt, 0);
+    std::vector<uint32_t> stack{ 0 };
+    node_seen[0] = 1;
+    auto bad = [&](uint32_t node, const std::string& what) {
+        return fail(PB2_ERR_INVALID_ARGUMENT, "BVH node " + std::to_string(node) + ": " + what);
+    };
+    while (!stack.empty()) {
+        const uint32_t ni = stack.back();
+        stack.pop_back();
+        const WideNode& w = nodes[ni];
+        float p[3];
+        std::memcpy(p, &w.w[0], 12);
+        int ex[3];
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t b = (w.w[0].w >> (8 * a)) & 0xFFu;
+            if (b == 0 || b == 255) return bad(ni, "exponent byte out of range");
+            ex[a] = (int)b - 127;
+        }
+        const uint32_t imask = w.w[0].w >> 24, child_base = w.w[1].x, tri_base = w.w[1].y;
+        uint8_t meta[8], q[6][8];
+        std::memcpy(meta, &w.w[1].z, 8);
+        std::memcpy(q[0], &w.w[2].x, 8);  // lo x
+        std::memcpy(q[1], &w.w[2].z, 8);  // lo y
+        std::memcpy(q[2], &w.w[3].x, 8);  // lo z
+        std::memcpy(q[3], &w.w[3].z, 8);  // hi x
+        std::memcpy(q[4], &w.w[4].x, 8);  // hi y
+        std::memcpy(q[5], &w.w[4].z, 8);  // hi z
+        uint32_t rank = 0;
+        for (int s = 0; s < 8; ++s) {
+            const uint8_t m = meta[s];
+            const bool internal = (imask >> s) & 1u;
+            if (m == 0) {
+                if (internal) return bad(ni, "empty slot marked internal");
+                continue;
+            }
+            double lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = (double)p[a] + std::ldexp((double)q[a][s], ex[a]);
+                hi[a] = (double)p[a] + std::ldexp((double)q[3 + a][s], ex[a]);
+                if (lo[a] > hi[a]) return bad(ni, "inverted child box");
+            }
+            if (internal) {
+                if (m != ((1u << 5) | (24u + s))) return bad(ni, "internal slot meta mismatch");
+                const uint64_t c = (uint64_t)child_base + rank++;
+                if (c >= nn) return bad(ni, "child index " + std::to_string(c) + " >= node count");
+                if (node_seen[c]++) return bad(ni, "child " + std::to_string(c) + " reached twice");
+                stack.push_back((uint32_t)c);
+            } else {
+                const uint32_t unary = m >> 5, off = m & 0x1Fu;
+                if (unary != 1u && unary != 3u && unary != 7u) return bad(ni, "leaf count not unary");
+                const uint32_t cnt = unary == 1u ? 1u : unary == 3u ? 2u : 3u;
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    const uint64_t sl = (uint64_t)tri_base + off + k;
+                    if (sl >= nt) return bad(ni, "triangle slot " + std::to_string(sl) + " >= triangle count");
+                    if (slot_seen[sl]++) return bad(ni, "triangle slot " + std::to_string(sl) + " in two leaves");
+                    const TriSlot& t = tris[sl];
+                    uint32_t prim;
+                    std::memcpy(&prim, &t.v0.w, 4);
+                    if (prim >= nt) return bad(ni, "primitive id out of range");
+                    if (prim_seen[prim]++) return bad(ni, "primitive " + std::to_string(prim) + " twice");
+                    const float* v[3] = { &t.v0.x, &t.v1.x, &t.v2.x };
+                    for (int j = 0; j < 3; ++j)
+                        for (int a = 0; a < 3; ++a)
+                            if (!(v[j][a] >= lo[a] && v[j][a] <= hi[a]))
+                                return bad(ni, "triangle outside its child box");
+                }
+            }
+        }
+    }
+    for (uint32_t i = 0; i < nn; ++i)
+        if (!node_seen[i]) return fail(PB2_ERR_INVALID_ARGUMENT, "BVH node " + std::to_string(i) + " unreachable");
+    for (uint32_t i = 0; i < nt; ++i)
+        if (!slot_seen[i]) return fail(PB2_ERR_INVALID_ARGUMENT, "triangle slot " + std::to_string(i) + " in no leaf");
+    return PB2_OK;
+}
+
 int pb2_accel_get_info(const pb2_accel* acc, pb2_accel_info* info) {
     if (!acc || !info) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_get_info: null argument");
     *info = acc->info;

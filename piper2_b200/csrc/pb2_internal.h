@@ -1,5 +1,6 @@
 // pb2_internal.h -- declarations shared between the library's translation units (not installed).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -13,6 +14,15 @@ namespace pb2 {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
+
+// The guiding network's inference weights (guiding.cu): the padded bf16 weight image and fp32 biases.
+struct GuideView {
+    const __nv_bfloat16* w16;
+    const float* b32;
+};
+cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n, float* out, cudaStream_t stream);
+cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
+                           cudaStream_t stream);
 
 cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
                              bool closest, bool count, uint32_t* work, unsigned long long* counters,
@@ -35,4 +45,16 @@ struct pb2_accel {
     // staging buffers of the *_host trace calls
     void* stage = nullptr;
     size_t stage_bytes = 0;
+};
+
+struct pb2_guide {
+    float* params = nullptr;  // fp32 master parameters, flat layout (per layer: W[out][in], then b[out])
+    float* m = nullptr;       // Adam moments
+    float* v = nullptr;
+    float* grad = nullptr;
+    __nv_bfloat16* w16 = nullptr;  // padded bf16 weight image used by the tensor-core tiles
+    float* b32 = nullptr;
+    float* scalars = nullptr;  // [0] weight sum of the batch, [1] loss
+    uint32_t step = 0;
+    pb2::GuideView view() const { return pb2::GuideView{ w16, b32 }; }
 };

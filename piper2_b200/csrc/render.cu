@@ -10,9 +10,11 @@
 // so each path's radiance equals the CPU oracle's bit for bit; only the film sums, which use
 // atomics in any order (as the reference's CAS loop does), differ in rounding.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
+#include "guiding.cuh"
 #include "pb2_internal.h"
 #include "shading.cuh"
 #include "traverse.cuh"
@@ -74,7 +76,9 @@ constexpr int kNumSurfaceTypes = 7;
 // Counter slots in Paths::counts
 enum : int {
     C_EXT_CUR = 0, C_EXT_NEXT = 1, C_SHADOW = 2, C_MIS = 3, C_SHADED = 4, C_SURF0 = 5,  // 5..11 per type
-    C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24, C_COUNT = 32
+    C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24,
+    C_CHECK = 25,  // 25..28: first failed index check (code, kernel, slot, value)
+    C_COUNT = 32
 };
 
 struct Paths {
@@ -123,6 +127,7 @@ struct LaunchParams {
     uint32_t num_lights;  // area lights
     float env[3];
     uint32_t path_count;
+    uint32_t checks;      // PB2_DEBUG_CHECKS: verify indices, record the first violation, skip the path
 };
 
 struct SceneView {
@@ -132,12 +137,33 @@ struct SceneView {
     const float* plane_cdf;
     const float* plane_pdf;
     BvhView bvh;
+    uint32_t material_count;
+};
+
+// Guided sampling state of a launch (all pointers device memory, indexed by path slot unless noted).
+constexpr int kMaxRecords = 3;  // pending training records per path (its first guided vertices)
+struct GuideState {
+    uint32_t enabled;
+    float sel_prob;
+    GuideView net;
+    float* mix;             // 40 floats per slot: lobe weights [8], means [8][3], concentrations [8]
+    float4* rec;            // record r of slot s, word k: rec[(r * 5 + k) * cap + s]
+    uint32_t* nrec;
+    uint32_t cap;
+    float* train;           // training records, 16 floats each
+    uint32_t* train_count;  // [0] written, [1] offered
+    uint32_t train_capacity;
+    float accept_prob;
+    uint32_t salt;
+    float bmin[3], binv[3];
 };
 
 // ---- helpers ----------------------------------------------------------------------------------------
 
+// Warp-aggregated queue append: the active lanes that push to the same counter (lanes may push to
+// different queues, e.g. one per material type) share one atomic.
 __device__ __forceinline__ uint32_t warp_push(uint32_t* counter) {
-    const unsigned mask = __activemask();
+    const unsigned mask = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(counter));
     const int leader = __ffs(mask) - 1;
     const unsigned lane = threadIdx.x & 31u;
     uint32_t base = 0;
@@ -151,6 +177,21 @@ __device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
     if ((int)(threadIdx.x & 31u) == __ffs(mask) - 1) atomicAdd(counter, (unsigned long long)v);
 }
+
+// Debug index checks (LaunchParams::checks): the first failure is recorded and the access skipped.
+enum CheckKernel : uint32_t { K_CLASSIFY = 1, K_SHADE = 2, K_FINISH = 3 };
+__device__ __noinline__ void check_failed(uint32_t* counts, uint32_t code, uint32_t kernel, uint32_t slot, uint32_t v) {
+    if (atomicCAS(&counts[C_CHECK], 0u, code) == 0u) {
+        counts[C_CHECK + 1] = kernel;
+        counts[C_CHECK + 2] = slot;
+        counts[C_CHECK + 3] = v;
+    }
+}
+#define PB2_CHECK(cond, code, kernel, slot, v)                              \
+    if (lp.checks && !(cond)) {                                             \
+        check_failed(ps.counts, (code), (kernel), (uint32_t)(slot), (uint32_t)(v)); \
+        continue;                                                           \
+    }
 
 // The pixel/sample of path p: p = ((row * rect.width) + col) * sample_count + k
 __device__ __forceinline__ void path_coords(const LaunchParams& lp, uint32_t p, uint32_t& sx, uint32_t& sy,
@@ -218,7 +259,7 @@ __global__ void k_camera_rays(LaunchParams lp, uint32_t sample, float4* __restri
     points[i] = make_float2(px, py);
 }
 
-__global__ void k_generate(LaunchParams lp, Paths ps) {
+__global__ void k_generate(LaunchParams lp, Paths ps, GuideState gs) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= lp.path_count) return;
     uint32_t sx, sy, s;
@@ -236,6 +277,7 @@ __global__ void k_generate(LaunchParams lp, Paths ps) {
     ps.depth[p] = 0;
     ps.point[p] = make_float2(px, py);
     ps.ext[0][p] = p;
+    if (gs.enabled) gs.nrec[p] = 0;
 }
 
 // ---- traversal over queues -----------------------------------------------------------------------
@@ -349,14 +391,61 @@ __device__ __forceinline__ void terminate_path(const LaunchParams& lp, const Pat
     }
 }
 
+__device__ __forceinline__ float luminance(float r, float g, float b) { return 0.2126f * r + 0.7152f * g + 0.0722f * b; }
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// Turns the path's pending guided vertices into training records: the incident radiance estimate along
+// the sampled direction is (radiance gathered after the vertex) / (throughput before the vertex's
+// sampling) x pdf / (f cos), so target / pdf = lum(S_end - S_v) / lum(pf_v).
+__device__ __forceinline__ void flush_records(const GuideState& gs, uint32_t slot, float4 s_end) {
+    const uint32_t n = gs.nrec[slot];
+    for (uint32_t r = 0; r < n; ++r) {
+        const float4 a = gs.rec[(r * 5 + 0) * gs.cap + slot];
+        const float4 b = gs.rec[(r * 5 + 1) * gs.cap + slot];
+        const float4 c = gs.rec[(r * 5 + 2) * gs.cap + slot];
+        const float4 pf = gs.rec[(r * 5 + 3) * gs.cap + slot];
+        const float4 sv = gs.rec[(r * 5 + 4) * gs.cap + slot];
+        const float lpf = luminance(pf.x, pf.y, pf.z);
+        const float dl = luminance(s_end.x - sv.x, s_end.y - sv.y, s_end.z - sv.z);
+        if (!(dl > 0.f && lpf > 0.f)) continue;
+        const float w = dl / lpf;
+        if (!(w < 3.0e38f)) continue;
+        atomicAdd(&gs.train_count[1], 1u);
+        const float u = (float)(hash32(slot * 3u + r + gs.salt * 0x9E3779B9u) >> 8) * (1.0f / 16777216.0f);
+        if (u >= gs.accept_prob) continue;
+        const uint32_t idx = atomicAdd(&gs.train_count[0], 1u);
+        if (idx >= gs.train_capacity) continue;
+        float4* o = reinterpret_cast<float4*>(gs.train + 16 * (size_t)idx);
+        o[0] = make_float4(a.x, a.y, a.z, a.w);
+        o[1] = make_float4(b.x, b.y, b.z, b.w);
+        o[2] = make_float4(c.x, c.y, c.z, c.w);
+        o[3] = make_float4(w, 0.f, 0.f, 0.f);
+    }
+    gs.nrec[slot] = 0;
+}
+
 // ---- classify extend results (PathTracing/Kernel.cpp:116-149) ------------------------------------
 
-__global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur, float4* film, float* sample_out) {
+__global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur, float4* film,
+                           float* sample_out) {
     const uint32_t n = ps.counts[C_EXT_CUR];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PB2_CHECK(n <= lp.path_count, 1, K_CLASSIFY, 0, n);
         const uint32_t slot = ps.ext[cur][i];
+        PB2_CHECK(slot < lp.path_count, 2, K_CLASSIFY, slot, i);
         const float4 h = ps.hit[slot];
         const uint32_t prim = __float_as_uint(h.y);
+        PB2_CHECK(prim == kInvalidPrim || ((prim & kPlaneFlag) ? (prim & ~kPlaneFlag) < sv.bvh.plane_count
+                                                                : prim < sv.bvh.tri_count),
+                  3, K_CLASSIFY, slot, prim);
         const float4 o4 = ps.o[slot], d4 = ps.d[slot];
         const float4 pf4 = ps.pf[slot];
         const bool specular = pf4.w != 0.0f;
@@ -392,10 +481,13 @@ __global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur
             continue;
         }
         if (missing || ps.depth[slot] >= lp.max_depth) {
+            if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
             terminate_path(lp, ps, slot, film, sample_out);
             continue;
         }
+        PB2_CHECK(sv.prim_material[prim] < sv.material_count, 4, K_CLASSIFY, slot, sv.prim_material[prim]);
         const uint32_t type = sv.materials[sv.prim_material[prim]].type;
+        PB2_CHECK(type < (uint32_t)kNumSurfaceTypes, 5, K_CLASSIFY, slot, type);
         ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
     }
 }
@@ -424,6 +516,9 @@ __device__ __forceinline__ uint32_t cdf_select(const float* cdf, const float* pd
         if (u >= cdf[mid]) l = mid + 1;
         else r = mid;
     }
+    // u rounds to 1.0f when the Sobol value is within 2^-25 of 1 (its float conversion rounds up); the
+    // reference then reads one past the end, here the last entry is used
+    if (r >= size) r = size - 1;
     u = (u - cdf[r]) / pdf[r];
     return r;
 }
@@ -485,15 +580,26 @@ __device__ __forceinline__ v3 to_local(const Frame& f, v3 v) {
                f.T.z * v.x + f.B.z * v.y + f.N.z * v.z);
 }
 
+// Material types whose continuation is guided: those whose BxDF sampler draws exactly the density its pdf
+// reports (Lambert and Oren-Nayar cosine sampling, the conductor's visible-normal sampling).  One-sample MIS
+// with the guide needs that density; the reference's microfacet lobes (Plastic, rough Glass, Substrate) report
+// a pdf that is not their sampler's density (Classic/Kernel.cpp:405-412), so they keep plain BxDF sampling.
+__host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_MATTE || t == PB2_SURFACE_CONDUCTOR; }
+
 template <int kType>
-__global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
+__global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PB2_CHECK(n <= lp.path_count, 10, K_SHADE, 0, n);
         const uint32_t slot = ps.surf[kType][i];
+        PB2_CHECK(slot < lp.path_count, 11, K_SHADE, slot, i);
         ++vertices;
         const float4 h = ps.hit[slot];
         const uint32_t prim = __float_as_uint(h.y);
+        PB2_CHECK(prim < sv.bvh.tri_count, 12, K_SHADE, slot, prim);
+        PB2_CHECK(ps.hit_slot[slot] < sv.bvh.tri_count, 13, K_SHADE, slot, ps.hit_slot[slot]);
+        PB2_CHECK(ps.dim[slot] <= PB2_SOBOL_DIMS, 14, K_SHADE, slot, ps.dim[slot]);
         const float4 o4 = ps.o[slot], d4 = ps.d[slot], pf4 = ps.pf[slot];
         const v3 o = mk3(o4.x, o4.y, o4.z), d = mk3(d4.x, d4.y, d4.z);
         spec pf = mksp(pf4.x, pf4.y, pf4.z);
@@ -526,6 +632,8 @@ __global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
             const float u = sc.next();
             uint32_t sel = (uint32_t)floorf(u * (float)count);
             if (sel > count - 1) sel = count - 1;
+            PB2_CHECK(sel == 0 || sv.lights[sel - 1].first_plane + sv.lights[sel - 1].plane_count <= sv.bvh.plane_count,
+                      15, K_SHADE, slot, sel);
             const float sel_pdf = 1.0f / (float)count;
             ps.mis_pf[slot] = make_float4(pf.r, pf.g, pf.b, sel_pdf);
             float4 nee = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -568,14 +676,63 @@ __global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
                 }
             }
         }
-        // continuation (PathTracing/Kernel.cpp:164-190)
-        BsdfSample ss;
-        float u1, u2;
-        sc.pair(u1, u2);
-        bsdf_sample(bsdf, u1, u2, wo, ng_sh, kPartAll, ss);
-        bool cont = ss.pdf > 0.0f && sp_valid(ss.f);
+        // continuation (PathTracing/Kernel.cpp:164-190); guided vertices sample 0.5 BxDF + 0.5 mixture
+        const bool guided = guided_type(kType) && gs.enabled && bsdf.no_specular;
+        v3 wi_sh;
+        spec fval;
+        float pdf;
+        int part;
+        bool cont;
+        if (!guided) {
+            BsdfSample ss;
+            float u1, u2;
+            sc.pair(u1, u2);
+            bsdf_sample(bsdf, u1, u2, wo, ng_sh, kPartAll, ss);
+            cont = ss.pdf > 0.0f && sp_valid(ss.f);
+            wi_sh = ss.wi;
+            fval = ss.f;
+            pdf = ss.pdf;
+            part = ss.part;
+        } else {
+            const float uc = sc.next();
+            float u1, u2;
+            sc.pair(u1, u2);
+            guide::Mixture mx;
+            const float* mp = gs.mix + 40 * (size_t)slot;
+#pragma unroll
+            for (int k = 0; k < guide::kLobes; ++k) {
+                mx.w[k] = mp[k];
+                mx.mu[k][0] = mp[8 + 3 * k];
+                mx.mu[k][1] = mp[9 + 3 * k];
+                mx.mu[k][2] = mp[10 + 3 * k];
+                mx.kappa[k] = mp[32 + k];
+            }
+            float pb, pg;
+            cont = true;
+            if (uc < gs.sel_prob) {
+                float x, y, z;
+                guide::mixture_sample(mx, uc / gs.sel_prob, u1, u2, x, y, z);
+                wi_sh = to_shading(fr, mk3(x, y, z));
+                fval = bsdf_eval(bsdf, wo, wi_sh, ng_sh, kPartAll);
+                pb = bsdf_pdf(bsdf, wo, wi_sh, kPartAll);
+                pg = guide::mixture_pdf(mx, x, y, z);
+            } else {
+                BsdfSample ss;
+                bsdf_sample(bsdf, u1, u2, wo, ng_sh, kPartAll, ss);
+                cont = ss.pdf > 0.0f && sp_valid(ss.f);
+                wi_sh = ss.wi;
+                fval = ss.f;
+                pb = ss.pdf;
+                const v3 wl = to_local(fr, ss.wi);
+                pg = cont ? guide::mixture_pdf(mx, wl.x, wl.y, wl.z) : 0.0f;
+            }
+            pdf = gs.sel_prob * pg + (1.0f - gs.sel_prob) * pb;
+            cont = cont && pdf > 0.0f && sp_valid(fval);
+            part = (dot3(wo, ng_sh) * dot3(wi_sh, ng_sh)) > 0.0f ? kPartR : kPartT;
+        }
+        const spec pf_in = pf;
         if (cont) {
-            pf = sp_muls(sp_mul(pf, ss.f), fabsf(ss.wi.z) / ss.pdf);
+            pf = sp_muls(sp_mul(pf, fval), fabsf(wi_sh.z) / pdf);
             if (depth > lp.min_rr_depth) {
                 const float p = fmaxf(0.05f, 1.0f - fmaxf(pf.r, fmaxf(pf.g, pf.b)));
                 if (sc.next() < p) cont = false;
@@ -583,13 +740,27 @@ __global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
             }
         }
         if (cont) {
-            const v3 nd = to_local(fr, ss.wi);
-            const v3 no = add3(hit, mul3s(fr.Ng, (ss.part & kPartR) ? 0.001f : -0.001f));
+            const v3 nd = to_local(fr, wi_sh);
+            const v3 no = add3(hit, mul3s(fr.Ng, (part & kPartR) ? 0.001f : -0.001f));
             ps.o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
             ps.d[slot] = make_float4(nd.x, nd.y, nd.z, 0.0f);
-            ps.pf[slot] = make_float4(pf.r, pf.g, pf.b, (ss.part & kPartSpecular) ? 1.0f : 0.0f);
+            ps.pf[slot] = make_float4(pf.r, pf.g, pf.b, (part & kPartSpecular) ? 1.0f : 0.0f);
             ps.depth[slot] = depth + 1u;
             flags |= 2u;
+            if (guided) {
+                const uint32_t r = gs.nrec[slot];
+                if (r < (uint32_t)kMaxRecords) {
+                    const v3 wl = to_local(fr, wo);
+                    const float px = (hit.x - gs.bmin[0]) * gs.binv[0], py = (hit.y - gs.bmin[1]) * gs.binv[1],
+                                pz = (hit.z - gs.bmin[2]) * gs.binv[2];
+                    gs.rec[(r * 5 + 0) * gs.cap + slot] = make_float4(px, py, pz, fr.N.x);
+                    gs.rec[(r * 5 + 1) * gs.cap + slot] = make_float4(fr.N.y, fr.N.z, wl.x, wl.y);
+                    gs.rec[(r * 5 + 2) * gs.cap + slot] = make_float4(wl.z, nd.x, nd.y, nd.z);
+                    gs.rec[(r * 5 + 3) * gs.cap + slot] = make_float4(pf_in.r, pf_in.g, pf_in.b, 0.0f);
+                    gs.nrec[slot] = r + 1;
+                    flags |= 8u;
+                }
+            }
         }
         ps.dim[slot] = sc.dim;
         ps.flags[slot] = flags;
@@ -598,13 +769,99 @@ __global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur) {
     if (vertices) warp_count(reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_VERTICES), vertices);
 }
 
+// ---- guide inference for the surface queues of the guided material types ------------------------------
+
+__global__ void __launch_bounds__(guide::kThreads) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
+    using namespace guide;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* w_s = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* b_s = reinterpret_cast<float*>(smem + kW16Elems * 2);
+    FwdTile* tiles = reinterpret_cast<FwdTile*>(smem + kW16Elems * 2 + kBiasElems * 4);
+    load_weights(gs.net, w_s, b_s);
+    __syncthreads();
+    uint32_t counts[kNumSurfaceTypes], total = 0;
+    for (int t = 0; t < kNumSurfaceTypes; ++t) {
+        counts[t] = guided_type(t) ? ps.counts[C_SURF0 + t] : 0u;
+        total += counts[t];
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    FwdTile& T = tiles[warp];
+    uint32_t slots16 = 0;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < (total + 15) / 16; tile += gridDim.x * kWarps) {
+        const uint32_t row = tile * 16 + lane;
+        uint32_t slot = 0xFFFFFFFFu;
+        if (lane < 16) {
+            float f[9] = { 0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f };
+            if (row < total) {
+                uint32_t idx = row;
+                int t = 0;
+                while (idx >= counts[t]) { idx -= counts[t]; ++t; }
+                slot = ps.surf[t][idx];
+                const float4 h = ps.hit[slot];
+                const float4 o4 = ps.o[slot], d4 = ps.d[slot];
+                const v3 d = mk3(d4.x, d4.y, d4.z);
+                const v3 hit = add3(mk3(o4.x, o4.y, o4.z), mul3s(d, h.x));
+                const float4* t4 = reinterpret_cast<const float4*>(sv.bvh.tris + ps.hit_slot[slot]);
+                const float4 a = t4[0], b = t4[1], c = t4[2];
+                const v3 ng = normalize3(cross3(sub3(mk3(b.x, b.y, b.z), mk3(a.x, a.y, a.z)),
+                                                sub3(mk3(c.x, c.y, c.z), mk3(a.x, a.y, a.z))));
+                const v3 N = dot3(d, ng) < 0.0f ? ng : neg3(ng);
+                f[0] = (hit.x - gs.bmin[0]) * gs.binv[0];
+                f[1] = (hit.y - gs.bmin[1]) * gs.binv[1];
+                f[2] = (hit.z - gs.bmin[2]) * gs.binv[2];
+                f[3] = N.x; f[4] = N.y; f[5] = N.z;
+                f[6] = -d.x; f[7] = -d.y; f[8] = -d.z;
+            }
+            encode_row(f, T.x + lane * kXStride);
+        }
+        __syncwarp();
+        forward_tile(w_s, b_s, T.x, T.h[0], T.h[1], T.y);
+        if (lane < 16 && slot != 0xFFFFFFFFu) {
+            Mixture m;
+            mixture_from_raw(T.y + lane * kOut, m);
+            float* mp = gs.mix + 40 * (size_t)slot;
+            for (int k = 0; k < kLobes; ++k) {
+                mp[k] = m.w[k];
+                mp[8 + 3 * k] = m.mu[k][0];
+                mp[9 + 3 * k] = m.mu[k][1];
+                mp[10 + 3 * k] = m.mu[k][2];
+                mp[32 + k] = m.kappa[k];
+            }
+            ++slots16;
+        }
+        __syncwarp();
+    }
+    (void)slots16;
+}
+
+__global__ void k_gather_batch(const float* __restrict__ src, uint32_t count, float* __restrict__ dst, uint32_t batch,
+                               uint32_t salt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) return;
+    const uint32_t j = hash32(i * 0x27d4eb2du + salt) % count;
+    const float4* s4 = reinterpret_cast<const float4*>(src + 16 * (size_t)j);
+    float4* d4 = reinterpret_cast<float4*>(dst + 16 * (size_t)i);
+    d4[0] = s4[0];
+    d4[1] = s4[1];
+    d4[2] = s4[2];
+    d4[3] = s4[3];
+}
+
 // ---- finish: add the vertex's MIS estimate, then re-queue or splat --------------------------------
 
-__global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur, float4* film, float* sample_out) {
+__global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur, float4* film,
+                         float* sample_out) {
     const uint32_t n = ps.counts[C_SHADED];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PB2_CHECK(n <= lp.path_count, 20, K_FINISH, 0, n);
         const uint32_t slot = ps.shaded_q[i];
+        PB2_CHECK(slot < lp.path_count, 21, K_FINISH, slot, i);
         const uint32_t flags = ps.flags[slot];
+        PB2_CHECK(!(flags & 4u) || __float_as_uint(ps.mhit[slot].y) == kInvalidPrim ||
+                      ((__float_as_uint(ps.mhit[slot].y) & kPlaneFlag)
+                           ? (__float_as_uint(ps.mhit[slot].y) & ~kPlaneFlag) < sv.bvh.plane_count
+                           : __float_as_uint(ps.mhit[slot].y) < sv.bvh.tri_count),
+                  22, K_FINISH, slot, __float_as_uint(ps.mhit[slot].y));
         if (flags & 1u) {
             const float4 nee = ps.nee[slot];
             spec part_a = sp_zero();
@@ -652,8 +909,13 @@ __global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, uint32_t cur, 
             const spec sample = sp_add(mksp(r.x, r.y, r.z), sp_mul(mksp(mpf.x, mpf.y, mpf.z), mis));
             ps.rad[slot] = make_float4(sample.r, sample.g, sample.b, 0.0f);
         }
-        if (flags & 2u) ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
-        else terminate_path(lp, ps, slot, film, sample_out);
+        if (flags & 8u) gs.rec[((gs.nrec[slot] - 1u) * 5 + 4) * gs.cap + slot] = ps.rad[slot];
+        if (flags & 2u) {
+            ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
+        } else {
+            if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
+            terminate_path(lp, ps, slot, film, sample_out);
+        }
     }
 }
 
@@ -700,6 +962,7 @@ struct pb2_pipeline {
     float* plane_cdf = nullptr;
     float* plane_pdf = nullptr;
     uint32_t num_lights = 0;
+    uint32_t material_count = 0;
     float env[3] = { 0, 0, 0 };
     float gauss_sub = 0.0f;
     // path state
@@ -708,7 +971,42 @@ struct pb2_pipeline {
     Paths ps{};
     pb2_launch_stats stats{};
     int sms = 0;
+    // scene box (guide input normalisation)
+    float bmin[3] = { 0, 0, 0 }, binv[3] = { 1, 1, 1 };
+    // attached guide and its per-slot / training buffers
+    pb2_guide* guide = nullptr;
+    pb2_guide_settings guide_settings{};
+    uint32_t guide_cap = 0;
+    void* guide_state = nullptr;
+    float* g_mix = nullptr;
+    float4* g_rec = nullptr;
+    uint32_t* g_nrec = nullptr;
+    float* g_train = nullptr;
+    float* g_batch = nullptr;
+    uint32_t* g_count = nullptr;
+    uint32_t g_train_capacity = 0, g_batch_capacity = 0;
+    uint32_t g_offered = 0;  // records offered by the launches since the last training call (host estimate)
+    uint32_t g_salt = 0;
 };
+
+static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
+    if (pl->guide_cap >= cap) return PB2_OK;
+    cudaFree(pl->guide_state);
+    pl->guide_state = nullptr;
+    pl->guide_cap = 0;
+    const size_t c = cap;
+    const size_t mix = ((c * 40 * 4 + 255) / 256) * 256, rec = ((c * kMaxRecords * 5 * 16 + 255) / 256) * 256;
+    cudaError_t e = cudaMalloc(&pl->guide_state, mix + rec + c * 4);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc guide path state");
+    char* p = static_cast<char*>(pl->guide_state);
+    pl->g_mix = reinterpret_cast<float*>(p);
+    pl->g_rec = reinterpret_cast<float4*>(p + mix);
+    pl->g_nrec = reinterpret_cast<uint32_t*>(p + mix + rec);
+    pl->guide_cap = cap;
+    return PB2_OK;
+}
+
+static size_t infer_smem() { return (size_t)guide::kW16Elems * 2 + guide::kBiasElems * 4 + guide::kWarps * sizeof(guide::FwdTile); }
 
 static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
     if (pl->capacity >= cap) return PB2_OK;
@@ -816,6 +1114,33 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
         return fail(PB2_ERR_NOT_SUPPORTED, "film larger than 2^25");
     }
     pl->gauss_sub = std::exp(-st->gaussian_alpha);
+    {
+        float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
+        for (uint32_t m = 0; m < scene->mesh_count; ++m) {
+            const pb2_mesh& me = scene->meshes[m];
+            for (uint32_t v = 0; v < me.vert_count; ++v)
+                for (int k = 0; k < 3; ++k) {
+                    const float x = me.vertices[3 * v + k] + me.translation[k];
+                    lo[k] = std::fmin(lo[k], x);
+                    hi[k] = std::fmax(hi[k], x);
+                }
+        }
+        for (uint32_t i = 0; i < scene->plane_count; ++i) {
+            const pb2_plane& pp = scene->planes[i];
+            for (int c = 0; c < 4; ++c)
+                for (int k = 0; k < 3; ++k) {
+                    const float x = pp.origin[k] + ((c & 1) ? pp.u[k] : 0.0f) + ((c & 2) ? pp.v[k] : 0.0f);
+                    lo[k] = std::fmin(lo[k], x);
+                    hi[k] = std::fmax(hi[k], x);
+                }
+        }
+        for (int k = 0; k < 3; ++k) {
+            if (!(lo[k] <= hi[k])) lo[k] = hi[k] = 0.0f;
+            const float ext = std::fmax(hi[k] - lo[k], 1e-6f);
+            pl->bmin[k] = lo[k] - 1e-3f * ext;
+            pl->binv[k] = 1.0f / (ext * 1.002f);
+        }
+    }
     // materials
     std::vector<DevMaterial> mats(scene->material_count ? scene->material_count : 1);
     for (uint32_t m = 0; m < scene->material_count; ++m) {
@@ -870,6 +1195,7 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
         L.inverse_area = 1.0f / total;
     }
     pl->num_lights = scene->area_light_count;
+    pl->material_count = scene->material_count;
     for (int k = 0; k < 3; ++k) pl->env[k] = scene->env_radiance[k];
     cudaError_t e;
     if ((e = cudaMalloc(&pl->materials, sizeof(DevMaterial) * mats.size())) ||
@@ -899,6 +1225,10 @@ int pb2_pipeline_destroy(pb2_pipeline* pl) {
     cudaFree(pl->plane_cdf);
     cudaFree(pl->plane_pdf);
     cudaFree(pl->state);
+    cudaFree(pl->guide_state);
+    cudaFree(pl->g_train);
+    cudaFree(pl->g_batch);
+    cudaFree(pl->g_count);
     delete pl;
     return PB2_OK;
 }
@@ -929,6 +1259,11 @@ static LaunchParams make_params(const pb2_pipeline* pl, const pb2_rect& rect, ui
     lp.num_lights = pl->num_lights;
     for (int k = 0; k < 3; ++k) lp.env[k] = pl->env[k];
     lp.path_count = rect.width * rect.height * sc;
+    static const bool checks = [] {
+        const char* v = std::getenv("PB2_DEBUG_CHECKS");
+        return v && v[0] == '1';
+    }();
+    lp.checks = checks ? 1u : 0u;
     return lp;
 }
 
@@ -963,6 +1298,33 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     int rc = alloc_paths(pl, (uint32_t)paths);
     if (rc) return rc;
     const LaunchParams lp = make_params(pl, *rect, sample_begin, sample_count);
+    GuideState gs{};
+    if (pl->guide) {
+        if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
+            return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
+        if ((rc = alloc_guide_slots(pl, (uint32_t)paths))) return rc;
+        gs.enabled = 1;
+        gs.sel_prob = pl->guide_settings.selection_prob;
+        gs.net = pl->guide->view();
+        gs.mix = pl->g_mix;
+        gs.rec = pl->g_rec;
+        gs.nrec = pl->g_nrec;
+        gs.cap = pl->guide_cap;
+        gs.train = pl->g_train;
+        gs.train_count = pl->g_count;
+        gs.train_capacity = pl->g_train_capacity;
+        // keep about `capacity` of the records the launches offer between two training calls: the expected
+        // count of this launch is estimated from the previous ones (all records are kept at first)
+        const double expect = (double)pl->g_offered + (double)paths * 1.5;
+        gs.accept_prob = expect > pl->g_train_capacity ? (float)(pl->g_train_capacity / expect) : 1.0f;
+        gs.salt = ++pl->g_salt;
+        for (int k = 0; k < 3; ++k) { gs.bmin[k] = pl->bmin[k]; gs.binv[k] = pl->binv[k]; }
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
+            attr = true;
+        }
+    }
     SceneView sv;
     sv.materials = pl->materials;
     sv.prim_material = pl->accel->prim_material;
@@ -970,6 +1332,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     sv.plane_cdf = pl->plane_cdf;
     sv.plane_pdf = pl->plane_pdf;
     sv.bvh = pl->accel->view;
+    sv.material_count = pl->material_count;
     Paths ps = pl->ps;
     float4* film = reinterpret_cast<float4*>(rgbw);
     cudaError_t e;
@@ -977,7 +1340,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     const uint32_t pc = (uint32_t)paths;
     if ((e = cudaMemcpyAsync(ps.counts + C_EXT_CUR, &pc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream)))
         return cuda_fail(e, "set count");
-    k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps);
+    k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps, gs);
     const int grid = pl->sms * 8;
     uint32_t* work = pl->accel->work;
     unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
@@ -990,7 +1353,23 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     }
     uint32_t cur = 0;
     const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
-    for (int bounce = 0;; ++bounce) {
+    // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed
+    static const bool debug_sync = [] {
+        const char* v = std::getenv("PB2_DEBUG_SYNC");
+        return v && v[0] == '1';
+    }();
+    const char* failed = nullptr;
+    auto checked = [&](const char* name) {
+        if (!debug_sync || failed) return;
+        cudaError_t err = cudaGetLastError();
+        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) {
+            failed = name;
+            e = err;
+        }
+    };
+    checked("k_generate");
+    for (int bounce = 0; !failed; ++bounce) {
         uint32_t active = 0;
         if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
             (e = cudaStreamSynchronize(stream)))
@@ -1001,22 +1380,38 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
         k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(sv.bvh, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
                                                                  stats);
-        k_classify<<<grid, 256, 0, stream>>>(lp, sv, ps, cur, film, sample_out);
-        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
-        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(lp, sv, ps, cur);
+        checked("k_trace_queue<extend>");
+        k_classify<<<grid, 256, 0, stream>>>(lp, sv, ps, gs, cur, film, sample_out);
+        checked("k_classify");
+        if (gs.enabled) k_guide_infer<<<pl->sms, guide::kThreads, infer_smem(), stream>>>(sv, ps, gs);
+        checked("k_guide_infer");
+        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<matte>");
+        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<plastic>");
+        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<glass>");
+        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<mirror>");
+        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<substrate>");
+        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<conductor>");
+        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        checked("k_shade<blackbody>");
         k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
                                                                    sstats);
+        checked("k_trace_queue<shadow>");
         k_trace_queue<Q_MIS><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats);
-        k_finish<<<grid, 256, 0, stream>>>(lp, sv, ps, cur, film, sample_out);
+        checked("k_trace_queue<mis>");
+        k_finish<<<grid, 256, 0, stream>>>(lp, sv, ps, gs, cur, film, sample_out);
+        checked("k_finish");
         k_advance<<<1, 1, 0, stream>>>(ps.counts);
-        if ((e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
+        checked("k_advance");
+        if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
         cur ^= 1u;
     }
+    if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
     uint32_t counts[C_COUNT];
     if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
         (e = cudaStreamSynchronize(stream)))
@@ -1029,7 +1424,85 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     std::memcpy(&v, counts + C_STAT_VERTICES, 8);
     pl->stats.path_vertices += v;
     pl->stats.paths += paths;
+    if (counts[C_CHECK])
+        return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
+                                      std::to_string(counts[C_CHECK + 1]) + " at slot " +
+                                      std::to_string(counts[C_CHECK + 2]) + ", value " +
+                                      std::to_string(counts[C_CHECK + 3]));
     if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+    if (gs.enabled) {
+        uint32_t tc[2];
+        if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaStreamSynchronize(stream)))
+            return cuda_fail(e, "read record count");
+        pl->g_offered = tc[1];
+    }
+    return PB2_OK;
+}
+
+int pb2_pipeline_set_guide(pb2_pipeline* pl, pb2_guide* guide, const pb2_guide_settings* settings) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_guide: null pipeline");
+    if (!guide) {
+        pl->guide = nullptr;
+        return PB2_OK;
+    }
+    if (!settings) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_guide: null settings");
+    if (!(settings->selection_prob > 0.0f && settings->selection_prob < 1.0f))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "selection_prob must lie in (0, 1): the BxDF keeps the estimator unbiased");
+    if (settings->record_capacity == 0 || settings->record_capacity > (1u << 26))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "record_capacity must lie in [1, 2^26]");
+    if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
+        return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
+    cudaError_t e;
+    if (settings->record_capacity > pl->g_train_capacity) {
+        cudaFree(pl->g_train);
+        pl->g_train = nullptr;
+        pl->g_train_capacity = 0;
+        if ((e = cudaMalloc(&pl->g_train, (size_t)settings->record_capacity * 64))) return cuda_fail(e, "cudaMalloc records");
+        pl->g_train_capacity = settings->record_capacity;
+    }
+    if (!pl->g_count) {
+        if ((e = cudaMalloc(&pl->g_count, 2 * sizeof(uint32_t)))) return cuda_fail(e, "cudaMalloc record count");
+    }
+    if ((e = cudaMemset(pl->g_count, 0, 2 * sizeof(uint32_t)))) return cuda_fail(e, "memset record count");
+    pl->g_offered = 0;
+    pl->guide = guide;
+    pl->guide_settings = *settings;
+    return PB2_OK;
+}
+
+int pb2_pipeline_train_guide(pb2_pipeline* pl, uint32_t steps, uint32_t batch, float lr, float* loss_host,
+                             void* stream_ptr) {
+    if (!pl || !pl->guide) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_train_guide: no guide attached");
+    if (batch == 0 || batch > (1u << 22)) return fail(PB2_ERR_INVALID_ARGUMENT, "batch must lie in [1, 2^22]");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    cudaError_t e;
+    uint32_t tc[2];
+    if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+        (e = cudaStreamSynchronize(stream)))
+        return cuda_fail(e, "read record count");
+    const uint32_t count = std::min(tc[0], pl->g_train_capacity);
+    float loss = 0.0f;
+    if (count > 0 && steps > 0) {
+        if (batch > pl->g_batch_capacity) {
+            cudaFree(pl->g_batch);
+            pl->g_batch = nullptr;
+            pl->g_batch_capacity = 0;
+            if ((e = cudaMalloc(&pl->g_batch, (size_t)batch * 64))) return cuda_fail(e, "cudaMalloc batch");
+            pl->g_batch_capacity = batch;
+        }
+        for (uint32_t s = 0; s < steps; ++s) {
+            k_gather_batch<<<(batch + 255) / 256, 256, 0, stream>>>(pl->g_train, count, pl->g_batch, batch,
+                                                                    ++pl->g_salt * 0x85ebca6bu);
+            if ((e = cudaGetLastError())) return cuda_fail(e, "k_gather_batch");
+            const int rc = pb2_guide_train(pl->guide, pl->g_batch, batch, lr, s + 1 == steps ? &loss : nullptr, stream_ptr);
+            if (rc) return rc;
+        }
+    }
+    if ((e = cudaMemsetAsync(pl->g_count, 0, 2 * sizeof(uint32_t), stream)) || (e = cudaStreamSynchronize(stream)))
+        return cuda_fail(e, "reset record count");
+    pl->g_offered = 0;
+    if (loss_host) *loss_host = loss;
     return PB2_OK;
 }
 

@@ -63,7 +63,12 @@ struct DevMaterial {
     float roughness0, roughness1;
 };
 
-enum LobeType : int { LOBE_LAMBERT, LOBE_OREN_NAYAR, LOBE_MF_REFL, LOBE_FRESNEL_SPEC, LOBE_MF_TRANS, LOBE_BLEND };
+// LOBE_GGX_VNDF is the conductor extension's lobe (no reference counterpart): the same GGX reflection
+// value as LOBE_MF_REFL, sampled with exact visible-normal sampling (Heitz 2018, "Sampling the GGX
+// Distribution of Visible Normals", JCGT 7(4)) and reporting that sampler's density,
+// pdf(wi) = G1(wo) D(wh) / (4 wo.z).  (The reference's MicrofacetReflection::pdf, Classic/Kernel.cpp:405-412,
+// is not the density of its sampler, which one-sample MIS with a guide cannot tolerate.)
+enum LobeType : int { LOBE_LAMBERT, LOBE_OREN_NAYAR, LOBE_MF_REFL, LOBE_FRESNEL_SPEC, LOBE_MF_TRANS, LOBE_BLEND, LOBE_GGX_VNDF };
 enum FresnelType : int { FRESNEL_DIELECTRIC, FRESNEL_SCHLICK };
 
 struct Lobe {
@@ -184,6 +189,28 @@ __device__ __forceinline__ v3 mf_sample_wh(float ax, float ay, v3 wi, float u1, 
 }
 
 __device__ __forceinline__ v3 half_vector(v3 a, v3 b) { return normalize3(mk3(a.x + b.x, a.y + b.y, a.z + b.z)); }
+
+// Heitz 2018, listing 1: a visible normal of the GGX distribution (ax, ay) seen from wo (wo.z > 0).
+__device__ __forceinline__ v3 ggx_sample_vndf(float ax, float ay, v3 wo, float u1, float u2) {
+    const v3 vh = normalize3(mk3(ax * wo.x, ay * wo.y, wo.z));
+    const float lensq = vh.x * vh.x + vh.y * vh.y;
+    v3 t1 = mk3(1.0f, 0.0f, 0.0f);
+    if (lensq > 0.0f) {
+        const float inv = 1.0f / sqrtf(lensq);
+        t1 = mk3(-vh.y * inv, vh.x * inv, 0.0f);
+    }
+    const v3 t2 = cross3(vh, t1);
+    const float r = sqrtf(u1);
+    float sp, cp;
+    pb2_sincosf(kTwoPi * u2, &sp, &cp);
+    const float p1 = r * cp;
+    const float s = 0.5f * (1.0f + vh.z);
+    const float p2 = (1.0f - s) * sqrt_safe(1.0f - p1 * p1) + s * (r * sp);
+    const float pz = sqrt_safe(1.0f - p1 * p1 - p2 * p2);
+    const v3 nh = mk3(p1 * t1.x + p2 * t2.x + pz * vh.x, p1 * t1.y + p2 * t2.y + pz * vh.y,
+                      p1 * t1.z + p2 * t2.z + pz * vh.z);
+    return normalize3(mk3(ax * nh.x, ay * nh.y, fmaxf(0.0f, nh.z)));
+}
 __device__ __forceinline__ v3 reflect3(v3 wo, v3 n) { return sub3(mul3s(n, 2.0f * dot3(wo, n)), wo); }
 __device__ __forceinline__ bool refract3(v3 wi, v3 n, float eta, v3& wt) {
     const float cos_i = dot3(n, wi);
@@ -241,6 +268,14 @@ __device__ __forceinline__ spec lobe_eval(const Lobe& L, v3 wo, v3 wi) {
                             (4.0f * (1.0f + mf_lambda(L.ax, L.ay, wo) + mf_lambda(L.ax, L.ay, wi)) * fabsf(wo.z * wi.z));
             return sp_mul(L.color, mksp(F.r * q, F.g * q, F.b * q));
         }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f || wi.z <= 0.0f) return sp_zero();
+            const v3 wh = half_vector(wo, wi);
+            const spec F = lobe_fresnel(L, dot3(wi, wh));
+            const float q = mf_d(L.ax, L.ay, wh) /
+                            (4.0f * (1.0f + mf_lambda(L.ax, L.ay, wo) + mf_lambda(L.ax, L.ay, wi)) * (wo.z * wi.z));
+            return sp_mul(L.color, mksp(F.r * q, F.g * q, F.b * q));
+        }
         case LOBE_MF_TRANS: {
             if (wi.z >= 0.0f) return sp_zero();
             v3 wh = normalize3(add3(wo, mul3s(wi, L.eta)));
@@ -282,6 +317,12 @@ __device__ __forceinline__ float lobe_pdf(const Lobe& L, v3 wo, v3 wi) {
             const float p1 = 1.0f + mf_lambda(L.ax, L.ay, wo);
             const float p2 = mf_lambda(L.ax, L.ay, wh);
             return fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+        }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
+            const v3 wh = half_vector(wo, wi);
+            if (dot3(wo, wh) <= 0.0f) return 0.0f;
+            return mf_d(L.ax, L.ay, wh) / (4.0f * wo.z * (1.0f + mf_lambda(L.ax, L.ay, wo)));
         }
         case LOBE_MF_TRANS: {
             if (wi.z >= 0.0f) return 0.0f;
@@ -326,6 +367,16 @@ __device__ __forceinline__ void lobe_sample(const Lobe& L, float u1, float u2, v
             res.part = L.part;
             const float p2 = mf_lambda(L.ax, L.ay, wh);
             res.pdf = fabsf(0.25f / (wo.z * p1 * (p1 + p2)));
+            return;
+        }
+        case LOBE_GGX_VNDF: {
+            if (wo.z <= 0.0f) return;
+            const v3 wh = ggx_sample_vndf(L.ax, L.ay, wo, u1, u2);
+            res.wi = reflect3(wo, wh);
+            if (res.wi.z <= 0.0f) return;
+            res.f = lobe_eval(L, wo, res.wi);
+            res.pdf = lobe_pdf(L, wo, res.wi);
+            res.part = L.part;
             return;
         }
         case LOBE_FRESNEL_SPEC: {
@@ -414,7 +465,7 @@ __device__ __forceinline__ void bsdf_init(const DevMaterial& m, bool front, Bsdf
         }
         case PB2_SURFACE_CONDUCTOR: {
             Lobe& L = b.l[b.n++];
-            L.type = LOBE_MF_REFL; L.part = kPartGlossy | kPartR;
+            L.type = LOBE_GGX_VNDF; L.part = kPartGlossy | kPartR;
             L.color = mksp(1.0f, 1.0f, 1.0f);
             L.color2 = c1;
             L.fresnel = FRESNEL_SCHLICK;

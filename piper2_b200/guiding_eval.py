@@ -1,0 +1,95 @@
+"""Time-to-equal-error of guided against plain path tracing on the hard-indirect room.
+
+Both integrators render the same frame at the same sample count; the error is the relative MSE against a
+plain render of many more samples taken from a disjoint Sobol range,
+
+    relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + 0.01),
+
+and since Monte-Carlo error falls as 1 / time, the time one integrator needs to reach the other's error is
+proportional to time x relMSE.  `speedup` = (T_plain relMSE_plain) / (T_guided relMSE_guided); the guided
+time includes its online training.  The reference's own noise adds the same amount to both errors, so the
+reported speed-up is, if anything, an underestimate.
+
+    python -m piper2_b200.guiding_eval [--width 640 --height 360 --spp 64 --ref-spp 1024]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+
+def _time(torch, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def evaluate(width=640, height=360, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=16, batch=8192,
+             learning_rate=5e-3, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64):
+    import torch
+
+    from . import api, scenes
+
+    sd = scenes.guiding_room(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, tess=tess)
+    out = {"workload": f"guiding room {width}x{height}, {spp} spp, max depth {max_depth}",
+           "reference": f"plain, {ref_spp} spp from samples [{spp}, {spp + ref_spp})"}
+    with api.Pipeline(sd) as pl:
+        film = pl.new_film()
+        for s in range(0, ref_spp, chunk):
+            pl.launch(film, sample_begin=spp + s, sample_count=min(chunk, ref_spp - s))
+        ref = pl.resolve(film).cpu().numpy().astype(np.float64)
+        # plain: one launch of all samples (its fastest form), after a warm-up launch
+        pl.launch(pl.new_film(), sample_begin=0, sample_count=min(spp, 4))
+        film = pl.new_film()
+        t_plain, _ = _time(torch, lambda: pl.launch(film, sample_begin=0, sample_count=spp))
+        plain = pl.resolve(film).cpu().numpy().astype(np.float64)
+        # guided: fresh network, progressive passes with online training
+        guide = api.Guide(seed=seed + 1)
+        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20)
+        film = pl.new_film()
+        t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
+                                                                 learning_rate))
+        guided = pl.resolve(film).cpu().numpy().astype(np.float64)
+        pl.set_guide(None)
+    e_plain, e_guided = rel_mse(plain, ref), rel_mse(guided, ref)
+    out.update({
+        "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
+        "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
+                   "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,
+                   "first_loss": losses[0] if losses else None, "last_loss": losses[-1] if losses else None},
+        "reference_mean": float(ref.mean()),
+        "relmse_ratio": e_plain / e_guided if e_guided > 0 else None,
+        "speedup": (t_plain * e_plain) / (t_guided * e_guided) if e_guided > 0 else None,
+    })
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--width", type=int, default=640)
+    ap.add_argument("--height", type=int, default=360)
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--ref-spp", type=int, default=1024)
+    ap.add_argument("--spp-per-pass", type=int, default=4)
+    ap.add_argument("--train-steps", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=5e-3)
+    ap.add_argument("--selection-prob", type=float, default=0.5)
+    ap.add_argument("--tess", type=int, default=15)
+    a = ap.parse_args()
+    print(json.dumps(evaluate(a.width, a.height, a.spp, a.ref_spp, a.spp_per_pass, a.train_steps, a.batch, a.lr,
+                              a.selection_prob, tess=a.tess)))
+
+
+if __name__ == "__main__":
+    main()

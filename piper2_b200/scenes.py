@@ -251,3 +251,150 @@ def soup_rays(n_rays: int = 1 << 22, seed: int = 1, kind: str = "closest") -> np
     rays["dir"] = d
     rays["tmin"] = 0.0
     return rays
+
+
+def _grid_quad(origin, u, v, nu, nv):
+    """Quad origin + [0,1]u + [0,1]v tessellated into nu x nv cells (2 triangles each)."""
+    o, u, v = (np.asarray(x, dtype=np.float64) for x in (origin, u, v))
+    a = np.linspace(0.0, 1.0, nu + 1)
+    b = np.linspace(0.0, 1.0, nv + 1)
+    A, B = np.meshgrid(a, b, indexing="ij")
+    verts = o + A[..., None] * u + B[..., None] * v
+    verts = verts.reshape(-1, 3)
+    idx = []
+    for i in range(nu):
+        for j in range(nv):
+            p00 = i * (nv + 1) + j
+            p10 = (i + 1) * (nv + 1) + j
+            p01 = p00 + 1
+            p11 = p10 + 1
+            idx += [[p00, p10, p11], [p00, p11, p01]]
+    return verts, np.array(idx, dtype=np.uint32)
+
+
+def guiding_room(seed: int = 0, width: int = 1280, height: int = 720, spp: int = 256, max_depth: int = 16,
+                 min_rr_depth: int = 5, tess: int = 15) -> SceneData:
+    """Hard indirect lighting: a 4 x 2.5 x 4 m room split by a wall at x = 2.5 with a 5 cm door gap; the only
+    area light (0.1 m^2, radiance 200) hangs behind the wall; the floor of the camera's side is glossy GGX
+    (alpha 0.1, the conductor extension); white Lambertian walls.  About 20k triangles (every quad is
+    tessellated)."""
+    rng = np.random.default_rng(seed)
+    sd = SceneData(name=f"guiding_room(seed={seed})")
+    white, floor = 0, 1
+    sd.materials = [material("Matte", (0.75, 0.75, 0.75, 1.0)),
+                    material("Conductor", color1=(0.9, 0.85, 0.8, 1.0), roughness=(0.1, 0.1))]
+    W, H, D = 4.0, 2.5, 4.0
+    xw = 2.5                                      # dividing wall
+    gap_z0, gap_z1, gap_h = 1.975, 2.025, 2.0     # 5 cm wide, 2 m tall door gap
+    quads = [
+        ((0, 0, 0), (xw, 0, 0), (0, 0, D), floor),            # glossy floor, camera side
+        ((xw, 0, 0), (W - xw, 0, 0), (0, 0, D), white),        # floor behind the wall
+        ((0, H, 0), (0, 0, D), (W, 0, 0), white),              # ceiling
+        ((0, 0, 0), (0, H, 0), (0, 0, D), white),              # x = 0 wall
+        ((W, 0, 0), (0, 0, D), (0, H, 0), white),              # x = W wall
+        ((0, 0, 0), (W, 0, 0), (0, H, 0), white),              # z = 0 wall
+        ((0, 0, D), (0, H, 0), (W, 0, 0), white),              # z = D wall
+        # dividing wall at x = xw: left of the gap, right of the gap, above the gap
+        ((xw, 0, 0), (0, 0, gap_z0), (0, H, 0), white),
+        ((xw, 0, gap_z1), (0, 0, D - gap_z1), (0, H, 0), white),
+        ((xw, gap_h, gap_z0), (0, 0, gap_z1 - gap_z0), (0, H - gap_h, 0), white),
+    ]
+    for o, u, v, mat in quads:
+        nu = max(1, int(round(tess * np.linalg.norm(u) / 4.0 * 3)))
+        nv = max(1, int(round(tess * np.linalg.norm(v) / 4.0 * 3)))
+        verts, ix = _grid_quad(o, u, v, nu, nv)
+        sd.meshes.append(MeshData(verts.astype(np.float32), ix, mat))
+    # a few seed-placed boxes in the camera's room
+    for _ in range(3):
+        c = (rng.uniform(0.4, 2.0), 0.0, rng.uniform(0.5, 3.5))
+        s = (rng.uniform(0.2, 0.5), rng.uniform(0.3, 0.9), rng.uniform(0.2, 0.5))
+        v, ix = _box(c, s, rng.uniform(-0.5, 0.5))
+        sd.meshes.append(MeshData(v.astype(np.float32), ix, white))
+    side = float(np.sqrt(0.1))
+    sd.planes = [plane_make((3.25 - side / 2, 2.45, 2.0 - side / 2), (side, 0.0, 0.0), (0.0, 0.0, side))]
+    sd.area_lights = [((200.0, 200.0, 200.0), 0, 1, (0.0, 0.0, 0.0))]
+    sd.env_radiance = (0.0, 0.0, 0.0)
+    cam = camera_from_config((0.15, 1.3, 0.25), (2.5, 1.0, 2.2), (0.0, 1.0, 0.0), (36.0, 20.25), 24.0, 1e30)
+    sd.settings = render_settings(width, height, spp, max_depth, min_rr_depth, cam)
+    return sd
+
+
+def _icosphere(subdiv: int):
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in v]
+    for _ in range(subdiv):
+        cache = {}
+        nf = []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    return np.array(verts), np.array(f, dtype=np.uint32)
+
+
+def _fbm(x, z, rng_offsets, octaves=6):
+    h = np.zeros_like(x)
+    amp, freq = 0.5, 1.0
+    for o in range(octaves):
+        ox, oz, ph = rng_offsets[o]
+        h += amp * np.sin(freq * 2.1 * x + ox) * np.cos(freq * 1.7 * z + oz) + amp * 0.5 * np.sin(freq * 3.3 * (x + z) + ph)
+        amp *= 0.5
+        freq *= 2.0
+    return h
+
+
+def mixed_materials(seed: int = 0, width: int = 1920, height: int = 1080, spp: int = 64, max_depth: int = 16,
+                    min_rr_depth: int = 5, grid: int = 1024, n_spheres: int = 200) -> SceneData:
+    """Mixed-material scene: a grid x grid heightfield terrain (2 grid^2 triangles) from 6-octave fBm, with
+    n_spheres translated subdivision-4 icospheres (5120 triangles each) whose material is drawn per sphere:
+    GGX conductor (alpha U[0.05, 0.5]), smooth dielectric (IOR 1.5, the reference's Glass) or Lambert
+    (albedo U[0.1, 0.9]).  Constant environment 0.5 and one small sun-like area light."""
+    rng = np.random.default_rng(seed)
+    sd = SceneData(name=f"mixed_materials(seed={seed})")
+    sd.materials = [material("Matte", (0.35, 0.32, 0.28, 1.0))]
+    size = 40.0
+    xs = np.linspace(-size / 2, size / 2, grid + 1)
+    X, Z = np.meshgrid(xs, xs, indexing="ij")
+    offs = rng.uniform(0, 6.28, size=(6, 3))
+    Y = 1.5 * _fbm(X / 8.0, Z / 8.0, offs)
+    verts = np.stack([X, Y, Z], axis=-1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(grid), np.arange(grid), indexing="ij")
+    p00 = (i * (grid + 1) + j).ravel()
+    p10 = p00 + (grid + 1)
+    ix = np.stack([np.stack([p00, p10 + 1, p10], 1), np.stack([p00, p00 + 1, p10 + 1], 1)], 1).reshape(-1, 3)
+    sd.meshes.append(MeshData(verts.astype(np.float32), ix.astype(np.uint32), 0))
+    sv, sf = _icosphere(4)
+    for k in range(n_spheres):
+        r = rng.uniform(0.3, 1.0)
+        px, pz = rng.uniform(-size / 2.5, size / 2.5, size=2)
+        py = float(1.5 * _fbm(np.array([px / 8.0]), np.array([pz / 8.0]), offs)[0]) + r
+        kind = rng.integers(0, 3)
+        if kind == 0:
+            a = rng.uniform(0.05, 0.5)
+            sd.materials.append(material("Conductor", color1=tuple(rng.uniform(0.5, 0.95, 3)) + (1.0,), roughness=(a, a)))
+        elif kind == 1:
+            sd.materials.append(material("Glass", (1, 1, 1, 1), (1, 1, 1, 1), (0.0, 0.0)))
+        else:
+            alb = rng.uniform(0.1, 0.9)
+            sd.materials.append(material("Matte", (alb, alb * rng.uniform(0.6, 1.0), alb * rng.uniform(0.6, 1.0), 1.0)))
+        sd.meshes.append(MeshData((sv * r).astype(np.float32), sf, len(sd.materials) - 1, (float(px), py, float(pz))))
+    sd.planes = [plane_make((-2.0, 30.0, -2.0), (4.0, 0.0, 0.0), (0.0, 0.0, 4.0))]
+    sd.area_lights = [((400.0, 380.0, 340.0), 0, 1, (0.0, 0.0, 0.0))]
+    sd.env_radiance = (0.5, 0.5, 0.5)
+    cam = camera_from_config((0.0, 8.0, -24.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), (36.0, 20.25), 28.0, 1e30)
+    sd.settings = render_settings(width, height, spp, max_depth, min_rr_depth, cam)
+    return sd

@@ -1,0 +1,235 @@
+"""Path-guiding kernels on the GPU against the float64 model (oracle/guide_ref.py).
+
+The network runs in bf16 (weights, encoded inputs and hidden activations rounded to bf16, fp32
+accumulation and outputs), so the forward pass is compared with a float64 evaluation that applies the
+same roundings (relative L2 error <= 5e-3) and with the unrounded float64 model (<= 5e-2).  The batch
+gradient is compared with a float64 backward pass that applies the kernel's bf16 roundings (cosine
+>= 0.9999, relative L2 <= 1e-2) and with the unrounded model (cosine >= 0.99); the Adam step exactly
+restates the update from the kernel's own gradient (1e-3 of the learning rate).  Guided rendering must stay unbiased: its image mean matches the plain integrator's
+within 4 standard errors."""
+import numpy as np
+import pytest
+
+import guide_ref as G
+from piper2_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _api():
+    from piper2_b200 import api
+
+    return api
+
+
+def bf16(x):
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32).astype(np.float64)
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _features(rng, n):
+    pos = rng.uniform(0, 1, (n, 3))
+    nrm = _unit(rng, n)
+    wo = _unit(rng, n)
+    f = np.zeros((n, 12), dtype=np.float32)
+    f[:, 0:3], f[:, 3:6], f[:, 6:9] = pos, nrm, wo
+    return f
+
+
+def _forward_bf16(params, f):
+    x = bf16(G.encode(f[:, 0:3].astype(np.float64), f[:, 3:6].astype(np.float64), f[:, 6:9].astype(np.float64)))
+    h = x
+    layers = G.unpack(np.asarray(params, dtype=np.float32))
+    for li, (W, b) in enumerate(layers):
+        z = h @ bf16(W).T + b.astype(np.float64)
+        h = bf16(np.maximum(z, 0.0)) if li < len(layers) - 1 else z
+    return h
+
+
+def _trained_params(seed):
+    """He-init weights with nonzero biases so every term of the forward pass matters."""
+    rng = np.random.default_rng(seed)
+    p = G.init_params(seed)
+    k = 0
+    for i, o in G.LAYERS:
+        k += o * i
+        p[k:k + o] = rng.normal(0, 0.1, o)
+        k += o
+    return p.astype(np.float32)
+
+
+@pytest.mark.parametrize("n", [1, 15, 16, 1000, 70001])
+def test_forward_matches_bf16_model(n):
+    api = _api()
+    rng = np.random.default_rng(n)
+    g = api.Guide(seed=11)
+    params = _trained_params(11)
+    g.set_params(params)
+    assert np.array_equal(g.get_params(), params)
+    f = _features(rng, n)
+    y = g.forward(f)
+    ref = _forward_bf16(params, f)
+    rel = np.linalg.norm(y[:, :40] - ref[:, :40]) / np.linalg.norm(ref[:, :40])
+    assert rel <= 5e-3, rel
+    full = G.forward(params.astype(np.float64),
+                     G.encode(f[:, 0:3].astype(np.float64), f[:, 3:6].astype(np.float64), f[:, 6:9].astype(np.float64)))
+    rel64 = np.linalg.norm(y[:, :40] - full[:, :40]) / np.linalg.norm(full[:, :40])
+    assert rel64 <= 5e-2, rel64
+
+
+def _records(rng, n, concentrated=False):
+    f = _features(rng, n)
+    wi = _unit(rng, n)
+    if concentrated:
+        mu = np.stack([np.cos(2 * np.pi * f[:, 0]), np.ones(n), np.sin(2 * np.pi * f[:, 0])], axis=1)
+        mu /= np.linalg.norm(mu, axis=1, keepdims=True)
+        wi = G.sample(_lobe_raw(mu), rng.uniform(0, 1, n), rng.uniform(0, 1, n), rng.uniform(0, 1, n))
+    rec = np.zeros((n, 16), dtype=np.float32)
+    rec[:, 0:9] = f[:, 0:9]
+    rec[:, 9:12] = wi
+    rec[:, 12] = rng.exponential(1.0, n) if not concentrated else 1.0
+    return rec
+
+
+def _lobe_raw(mu):
+    """Raw outputs of a single dominant lobe around mu with concentration ~20."""
+    n = len(mu)
+    y = np.zeros((n, 48))
+    y[:, 0] = 20.0
+    y[:, 1:4] = mu
+    y[:, 4] = 20.0  # softplus(20) + 0.05 ~ 20
+    return y
+
+
+def _gradient_bf16(params, rec):
+    """Float64 loss gradient applying the kernel's roundings: bf16 weights, inputs and activations, the
+    output delta and the back-propagated deltas rounded to bf16 before each GEMM (bias of the output layer
+    from the unrounded delta)."""
+    layers = [(bf16(W), b.astype(np.float64)) for W, b in G.unpack(np.asarray(params, dtype=np.float32))]
+    x = bf16(G.encode(rec[:, 0:3].astype(np.float64), rec[:, 3:6].astype(np.float64), rec[:, 6:9].astype(np.float64)))
+    hs = [x]
+    for W, b in layers[:-1]:
+        hs.append(bf16(np.maximum(hs[-1] @ W.T + b, 0.0)))
+    y = hs[-1] @ layers[-1][0].T + layers[-1][1]
+    wi = rec[:, 9:12].astype(np.float64)
+    loss, dy = G.loss_and_grad_y(y, wi, rec[:, 12].astype(np.float64))
+    grads = [None] * 5
+    d = bf16(dy)
+    grads[4] = (d.T @ hs[4], dy.sum(axis=0))
+    d = bf16((d @ layers[4][0]) * (hs[4] > 0))
+    for li in range(3, -1, -1):
+        gw = d.T @ hs[li]
+        gb = d.sum(axis=0)
+        grads[li] = (gw, gb)
+        if li > 0:
+            d = bf16((d @ layers[li][0]) * (hs[li] > 0))
+    return np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads]), loss
+
+
+@pytest.mark.parametrize("n", [1, 64, 5000])
+def test_gradient_matches_float64(n):
+    api = _api()
+    rng = np.random.default_rng(100 + n)
+    g = api.Guide(seed=5)
+    params = _trained_params(5)
+    g.set_params(params)
+    rec = _records(rng, n)
+    grad, loss = g.gradient(rec)
+    ref, ref_loss = _gradient_bf16(params, rec)
+    cos = float(grad @ ref / (np.linalg.norm(grad) * np.linalg.norm(ref)))
+    rel = float(np.linalg.norm(grad - ref) / np.linalg.norm(ref))
+    assert cos >= 0.9999 and rel <= 1e-2, (cos, rel)
+    assert abs(loss - ref_loss) <= 1e-3 * abs(ref_loss) + 1e-4, (loss, ref_loss)
+    # against the unrounded model: the size of the bf16 error itself
+    p64 = params.astype(np.float64)
+    x = G.encode(rec[:, 0:3].astype(np.float64), rec[:, 3:6].astype(np.float64), rec[:, 6:9].astype(np.float64))
+    y, acts = G.forward(p64, x, keep=True)
+    _, dy = G.loss_and_grad_y(y, rec[:, 9:12].astype(np.float64), rec[:, 12].astype(np.float64))
+    full = G.backward(p64, acts, dy)
+    cos64 = float(grad @ full / (np.linalg.norm(grad) * np.linalg.norm(full)))
+    assert cos64 >= 0.99, cos64
+
+
+def test_adam_step_restates_update():
+    api = _api()
+    rng = np.random.default_rng(9)
+    g = api.Guide(seed=3)
+    params = _trained_params(3)
+    g.set_params(params)
+    rec = _records(rng, 4096)
+    grad, _ = g.gradient(rec)
+    lr = 1e-3
+    g.train(rec, learning_rate=lr)
+    p1 = g.get_params()
+    # first Adam step: m^ = g, v^ = g^2 -> update = -lr g / (|g| + eps); accumulation order of the
+    # gradient differs between the two calls, so compare where |g| is well above eps and rounding
+    upd = p1.astype(np.float64) - params
+    exp = -lr * grad / (np.abs(grad) + 1e-8)
+    big = np.abs(grad) > 1e-5
+    assert big.mean() > 0.5
+    assert np.max(np.abs(upd[big] - exp[big])) <= 1e-3 * lr + 1e-7 * np.abs(params[big]).max()
+
+
+def test_training_reduces_the_loss():
+    api = _api()
+    rng = np.random.default_rng(12)
+    g = api.Guide(seed=21)
+    first = None
+    losses = []
+    for step in range(300):
+        rec = _records(rng, 4096, concentrated=True)
+        loss = g.train(rec, learning_rate=5e-3)
+        if first is None:
+            first = loss
+        losses.append(loss)
+    late = float(np.mean(losses[-20:]))
+    # uniform density gives log(4 pi) = 2.53; a vMF with kappa 20 reaches about -0.15
+    assert first > 1.0
+    assert late < first - 1.5, (first, late)
+
+
+def _mean_and_se(pl):
+    film, samples = pl.render(samples=True)
+    rad = samples[..., 2:5].reshape(-1, 3).astype(np.float64)
+    return rad.mean(axis=0), rad.std(axis=0) / np.sqrt(len(rad))
+
+
+def test_guided_render_is_unbiased():
+    api = _api()
+    sd = scenes.cornell_box(seed=0, width=128, height=128, spp=16, max_depth=8)
+    with api.Pipeline(sd) as pl:
+        m0, s0 = _mean_and_se(pl)
+    g = api.Guide(seed=2)
+    with api.Pipeline(sd) as pl:
+        pl.set_guide(g, selection_prob=0.5, record_capacity=1 << 17)
+        # a few rounds of online training so the guide is far from uniform
+        for it in range(4):
+            film = pl.new_film()
+            pl.launch(film, sample_begin=0, sample_count=4)
+            loss = pl.train_guide(steps=20, batch=4096, learning_rate=5e-3)
+            assert np.isfinite(loss) and loss != 0.0
+        m1, s1 = _mean_and_se(pl)
+    se = np.sqrt(s0 ** 2 + s1 ** 2)
+    assert np.all(np.abs(m1 - m0) <= 4 * se + 1e-6), (m0, m1, se)
+
+
+def test_guide_settings_are_checked():
+    api = _api()
+    from piper2_b200 import capi
+
+    sd = scenes.cornell_box(seed=0, width=16, height=16, spp=1, max_depth=8)
+    g = api.Guide(seed=1)
+    with api.Pipeline(sd) as pl:
+        for bad in (0.0, 1.0, -0.5):
+            with pytest.raises(capi.PB2Error):
+                pl.set_guide(g, selection_prob=bad)
+        with pytest.raises(capi.PB2Error):
+            pl.set_guide(g, record_capacity=0)
+        with pytest.raises(capi.PB2Error):
+            pl.train_guide(steps=1)

@@ -139,3 +139,44 @@ def test_counters_and_invalid_arguments():
         assert nv >= 1000 and nt > 0
         with pytest.raises(capi.PB2Error):
             capi.check(capi.lib().pb2_trace_closest(acc.h, None, 10, None, None))
+
+
+def _structure_scenes():
+    return {
+        "soup_1": scenes.triangle_soup(1, seed=2),
+        "soup_9": scenes.triangle_soup(9, seed=2),
+        "soup_100k": scenes.triangle_soup(100_000, seed=2),
+        "cornell": scenes.cornell_box(seed=0),
+        "guiding_room": scenes.guiding_room(seed=0, width=64, height=36),
+    }
+
+
+@pytest.mark.parametrize("name", ["soup_1", "soup_9", "soup_100k", "cornell", "guiding_room"])
+def test_bvh_structure_validates(name):
+    """Every child and triangle index in range and reached once; every triangle inside its child box."""
+    sd = _structure_scenes()[name]
+    with _api().Accel(sd) as acc:
+        acc.validate()
+        info = acc.info()
+        assert info.triangle_count == sum(len(m.indices) for m in sd.meshes)
+
+
+def test_guiding_room_traversal_vs_oracle(oracle):
+    """Axis-aligned, coplanar, tessellated walls: closest and any hit against the oracle's BVH."""
+    sd = scenes.guiding_room(seed=0, width=64, height=36)
+    rng = np.random.default_rng(4)
+    n = 100_000
+    rays = np.zeros(n, dtype=capi.RAY_DTYPE)
+    rays["org"] = rng.uniform((0.05, 0.05, 0.05), (3.95, 2.45, 3.95), size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d[: n // 10] = np.round(d[: n // 10])  # some axis-aligned and diagonal directions
+    d[np.all(d == 0, axis=1)] = (0.0, 1.0, 0.0)
+    rays["dir"] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays["tmin"] = 1e-3
+    rays["tmax"] = 1e5
+    o = oracle.OracleScene(sd, use_bvh=True)
+    with _api().Accel(sd) as acc:
+        acc.validate()
+        h = acc.trace_closest(rays)
+        _assert_hits_equal(h, o.trace_closest(rays))
+        assert np.array_equal(acc.trace_any(rays), o.trace_any(rays))
