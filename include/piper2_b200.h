@@ -307,14 +307,17 @@ int pb2_guide_train(pb2_guide* guide, const float* records_dev, uint32_t n, floa
                     void* stream);
 
 typedef struct pb2_guide_settings {
-    float selection_prob;      /* probability of sampling the guide at a non-specular vertex (0.5) */
-    uint32_t record_capacity;  /* training records kept per launch (e.g. 262144) */
+    float selection_prob;      /* probability of sampling the guide at a guided vertex (0.5) */
+    uint32_t record_capacity;  /* training records kept between two training calls (e.g. 2^20) */
+    float weight_quantile;     /* training weights are clamped at this quantile of the call's records
+                                  (e.g. 0.99; 0 or 1 = no clamp) */
 } pb2_guide_settings;
 
 /* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */
 int pb2_pipeline_set_guide(pb2_pipeline* pipeline, pb2_guide* guide, const pb2_guide_settings* settings);
-/* Runs `steps` Adam steps of `batch` records drawn from the records of the launches since the last call,
- * then clears them.  Writes the last step's loss. */
+/* Runs `steps` Adam steps of `batch` records drawn uniformly from the records of the launches since the
+ * last call (weights clamped per pb2_guide_settings.weight_quantile), then clears them.  Writes the last
+ * step's loss. */
 int pb2_pipeline_train_guide(pb2_pipeline* pipeline, uint32_t steps, uint32_t batch, float learning_rate,
                              float* loss_host, void* stream);
 

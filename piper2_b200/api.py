@@ -183,22 +183,22 @@ class Pipeline:
         capi.check(capi.lib().pb2_pipeline_get_stats(self.h, C.byref(s), _stream()))
         return s
 
-    def set_guide(self, guide, selection_prob=0.5, record_capacity=1 << 18):
+    def set_guide(self, guide, selection_prob=0.5, record_capacity=1 << 20, weight_quantile=0.99):
         """Attach a :class:`Guide` (None detaches); later launches sample and record with it."""
         self._guide = guide
         if guide is None:
             capi.check(capi.lib().pb2_pipeline_set_guide(self.h, None, None))
             return
-        st = capi.GuideSettings(float(selection_prob), int(record_capacity))
+        st = capi.GuideSettings(float(selection_prob), int(record_capacity), float(weight_quantile))
         capi.check(capi.lib().pb2_pipeline_set_guide(self.h, guide.h, C.byref(st)))
 
-    def train_guide(self, steps, batch=4096, learning_rate=5e-3) -> float:
+    def train_guide(self, steps, batch=1 << 16, learning_rate=1e-2) -> float:
         """Adam steps on the records of the launches since the last call; returns the last loss."""
         loss = C.c_float(0.0)
         capi.check(capi.lib().pb2_pipeline_train_guide(self.h, steps, batch, learning_rate, C.byref(loss), _stream()))
         return loss.value
 
-    def render_guided(self, film, spp, spp_per_pass=4, train_steps=16, batch=8192, learning_rate=5e-3,
+    def render_guided(self, film, spp, spp_per_pass=4, train_steps=4, batch=1 << 16, learning_rate=1e-2,
                       train_passes=None, rect=None, sample_begin=0):
         """Progressive guided render: `spp / spp_per_pass` launches into `film`, each followed (for the first
         `train_passes`, default all) by `train_steps` Adam steps on the records it produced.  Every pass is

@@ -104,7 +104,7 @@ _lib = None
 
 # (name, restype, argtypes) for every entry point declared in include/piper2_b200.h
 class GuideSettings(C.Structure):
-    _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32)]
+    _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32), ("weight_quantile", C.c_float)]
 
 
 SIGNATURES = [

@@ -834,8 +834,22 @@ __global__ void __launch_bounds__(guide::kThreads) k_guide_infer(SceneView sv, P
     (void)slots16;
 }
 
+// log2 histogram of the training records' weights (64 bins, exponent -32 .. 31)
+__global__ void k_weight_hist(const float* __restrict__ rec, uint32_t count, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[64];
+    if (threadIdx.x < 64) h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int e = (int)((__float_as_uint(rec[16 * (size_t)i + 12]) >> 23) & 0xFFu) - 127;
+        atomicAdd(&h[min(max(e + 32, 0), 63)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 64 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+// a training batch drawn uniformly from the records, weights clamped at `clamp`
 __global__ void k_gather_batch(const float* __restrict__ src, uint32_t count, float* __restrict__ dst, uint32_t batch,
-                               uint32_t salt) {
+                               uint32_t salt, float clamp) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= batch) return;
     const uint32_t j = hash32(i * 0x27d4eb2du + salt) % count;
@@ -844,7 +858,9 @@ __global__ void k_gather_batch(const float* __restrict__ src, uint32_t count, fl
     d4[0] = s4[0];
     d4[1] = s4[1];
     d4[2] = s4[2];
-    d4[3] = s4[3];
+    float4 w = s4[3];
+    w.x = fminf(w.x, clamp);
+    d4[3] = w;
 }
 
 // ---- finish: add the vertex's MIS estimate, then re-queue or splat --------------------------------
@@ -1451,6 +1467,8 @@ int pb2_pipeline_set_guide(pb2_pipeline* pl, pb2_guide* guide, const pb2_guide_s
         return fail(PB2_ERR_INVALID_ARGUMENT, "selection_prob must lie in (0, 1): the BxDF keeps the estimator unbiased");
     if (settings->record_capacity == 0 || settings->record_capacity > (1u << 26))
         return fail(PB2_ERR_INVALID_ARGUMENT, "record_capacity must lie in [1, 2^26]");
+    if (!(settings->weight_quantile >= 0.0f && settings->weight_quantile <= 1.0f))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "weight_quantile must lie in [0, 1]");
     if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
         return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
     cudaError_t e;
@@ -1488,12 +1506,35 @@ int pb2_pipeline_train_guide(pb2_pipeline* pl, uint32_t steps, uint32_t batch, f
             cudaFree(pl->g_batch);
             pl->g_batch = nullptr;
             pl->g_batch_capacity = 0;
-            if ((e = cudaMalloc(&pl->g_batch, (size_t)batch * 64))) return cuda_fail(e, "cudaMalloc batch");
+            if ((e = cudaMalloc(&pl->g_batch, (size_t)batch * 64 + 64 * sizeof(uint32_t))))
+                return cuda_fail(e, "cudaMalloc batch");
             pl->g_batch_capacity = batch;
+        }
+        // weight clamp at the configured quantile of this call's records (log2 bins): a few extreme
+        // radiance samples must not dominate a batch's self-normalised loss
+        float clamp = 3.0e38f;
+        const float q = pl->guide_settings.weight_quantile;
+        if (q > 0.0f && q < 1.0f) {
+            uint32_t* hist = reinterpret_cast<uint32_t*>(pl->g_batch + (size_t)batch * 16);
+            uint32_t h[64];
+            if ((e = cudaMemsetAsync(hist, 0, sizeof(h), stream))) return cuda_fail(e, "memset histogram");
+            k_weight_hist<<<pl->sms, 256, 0, stream>>>(pl->g_train, count, hist);
+            if ((e = cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, stream)) ||
+                (e = cudaStreamSynchronize(stream)))
+                return cuda_fail(e, "weight histogram");
+            uint64_t cum = 0;
+            const uint64_t target = (uint64_t)std::ceil((double)q * count);
+            for (int b = 0; b < 64; ++b) {
+                cum += h[b];
+                if (cum >= target) {
+                    clamp = std::ldexp(1.0f, b - 32 + 1);
+                    break;
+                }
+            }
         }
         for (uint32_t s = 0; s < steps; ++s) {
             k_gather_batch<<<(batch + 255) / 256, 256, 0, stream>>>(pl->g_train, count, pl->g_batch, batch,
-                                                                    ++pl->g_salt * 0x85ebca6bu);
+                                                                    ++pl->g_salt * 0x85ebca6bu, clamp);
             if ((e = cudaGetLastError())) return cuda_fail(e, "k_gather_batch");
             const int rc = pb2_guide_train(pl->guide, pl->g_batch, batch, lr, s + 1 == steps ? &loss : nullptr, stream_ptr);
             if (rc) return rc;

@@ -34,8 +34,9 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def evaluate(width=640, height=360, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=16, batch=8192,
-             learning_rate=5e-3, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64):
+def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
+             learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
+             weight_quantile=0.99):
     import torch
 
     from . import api, scenes
@@ -55,10 +56,10 @@ def evaluate(width=640, height=360, spp=64, ref_spp=1024, spp_per_pass=4, train_
         plain = pl.resolve(film).cpu().numpy().astype(np.float64)
         # guided: fresh network, progressive passes with online training
         guide = api.Guide(seed=seed + 1)
-        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20)
+        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile)
         film = pl.new_film()
         t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
-                                                                 learning_rate))
+                                                                 learning_rate, train_passes))
         guided = pl.resolve(film).cpu().numpy().astype(np.float64)
         pl.set_guide(None)
     e_plain, e_guided = rel_mse(plain, ref), rel_mse(guided, ref)
@@ -66,6 +67,7 @@ def evaluate(width=640, height=360, spp=64, ref_spp=1024, spp_per_pass=4, train_
         "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
                    "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,
+                   "train_passes": train_passes, "learning_rate": learning_rate, "weight_quantile": weight_quantile,
                    "first_loss": losses[0] if losses else None, "last_loss": losses[-1] if losses else None},
         "reference_mean": float(ref.mean()),
         "relmse_ratio": e_plain / e_guided if e_guided > 0 else None,
@@ -76,19 +78,22 @@ def evaluate(width=640, height=360, spp=64, ref_spp=1024, spp_per_pass=4, train_
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--width", type=int, default=640)
-    ap.add_argument("--height", type=int, default=360)
+    ap.add_argument("--width", type=int, default=1280)
+    ap.add_argument("--height", type=int, default=720)
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--ref-spp", type=int, default=1024)
     ap.add_argument("--spp-per-pass", type=int, default=4)
-    ap.add_argument("--train-steps", type=int, default=16)
-    ap.add_argument("--batch", type=int, default=8192)
-    ap.add_argument("--lr", type=float, default=5e-3)
+    ap.add_argument("--train-steps", type=int, default=4)
+    ap.add_argument("--train-passes", type=int, default=None)
+    ap.add_argument("--batch", type=int, default=1 << 16)
+    ap.add_argument("--lr", type=float, default=1e-2)
     ap.add_argument("--selection-prob", type=float, default=0.5)
+    ap.add_argument("--weight-quantile", type=float, default=0.99)
     ap.add_argument("--tess", type=int, default=15)
     a = ap.parse_args()
     print(json.dumps(evaluate(a.width, a.height, a.spp, a.ref_spp, a.spp_per_pass, a.train_steps, a.batch, a.lr,
-                              a.selection_prob, tess=a.tess)))
+                              a.selection_prob, tess=a.tess, train_passes=a.train_passes,
+                              weight_quantile=a.weight_quantile)))
 
 
 if __name__ == "__main__":
