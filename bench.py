@@ -261,40 +261,45 @@ def run_ours(args):
     print(json.dumps(line))
 
 
+def _render_rate(pl, rect, spp, chunk, frames=1):
+    """Device time of `frames` full renders of `rect` at `spp`, launched `chunk` samples at a time."""
+    import torch
+
+    film = pl.new_film()
+    pl.launch(film, rect, 0, min(chunk, spp))
+    torch.cuda.synchronize()
+    s0 = pl.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(frames):
+        for b in range(0, spp, chunk):
+            pl.launch(film, rect, b, min(chunk, spp - b))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s1 = pl.stats()
+    rays = (s1.closest_rays - s0.closest_rays) + (s1.shadow_rays - s0.shadow_rays)
+    samples = rect.width * rect.height * spp * frames
+    return {"samples_per_s": round(samples / (ms * 1e-3), 1), "mrays_per_s": round(rays / (ms * 1e-3) / 1e6, 2),
+            "ms_per_frame": round(ms / frames, 3), "rays_per_sample": round(rays / samples, 3)}
+
+
 def render_bench(args):
-    """The render path on the Cornell-box configuration (256 x 256, 16 spp, depth 8, NEE + MIS): device time
-    of full-frame launches, against the reference's own kernels compiled natively (oracle/_ref) on all
-    host cores over a bounded crop."""
+    """The render path: the Cornell-box configuration (256 x 256, 16 spp, depth 8) against the reference's own
+    kernels compiled natively (oracle/_ref) on all host cores over a bounded crop; the mixed-materials
+    configuration (3.1M triangles, 1920 x 1080, 64 spp, depth 16); guided vs plain on the hard-indirect room
+    at reduced size."""
     import torch
 
     import oracle_py
 
-    from piper2_b200 import api, capi, scenes
+    from piper2_b200 import api, capi, guiding_eval, scenes
 
     sd = scenes.cornell_box(seed=0)
     st = sd.settings
-    samples_per_frame = st.width * st.height * st.samples_per_pixel
     with api.Pipeline(sd) as pl:
-        film = pl.new_film()
-        for _ in range(3):
-            pl.launch(film)
-        torch.cuda.synchronize()
-        s0 = pl.stats()
-        c0, h0 = s0.closest_rays, s0.shadow_rays
-        frames = max(3, args.steps // 2)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(frames):
-            pl.launch(film)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        s1 = pl.stats()
-        rays = (s1.closest_rays - c0) + (s1.shadow_rays - h0)
-    out = {"workload": "Cornell box 256x256, 16 spp, max depth 8, NEE+MIS (plain BxDF sampling)",
-           "samples_per_s": round(samples_per_frame * frames / (ms * 1e-3), 1),
-           "mrays_per_s": round(rays / (ms * 1e-3) / 1e6, 2), "ms_per_frame": round(ms / frames, 3),
-           "rays_per_sample": round(rays / (samples_per_frame * frames), 3)}
+        out = {"workload": "Cornell box 256x256, 16 spp, max depth 8, NEE+MIS (plain BxDF sampling)"}
+        out.update(_render_rate(pl, pl.rect, st.samples_per_pixel, st.samples_per_pixel, frames=max(3, args.steps // 2)))
     if oracle_py.ref_available():
         crop = capi.Rect(0, 96, 256, 16)
         rs = oracle_py.RefScene(sd, use_bvh=True)
@@ -306,7 +311,17 @@ def render_bench(args):
         out["cpu_baseline"] = {"value": round(n / dt, 1), "unit": "samples/s", "cores": threads, "kind": "reference",
                                "sample": "rows 96-111 of the frame (65,536 samples) through the reference's own "
                                          "kernels compiled natively, CPU BVH in place of Embree"}
-    return out
+    result = {"cornell": out}
+    md = scenes.mixed_materials(seed=0)
+    with api.Pipeline(md) as pl:
+        mm = {"workload": "mixed materials 1920x1080, 64 spp, max depth 16, 3.1M triangles (terrain + 200 "
+                          "icospheres: Lambert / smooth dielectric / GGX conductor), env 0.5 + sun"}
+        mm.update(_render_rate(pl, pl.rect, md.settings.samples_per_pixel, 8))
+    result["mixed_materials"] = mm
+    torch.cuda.empty_cache()
+    g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512)
+    result["guiding"] = g
+    return result
 
 
 def cpu_baseline(soup, crays, arays, args, sample=None):
