@@ -321,6 +321,40 @@ int pb2_pipeline_set_guide(pb2_pipeline* pipeline, pb2_guide* guide, const pb2_g
 int pb2_pipeline_train_guide(pb2_pipeline* pipeline, uint32_t steps, uint32_t batch, float learning_rate,
                              float* loss_host, void* stream);
 
+/* ---- batched multi-scene rendering (no reference counterpart: the reference renders one scene per
+ * pipeline and frame, FixedSampler.cpp:68-133) -----------------------------------------------------
+ * All scenes share one wavefront of path slots: a slot whose path is splatted is refilled from one global
+ * (scene, pixel, sample) index space, so scenes and films of uneven size keep every launch full.  Each path
+ * is the one a single-scene launch of the full frame traces for that (pixel, sample); films match per-scene
+ * renders within accumulation rounding.  Two wavefront iterations run as one captured CUDA graph on the
+ * batch's own stream, ordered after the caller's stream. */
+typedef struct pb2_batch pb2_batch;
+typedef struct pb2_batch_config {
+    uint32_t capacity;            /* path slots in flight, [1024, 2^26] */
+    uint32_t shade_block;         /* threads per block of the shading kernels (64/128/256/512) */
+    uint32_t trace_blocks_per_sm; /* resident blocks per SM of the persistent traversal kernels */
+    uint32_t use_graph;           /* 1: replay the captured iteration graph, 0: plain launches */
+} pb2_batch_config;
+
+/* One pipeline per (scene, settings) pair; spp per scene as in pb2_render_settings. */
+int pb2_batch_create(const pb2_scene* scenes, const pb2_render_settings* settings, uint32_t count, void* stream,
+                     pb2_batch** out);
+int pb2_batch_destroy(pb2_batch* batch);
+int pb2_batch_get_config(const pb2_batch* batch, pb2_batch_config* config);
+int pb2_batch_set_config(pb2_batch* batch, const pb2_batch_config* config);
+/* Times short runs of candidate configurations (capacity, then shading block, then traversal blocks per
+ * SM) and keeps the fastest; writes it and the tuning time. */
+int pb2_batch_autotune(pb2_batch* batch, void* stream, pb2_batch_config* chosen, float* tune_ms);
+/* Clears the films and renders every scene's samples; returns when they are done. */
+int pb2_batch_render(pb2_batch* batch, void* stream);
+/* Device pointer of scene `scene`'s RGBW film (width x height float4) and its size. */
+int pb2_batch_film(const pb2_batch* batch, uint32_t scene, float** rgbw_dev, uint32_t* width, uint32_t* height);
+/* Per-scene completion time (ms after the render started, device clock) of the last render, its total
+ * device time and the number of wavefront iterations. */
+int pb2_batch_timing(const pb2_batch* batch, float* scene_ms, uint32_t count, float* total_ms,
+                     uint32_t* iterations);
+int pb2_batch_get_stats(const pb2_batch* batch, pb2_launch_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

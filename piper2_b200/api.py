@@ -5,6 +5,8 @@
 * :class:`Pipeline`  -- ``Tracer::buildPipeline`` -> ``Pipeline::prepare`` -> ``TraceLauncher::launch``
   (Src/Interface/BuiltinComponent/Tracer.hpp:100-159) and the FixedSampler film resolve
   (Src/BuiltinComponent/RenderDriver/FixedSampler/FixedSampler.cpp:68-133).
+* :class:`Batch`     -- many scenes of uneven size rendered through one shared wavefront (no counterpart in
+  the reference, which renders one scene per pipeline).
 * :class:`Guide`     -- the learned path-guiding network (no counterpart in the reference: its
   PathTracing integrator samples BxDFs only), attached with :meth:`Pipeline.set_guide`.
 
@@ -210,6 +212,95 @@ class Pipeline:
             if train_steps and (train_passes is None or p < train_passes) and p + 1 < passes:
                 losses.append(self.train_guide(train_steps, batch, learning_rate))
         return losses
+
+
+class _DeviceArray:
+    """A float32 device buffer owned by the library, seen by torch through the CUDA array interface."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+
+class Batch:
+    """Scenes rendered together: one wavefront of path slots refilled from all scenes' (pixel, sample) space."""
+
+    def __init__(self, scene_datas, settings=None):
+        torch = _torch()
+        torch.cuda.init()
+        self.scene_datas = list(scene_datas)
+        n = len(self.scene_datas)
+        self._conv = [sd.to_ctypes() for sd in self.scene_datas]
+        self._scenes = (capi.Scene * n)(*[c[0] for c in self._conv])
+        sts = settings if settings is not None else [sd.settings for sd in self.scene_datas]
+        self._settings = (capi.RenderSettings * n)(*sts)
+        h = C.c_void_p()
+        capi.check(capi.lib().pb2_batch_create(C.cast(self._scenes, C.c_void_p), C.cast(self._settings, C.c_void_p),
+                                               n, _stream(), C.byref(h)))
+        self.h = h
+        self.count = n
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().pb2_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def config(self) -> capi.BatchConfig:
+        c = capi.BatchConfig()
+        capi.check(capi.lib().pb2_batch_get_config(self.h, C.byref(c)))
+        return c
+
+    def set_config(self, **kw):
+        c = self.config
+        for k, v in kw.items():
+            setattr(c, k, int(v))
+        capi.check(capi.lib().pb2_batch_set_config(self.h, C.byref(c)))
+
+    def autotune(self):
+        """Picks capacity and launch shapes by timing short runs; returns (config, tuning ms)."""
+        c = capi.BatchConfig()
+        ms = C.c_float(0.0)
+        capi.check(capi.lib().pb2_batch_autotune(self.h, _stream(), C.byref(c), C.byref(ms)))
+        return c, ms.value
+
+    def render(self):
+        capi.check(capi.lib().pb2_batch_render(self.h, _stream()))
+
+    def film(self, i):
+        """Scene i's RGBW film as a numpy array (H x W x 4)."""
+        torch = _torch()
+        ptr = C.c_void_p()
+        w, h = C.c_uint32(), C.c_uint32()
+        capi.check(capi.lib().pb2_batch_film(self.h, i, C.byref(ptr), C.byref(w), C.byref(h)))
+        view = torch.as_tensor(_DeviceArray(ptr.value, (h.value, w.value, 4)), device="cuda")
+        torch.cuda.synchronize()
+        return view.cpu().numpy()
+
+    def timing(self):
+        """(per-scene completion ms, total device ms, wavefront iterations) of the last render."""
+        ms = np.zeros(self.count, dtype=np.float32)
+        tot = C.c_float(0.0)
+        it = C.c_uint32(0)
+        capi.check(capi.lib().pb2_batch_timing(self.h, ms.ctypes.data_as(C.c_void_p), self.count, C.byref(tot),
+                                               C.byref(it)))
+        return ms, tot.value, it.value
+
+    def stats(self) -> capi.LaunchStats:
+        s = capi.LaunchStats()
+        capi.check(capi.lib().pb2_batch_get_stats(self.h, C.byref(s)))
+        return s
 
 
 class Guide:

@@ -103,6 +103,11 @@ class PB2Error(RuntimeError):
 _lib = None
 
 # (name, restype, argtypes) for every entry point declared in include/piper2_b200.h
+class BatchConfig(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("shade_block", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
+                ("use_graph", C.c_uint32)]
+
+
 class GuideSettings(C.Structure):
     _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32), ("weight_quantile", C.c_float)]
 
@@ -140,6 +145,16 @@ SIGNATURES = [
     ("pb2_pipeline_get_stats", C.c_int, [C.c_void_p, C.POINTER(LaunchStats), C.c_void_p]),
     ("pb2_pipeline_camera_rays", C.c_int, [C.c_void_p, C.POINTER(Rect), C.c_uint32, C.c_void_p, C.c_void_p,
                                             C.c_void_p]),
+    ("pb2_batch_create", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("pb2_batch_destroy", C.c_int, [C.c_void_p]),
+    ("pb2_batch_get_config", C.c_int, [C.c_void_p, C.POINTER(BatchConfig)]),
+    ("pb2_batch_set_config", C.c_int, [C.c_void_p, C.POINTER(BatchConfig)]),
+    ("pb2_batch_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(BatchConfig), C.POINTER(C.c_float)]),
+    ("pb2_batch_render", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pb2_batch_film", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    ("pb2_batch_timing", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
+    ("pb2_batch_get_stats", C.c_int, [C.c_void_p, C.POINTER(LaunchStats)]),
     ("pb2_guide_param_count", C.c_uint32, []),
     ("pb2_guide_create", C.c_int, [C.c_uint32, C.POINTER(C.c_void_p)]),
     ("pb2_guide_destroy", C.c_int, [C.c_void_p]),

@@ -9,6 +9,8 @@
 // All per-path arithmetic is the reference's (PathTracing/Kernel.cpp:23-193) in its operation order,
 // so each path's radiance equals the CPU oracle's bit for bit; only the film sums, which use
 // atomics in any order (as the reference's CAS loop does), differ in rounding.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -78,6 +80,7 @@ enum : int {
     C_EXT_CUR = 0, C_EXT_NEXT = 1, C_SHADOW = 2, C_MIS = 3, C_SHADED = 4, C_SURF0 = 5,  // 5..11 per type
     C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24,
     C_CHECK = 25,  // 25..28: first failed index check (code, kernel, slot, value)
+    C_FREE0 = 29,  // 29, 30: batched launches, slots freed (ping-pong with the extend queues)
     C_COUNT = 32
 };
 
@@ -111,6 +114,9 @@ struct Paths {
     uint32_t* mis_q;
     uint32_t* shaded_q;
     uint32_t* counts;  // C_COUNT entries
+    // batched launches: scene of each slot, freed-slot queues
+    uint32_t* scene;
+    uint32_t* free_q[2];
 };
 
 struct LaunchParams {
@@ -158,6 +164,57 @@ struct GuideState {
     float bmin[3], binv[3];
 };
 
+// Where a kernel finds the launch parameters, scene and film of a path slot.
+// One scene per launch: everything is a kernel parameter.
+struct SingleCtx {
+    static constexpr bool kBatch = false;
+    LaunchParams lp;
+    SceneView sv;
+    float4* film;
+    float* sample_out;
+    __device__ __forceinline__ const LaunchParams& P(uint32_t) const { return lp; }
+    __device__ __forceinline__ const SceneView& S(uint32_t) const { return sv; }
+    __device__ __forceinline__ const BvhView& bvh(uint32_t) const { return sv.bvh; }
+    __device__ __forceinline__ float4* film_of(uint32_t) const { return film; }
+    __device__ __forceinline__ uint32_t capacity() const { return lp.path_count; }
+    __device__ __forceinline__ bool checks() const { return lp.checks != 0u; }
+};
+
+// Many scenes per launch: each slot carries its scene; the scene table is in device memory.
+struct BatchScene {
+    LaunchParams lp;      // rect = full frame, sample_begin 0, sample_count = the scene's spp
+    SceneView sv;
+    float4* film;
+    uint64_t path_begin;  // first global path index of the scene
+    uint64_t path_count;  // width x height x spp
+};
+struct BatchState {
+    unsigned long long next;   // next global path index to generate
+    unsigned long long total;  // sum of the scenes' path counts
+    unsigned long long claim_begin;
+    uint32_t claim_count;
+    uint32_t claim_base;       // extend-queue position of the first regenerated path
+    unsigned long long t_start;
+};
+struct BatchCtx {
+    static constexpr bool kBatch = true;
+    const BatchScene* scenes;
+    uint32_t scene_count;
+    uint32_t cap;
+    uint32_t check;
+    uint32_t* remaining;          // per scene: paths not yet splatted
+    unsigned long long* done_ns;  // per scene: %globaltimer when its last path was splatted
+    BatchState* state;
+    const uint32_t* scene_of;     // = Paths::scene
+    __device__ __forceinline__ const BatchScene& B(uint32_t slot) const { return scenes[scene_of[slot]]; }
+    __device__ __forceinline__ const LaunchParams& P(uint32_t slot) const { return B(slot).lp; }
+    __device__ __forceinline__ const SceneView& S(uint32_t slot) const { return B(slot).sv; }
+    __device__ __forceinline__ const BvhView& bvh(uint32_t slot) const { return B(slot).sv.bvh; }
+    __device__ __forceinline__ float4* film_of(uint32_t slot) const { return B(slot).film; }
+    __device__ __forceinline__ uint32_t capacity() const { return cap; }
+    __device__ __forceinline__ bool checks() const { return check != 0u; }
+};
+
 // ---- helpers ----------------------------------------------------------------------------------------
 
 // Warp-aggregated queue append: the active lanes that push to the same counter (lanes may push to
@@ -188,7 +245,7 @@ __device__ __noinline__ void check_failed(uint32_t* counts, uint32_t code, uint3
     }
 }
 #define PB2_CHECK(cond, code, kernel, slot, v)                              \
-    if (lp.checks && !(cond)) {                                             \
+    if (ctx.checks() && !(cond)) {                                          \
         check_failed(ps.counts, (code), (kernel), (uint32_t)(slot), (uint32_t)(v)); \
         continue;                                                           \
     }
@@ -288,8 +345,9 @@ constexpr int kQSteps = 4;
 
 enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
 
-template <int kKind>
-__global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(BvhView bvh, Paths ps, const uint32_t* __restrict__ queue,
+template <int kKind, class Ctx>
+__global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(const __grid_constant__ Ctx ctx, Paths ps,
+                                                           const uint32_t* __restrict__ queue,
                                                            const uint32_t* __restrict__ count_ptr, uint32_t* work,
                                                            unsigned long long* stat) {
     constexpr bool kClosest = kKind != Q_SHADOW;
@@ -299,6 +357,8 @@ __global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(BvhView bvh, Path
     tr.bind_stack(stack_smem);
     bool active = false;
     uint32_t slot = 0;
+    BvhView bvh{};
+    if constexpr (!Ctx::kBatch) bvh = ctx.bvh(0);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
     uint32_t rays = 0;
@@ -313,6 +373,7 @@ __global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(BvhView bvh, Path
                 const uint32_t idx = base + __popc(inactive & lt_mask);
                 if (idx < n) {
                     slot = queue[idx];
+                    if constexpr (Ctx::kBatch) bvh = ctx.bvh(slot);
                     float4 a, b;
                     if (kKind == Q_EXTEND) {
                         a = ps.o[slot]; b = ps.d[slot];
@@ -380,14 +441,28 @@ __device__ __forceinline__ void splat(const LaunchParams& lp, float4* film, floa
     }
 }
 
-__device__ __forceinline__ void terminate_path(const LaunchParams& lp, const Paths& ps, uint32_t slot, float4* film,
-                                               float* sample_out) {
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A finished path: splat its radiance; in a batched launch also free its slot and count the scene down.
+template <class Ctx>
+__device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, uint32_t slot, uint32_t cur) {
     const float4 r = ps.rad[slot];
     const float2 pt = ps.point[slot];
-    if (film) splat(lp, film, pt.x, pt.y, mksp(r.x, r.y, r.z));
-    if (sample_out) {
-        float* o = sample_out + 5 * (size_t)slot;
-        o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
+    float4* film = ctx.film_of(slot);
+    if (film) splat(ctx.P(slot), film, pt.x, pt.y, mksp(r.x, r.y, r.z));
+    if constexpr (Ctx::kBatch) {
+        const uint32_t scene = ps.scene[slot];
+        ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
+        if (atomicSub(&ctx.remaining[scene], 1u) == 1u) ctx.done_ns[scene] = globaltimer();
+    } else {
+        if (ctx.sample_out) {
+            float* o = ctx.sample_out + 5 * (size_t)slot;
+            o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
+        }
     }
 }
 
@@ -434,13 +509,15 @@ __device__ __forceinline__ void flush_records(const GuideState& gs, uint32_t slo
 
 // ---- classify extend results (PathTracing/Kernel.cpp:116-149) ------------------------------------
 
-__global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur, float4* film,
-                           float* sample_out) {
+template <class Ctx>
+__global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_EXT_CUR];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        PB2_CHECK(n <= lp.path_count, 1, K_CLASSIFY, 0, n);
+        PB2_CHECK(n <= ctx.capacity(), 1, K_CLASSIFY, 0, n);
         const uint32_t slot = ps.ext[cur][i];
-        PB2_CHECK(slot < lp.path_count, 2, K_CLASSIFY, slot, i);
+        PB2_CHECK(slot < ctx.capacity(), 2, K_CLASSIFY, slot, i);
+        const LaunchParams& lp = ctx.P(slot);
+        const SceneView& sv = ctx.S(slot);
         const float4 h = ps.hit[slot];
         const uint32_t prim = __float_as_uint(h.y);
         PB2_CHECK(prim == kInvalidPrim || ((prim & kPlaneFlag) ? (prim & ~kPlaneFlag) < sv.bvh.plane_count
@@ -482,7 +559,7 @@ __global__ void k_classify(LaunchParams lp, SceneView sv, Paths ps, GuideState g
         }
         if (missing || ps.depth[slot] >= lp.max_depth) {
             if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
-            terminate_path(lp, ps, slot, film, sample_out);
+            terminate_path(ctx, ps, slot, cur);
             continue;
         }
         PB2_CHECK(sv.prim_material[prim] < sv.material_count, 4, K_CLASSIFY, slot, sv.prim_material[prim]);
@@ -586,14 +663,16 @@ __device__ __forceinline__ v3 to_local(const Frame& f, v3 v) {
 // a pdf that is not their sampler's density (Classic/Kernel.cpp:405-412), so they keep plain BxDF sampling.
 __host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_MATTE || t == PB2_SURFACE_CONDUCTOR; }
 
-template <int kType>
-__global__ void k_shade(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur) {
+template <int kType, class Ctx>
+__global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        PB2_CHECK(n <= lp.path_count, 10, K_SHADE, 0, n);
+        PB2_CHECK(n <= ctx.capacity(), 10, K_SHADE, 0, n);
         const uint32_t slot = ps.surf[kType][i];
-        PB2_CHECK(slot < lp.path_count, 11, K_SHADE, slot, i);
+        PB2_CHECK(slot < ctx.capacity(), 11, K_SHADE, slot, i);
+        const LaunchParams& lp = ctx.P(slot);
+        const SceneView& sv = ctx.S(slot);
         ++vertices;
         const float4 h = ps.hit[slot];
         const uint32_t prim = __float_as_uint(h.y);
@@ -865,13 +944,15 @@ __global__ void k_gather_batch(const float* __restrict__ src, uint32_t count, fl
 
 // ---- finish: add the vertex's MIS estimate, then re-queue or splat --------------------------------
 
-__global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, GuideState gs, uint32_t cur, float4* film,
-                         float* sample_out) {
+template <class Ctx>
+__global__ void k_finish(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_SHADED];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        PB2_CHECK(n <= lp.path_count, 20, K_FINISH, 0, n);
+        PB2_CHECK(n <= ctx.capacity(), 20, K_FINISH, 0, n);
         const uint32_t slot = ps.shaded_q[i];
-        PB2_CHECK(slot < lp.path_count, 21, K_FINISH, slot, i);
+        PB2_CHECK(slot < ctx.capacity(), 21, K_FINISH, slot, i);
+        const LaunchParams& lp = ctx.P(slot);
+        const SceneView& sv = ctx.S(slot);
         const uint32_t flags = ps.flags[slot];
         PB2_CHECK(!(flags & 4u) || __float_as_uint(ps.mhit[slot].y) == kInvalidPrim ||
                       ((__float_as_uint(ps.mhit[slot].y) & kPlaneFlag)
@@ -930,8 +1011,78 @@ __global__ void k_finish(LaunchParams lp, SceneView sv, Paths ps, GuideState gs,
             ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
         } else {
             if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
-            terminate_path(lp, ps, slot, film, sample_out);
+            terminate_path(ctx, ps, slot, cur);
         }
+    }
+}
+
+// ---- batched launches: slot regeneration from one global path index space ------------------------
+
+__global__ void k_batch_init(Paths ps, uint32_t cap, BatchState* st, unsigned long long total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cap) {
+        ps.free_q[0][i] = i;
+        ps.scene[i] = 0;
+    }
+    if (i == 0) {
+        ps.counts[C_FREE0] = cap;
+        ps.counts[C_FREE0 + 1] = 0;
+        st->next = 0;
+        st->total = total;
+        st->claim_count = 0;
+    }
+}
+
+// Start of the timed region of a batched render (the per-scene completion times are relative to it).
+__global__ void k_batch_clock(BatchState* st) { st->t_start = globaltimer(); }
+
+// Claims min(free slots, paths left) new paths for iteration `cur` and reserves their extend-queue places;
+// clears the traversal work counters of the iteration.
+__global__ void k_batch_claim(Paths ps, BatchState* st, uint32_t cur, uint32_t* work) {
+    const uint32_t f = ps.counts[C_FREE0 + cur];
+    ps.counts[C_FREE0 + cur] = 0;
+    const unsigned long long left = st->total - st->next;
+    const uint32_t m = left < (unsigned long long)f ? (uint32_t)left : f;
+    st->claim_begin = st->next;
+    st->claim_count = m;
+    st->next += m;
+    st->claim_base = ps.counts[C_EXT_CUR];
+    ps.counts[C_EXT_CUR] += m;
+    work[0] = work[1] = work[2] = 0;
+}
+
+// Starts the claimed paths in the freed slots: the same camera path a single-scene launch of the full frame
+// starts for that (pixel, sample).
+__global__ void k_batch_regen(const __grid_constant__ BatchCtx ctx, Paths ps, uint32_t cur) {
+    const BatchState& st = *ctx.state;
+    const uint32_t m = st.claim_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ps.free_q[cur][i];
+        const unsigned long long g = st.claim_begin + i;
+        uint32_t lo = 0, hi = ctx.scene_count;  // last scene with path_begin <= g
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (ctx.scenes[mid].path_begin <= g) lo = mid;
+            else hi = mid;
+        }
+        const BatchScene& sc = ctx.scenes[lo];
+        const LaunchParams& lp = sc.lp;
+        uint32_t sx, sy, smp;
+        path_coords(lp, (uint32_t)(g - sc.path_begin), sx, sy, smp);
+        uint64_t index;
+        float px, py;
+        v3 o, d;
+        primary_ray(lp, sx, sy, smp, index, px, py, o, d);
+        ps.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+        ps.d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        ps.pf[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        ps.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.sidx[slot] = index;
+        ps.dim[slot] = 5;
+        ps.depth[slot] = 0;
+        ps.point[slot] = make_float2(px, py);
+        ps.scene[slot] = lo;
+        ps.ext[cur][st.claim_base + i] = slot;
     }
 }
 
@@ -1024,33 +1175,20 @@ static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
 
 static size_t infer_smem() { return (size_t)guide::kW16Elems * 2 + guide::kBiasElems * 4 + guide::kWarps * sizeof(guide::FwdTile); }
 
-static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
-    if (pl->capacity >= cap) return PB2_OK;
-    cudaFree(pl->state);
-    pl->state = nullptr;
-    pl->capacity = 0;
-    const size_t c = cap;
-    size_t bytes = 0;
-    auto sz = [&](size_t b) { bytes += ((b + 255) / 256) * 256; };
-    // 14 float4 arrays, sidx, dim, depth, point, hit_slot, mr_pdf, flags, occ, queues (2 + types + 3), counts
-    sz(c * 16 * 14); sz(c * 8); sz(c * 4); sz(c * 4); sz(c * 8); sz(c * 4); sz(c * 8); sz(c * 4); sz(c * 4);
-    for (int q = 0; q < 2 + kNumSurfaceTypes + 3; ++q) sz(c * 4);
-    sz(sizeof(uint32_t) * C_COUNT);
-    cudaError_t e = cudaMalloc(&pl->state, bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc path state");
-    char* p = static_cast<char*>(pl->state);
+// Carves the SoA path state of `c` slots out of `base` (or only measures it when base is null); returns the
+// bytes used.  `batch` adds the per-slot scene ids and the two freed-slot queues.
+static size_t carve_paths(char* base, size_t c, bool batch, Paths& s) {
+    char* p = base;
     auto carve = [&](size_t b) {
         void* r = p;
         p += ((b + 255) / 256) * 256;
         return r;
     };
-    Paths& s = pl->ps;
     s.o = (float4*)carve(c * 16); s.d = (float4*)carve(c * 16); s.pf = (float4*)carve(c * 16);
     s.rad = (float4*)carve(c * 16); s.hit = (float4*)carve(c * 16); s.mis_pf = (float4*)carve(c * 16);
     s.nee = (float4*)carve(c * 16); s.sh_o = (float4*)carve(c * 16); s.sh_d = (float4*)carve(c * 16);
     s.mr_o = (float4*)carve(c * 16); s.mr_d = (float4*)carve(c * 16); s.mr_f = (float4*)carve(c * 16);
     s.mhit = (float4*)carve(c * 16);
-    carve(c * 16);  // spare
     s.sidx = (unsigned long long*)carve(c * 8);
     s.dim = (uint32_t*)carve(c * 4);
     s.depth = (uint32_t*)carve(c * 4);
@@ -1066,8 +1204,33 @@ static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
     s.mis_q = (uint32_t*)carve(c * 4);
     s.shaded_q = (uint32_t*)carve(c * 4);
     s.counts = (uint32_t*)carve(sizeof(uint32_t) * C_COUNT);
-    pl->capacity = cap;
+    if (batch) {
+        s.scene = (uint32_t*)carve(c * 4);
+        s.free_q[0] = (uint32_t*)carve(c * 4);
+        s.free_q[1] = (uint32_t*)carve(c * 4);
+    } else {
+        s.scene = nullptr;
+        s.free_q[0] = s.free_q[1] = nullptr;
+    }
+    return (size_t)(p - base);
+}
+
+static int alloc_path_state(void** mem, uint32_t* capacity, Paths* ps, uint32_t cap, bool batch) {
+    if (*capacity >= cap) return PB2_OK;
+    cudaFree(*mem);
+    *mem = nullptr;
+    *capacity = 0;
+    Paths probe{};
+    const size_t bytes = carve_paths(nullptr, cap, batch, probe);
+    cudaError_t e = cudaMalloc(mem, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc path state");
+    carve_paths(static_cast<char*>(*mem), cap, batch, *ps);
+    *capacity = cap;
     return PB2_OK;
+}
+
+static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
+    return alloc_path_state(&pl->state, &pl->capacity, &pl->ps, cap, false);
 }
 
 static float remap_roughness(float roughness) {
@@ -1364,7 +1527,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     static int qblocks = 0;
     if (!qblocks) {
         int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND>, kQThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0);
         qblocks = pl->sms * (per > 0 ? per : 1);
     }
     uint32_t cur = 0;
@@ -1385,6 +1548,11 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         }
     };
     checked("k_generate");
+    SingleCtx ctx;
+    ctx.lp = lp;
+    ctx.sv = sv;
+    ctx.film = film;
+    ctx.sample_out = sample_out;
     for (int bounce = 0; !failed; ++bounce) {
         uint32_t active = 0;
         if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
@@ -1394,33 +1562,33 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
         const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
         cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
-        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(sv.bvh, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
+        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
                                                                  stats);
         checked("k_trace_queue<extend>");
-        k_classify<<<grid, 256, 0, stream>>>(lp, sv, ps, gs, cur, film, sample_out);
+        k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_classify");
         if (gs.enabled) k_guide_infer<<<pl->sms, guide::kThreads, infer_smem(), stream>>>(sv, ps, gs);
         checked("k_guide_infer");
-        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<matte>");
-        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<plastic>");
-        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<glass>");
-        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<mirror>");
-        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<substrate>");
-        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<conductor>");
-        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(lp, sv, ps, gs, cur);
+        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<blackbody>");
-        k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
+        k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
                                                                    sstats);
         checked("k_trace_queue<shadow>");
-        k_trace_queue<Q_MIS><<<qblocks, kQThreads, 0, stream>>>(sv.bvh, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats);
+        k_trace_queue<Q_MIS><<<qblocks, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats);
         checked("k_trace_queue<mis>");
-        k_finish<<<grid, 256, 0, stream>>>(lp, sv, ps, gs, cur, film, sample_out);
+        k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_finish");
         k_advance<<<1, 1, 0, stream>>>(ps.counts);
         checked("k_advance");
@@ -1558,6 +1726,416 @@ int pb2_film_resolve(const float* rgbw, uint32_t n, float* rgb, void* stream) {
 int pb2_pipeline_get_stats(const pb2_pipeline* pl, pb2_launch_stats* stats, void*) {
     if (!pl || !stats) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_get_stats: null argument");
     *stats = pl->stats;
+    return PB2_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================================================
+// batched multi-scene rendering
+// ====================================================================================================
+
+struct pb2_batch {
+    std::vector<pb2_pipeline*> pipes;
+    std::vector<BatchScene> host_scenes;
+    std::vector<size_t> film_offset;  // float4 elements
+    BatchScene* scenes = nullptr;
+    uint32_t* remaining = nullptr;
+    unsigned long long* done_ns = nullptr;
+    BatchState* state = nullptr;
+    uint32_t* work = nullptr;
+    float4* films = nullptr;
+    size_t film_elems = 0;
+    unsigned long long total_paths = 0;
+    // path state
+    void* mem = nullptr;
+    uint32_t allocated = 0;  // slots the path state was carved for
+    uint32_t capacity = 0;   // slots the current config may use (<= allocated)
+    Paths ps{};
+    pb2_batch_config config{};
+    int sms = 0;
+    int trace_blocks_max = 0;
+    // the batch's own non-blocking stream: graphs cannot be captured on the legacy default stream
+    cudaStream_t own = nullptr;
+    // captured graph of two wavefront iterations (cur = 0 then 1) for `graph_config`
+    cudaGraphExec_t graph = nullptr;
+    pb2_batch_config graph_config{};
+    // results of the last render
+    std::vector<float> scene_ms;
+    float total_ms = 0.0f;
+    uint32_t iterations = 0;
+    pb2_launch_stats stats{};
+};
+
+static void batch_release_graph(pb2_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+static BatchCtx batch_ctx(const pb2_batch* b) {
+    BatchCtx c;
+    c.scenes = b->scenes;
+    c.scene_count = (uint32_t)b->pipes.size();
+    c.cap = b->capacity;
+    c.check = make_params(b->pipes[0], b->pipes[0]->full, 0, 1).checks;
+    c.remaining = b->remaining;
+    c.done_ns = b->done_ns;
+    c.state = b->state;
+    c.scene_of = b->ps.scene;
+    return c;
+}
+
+// One wavefront iteration over every scene: regenerate freed slots, then one bounce.
+static cudaError_t batch_iteration(pb2_batch* b, uint32_t cur, cudaStream_t stream) {
+    const BatchCtx ctx = batch_ctx(b);
+    const Paths& ps = b->ps;
+    GuideState gs{};
+    const int grid = b->sms * 8;
+    const int sb = (int)b->config.shade_block;
+    const int tb = b->sms * (int)b->config.trace_blocks_per_sm;
+    unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
+    unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
+    k_batch_claim<<<1, 1, 0, stream>>>(ps, b->state, cur, b->work);
+    k_batch_regen<<<grid, 256, 0, stream>>>(ctx, ps, cur);
+    k_trace_queue<Q_EXTEND><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, b->work, stats);
+    k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_MATTE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_PLASTIC><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_GLASS><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_MIRROR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_SUBSTRATE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_CONDUCTOR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_shade<PB2_SURFACE_BLACKBODY><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    k_trace_queue<Q_SHADOW><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, b->work + 1, sstats);
+    k_trace_queue<Q_MIS><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, b->work + 2, stats);
+    k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+    k_advance<<<1, 1, 0, stream>>>(ps.counts);
+    return cudaGetLastError();
+}
+
+static bool same_config(const pb2_batch_config& a, const pb2_batch_config& b) {
+    return a.capacity == b.capacity && a.shade_block == b.shade_block &&
+           a.trace_blocks_per_sm == b.trace_blocks_per_sm;
+}
+
+// Resets films, counters and the path index space for a render with the current config.
+static int batch_reset(pb2_batch* b, cudaStream_t stream) {
+    if (b->allocated < b->config.capacity) {
+        batch_release_graph(b);  // the graph holds pointers into the old path state
+        const int rc = alloc_path_state(&b->mem, &b->allocated, &b->ps, b->config.capacity, true);
+        if (rc) return rc;
+    }
+    if (b->capacity != b->config.capacity) batch_release_graph(b);
+    b->capacity = b->config.capacity;
+    cudaError_t e;
+    std::vector<uint32_t> rem(b->pipes.size());
+    for (size_t i = 0; i < b->pipes.size(); ++i) rem[i] = (uint32_t)b->host_scenes[i].path_count;
+    if ((e = cudaMemsetAsync(b->films, 0, sizeof(float4) * b->film_elems, stream)) ||
+        (e = cudaMemsetAsync(b->ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream)) ||
+        (e = cudaMemsetAsync(b->done_ns, 0, sizeof(unsigned long long) * b->pipes.size(), stream)) ||
+        (e = cudaMemcpyAsync(b->remaining, rem.data(), sizeof(uint32_t) * rem.size(), cudaMemcpyHostToDevice, stream)))
+        return cuda_fail(e, "batch reset");
+    k_batch_init<<<(b->capacity + 255) / 256, 256, 0, stream>>>(b->ps, b->capacity, b->state, b->total_paths);
+    if ((e = cudaGetLastError())) return cuda_fail(e, "k_batch_init");
+    // the host copy of `rem` must outlive the asynchronous copy
+    if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "batch reset sync");
+    return PB2_OK;
+}
+
+// Runs iterations until every path of every scene is splatted (or `max_iterations` when non-zero).
+static int batch_run(pb2_batch* b, cudaStream_t stream, uint32_t max_iterations, float* ms_out) {
+    cudaError_t e;
+    const bool use_graph = b->config.use_graph != 0;
+    if (use_graph && !(b->graph && same_config(b->graph_config, b->config))) {
+        batch_release_graph(b);
+        cudaGraph_t g;
+        if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal))) return cuda_fail(e, "begin capture");
+        cudaError_t le = batch_iteration(b, 0, stream);
+        if (le == cudaSuccess) le = batch_iteration(b, 1, stream);
+        e = cudaStreamEndCapture(stream, &g);
+        if (le != cudaSuccess || e != cudaSuccess) return cuda_fail(le != cudaSuccess ? le : e, "capture batch iteration");
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e) {
+            b->graph = nullptr;
+            return cuda_fail(e, "instantiate batch graph");
+        }
+        b->graph_config = b->config;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto done_events = [&]() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    };
+    cudaEventRecord(e0, stream);
+    k_batch_clock<<<1, 1, 0, stream>>>(b->state);
+    uint32_t it = 0;
+    const uint32_t check_every = 8;  // iterations between host checks of completion
+    // generous bound: every path needs at most (max depth + light pass-throughs) bounces
+    uint64_t per_path = 0;
+    for (auto* p : b->pipes) per_path = std::max<uint64_t>(per_path, 4ull * (p->settings.max_depth + 2) + 64);
+    const uint64_t max_it = (b->total_paths / std::max<uint32_t>(1u, b->capacity) + 2) * per_path;
+    for (;;) {
+        for (uint32_t k = 0; k < check_every; k += 2) {
+            if (use_graph) {
+                if ((e = cudaGraphLaunch(b->graph, stream))) {
+                    done_events();
+                    return cuda_fail(e, "graph launch");
+                }
+            } else if ((e = batch_iteration(b, 0, stream)) || (e = batch_iteration(b, 1, stream))) {
+                done_events();
+                return cuda_fail(e, "batch iteration");
+            }
+            it += 2;
+        }
+        uint32_t active = 0;
+        unsigned long long next = 0;
+        if ((e = cudaMemcpyAsync(&active, b->ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaMemcpyAsync(&next, &b->state->next, sizeof(next), cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaStreamSynchronize(stream))) {
+            done_events();
+            return cuda_fail(e, "batch progress");
+        }
+        if (active == 0 && next == b->total_paths) break;
+        if (max_iterations && it >= max_iterations) break;
+        if (it > max_it) {
+            done_events();
+            return fail(PB2_ERR_DEVICE_TIMEOUT, "batch did not finish");
+        }
+    }
+    cudaEventRecord(e1, stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    done_events();
+    b->iterations = it;
+    if (ms_out) *ms_out = ms;
+    uint32_t counts[C_COUNT];
+    if ((e = cudaMemcpy(counts, b->ps.counts, sizeof(counts), cudaMemcpyDeviceToHost))) return cuda_fail(e, "batch stats");
+    if (counts[C_CHECK])
+        return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
+                                      std::to_string(counts[C_CHECK + 1]) + " at slot " +
+                                      std::to_string(counts[C_CHECK + 2]) + ", value " +
+                                      std::to_string(counts[C_CHECK + 3]));
+    if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+    std::memcpy(&b->stats.closest_rays, counts + C_STAT_CLOSEST, 8);
+    std::memcpy(&b->stats.shadow_rays, counts + C_STAT_SHADOW, 8);
+    std::memcpy(&b->stats.path_vertices, counts + C_STAT_VERTICES, 8);
+    return PB2_OK;
+}
+
+// Orders the batch's stream after the caller's stream; the batch then works on its own stream and
+// synchronises it before returning.
+static int batch_stream(pb2_batch* b, void* stream_ptr, cudaStream_t* out) {
+    cudaError_t e;
+    if (!b->own && (e = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking))) return cuda_fail(e, "batch stream");
+    if ((e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream_ptr)))) return cuda_fail(e, "caller stream");
+    *out = b->own;
+    return PB2_OK;
+}
+
+extern "C" {
+
+int pb2_batch_create(const pb2_scene* scenes, const pb2_render_settings* settings, uint32_t count, void* stream_ptr,
+                     pb2_batch** out) {
+    if (!scenes || !settings || !out || count == 0) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_create: bad argument");
+    *out = nullptr;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    auto* b = new pb2_batch();
+    auto cleanup = [&](int code) {
+        pb2_batch_destroy(b);
+        return code;
+    };
+    for (uint32_t i = 0; i < count; ++i) {
+        pb2_pipeline* pl = nullptr;
+        const int rc = pb2_pipeline_create(&scenes[i], &settings[i], stream_ptr, &pl);
+        if (rc) return cleanup(rc);
+        b->pipes.push_back(pl);
+    }
+    size_t film = 0;
+    unsigned long long path = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        pb2_pipeline* pl = b->pipes[i];
+        BatchScene sc{};
+        sc.lp = make_params(pl, pl->full, 0, pl->settings.samples_per_pixel);
+        sc.sv.materials = pl->materials;
+        sc.sv.prim_material = pl->accel->prim_material;
+        sc.sv.lights = pl->lights;
+        sc.sv.plane_cdf = pl->plane_cdf;
+        sc.sv.plane_pdf = pl->plane_pdf;
+        sc.sv.bvh = pl->accel->view;
+        sc.sv.material_count = pl->material_count;
+        const unsigned long long n = (unsigned long long)pl->full.width * pl->full.height * pl->settings.samples_per_pixel;
+        if (n >= 0xFFFFFFFFull) return cleanup(fail(PB2_ERR_INVALID_ARGUMENT, "a batched scene has 2^32 paths or more"));
+        sc.path_begin = path;
+        sc.path_count = n;
+        path += n;
+        b->film_offset.push_back(film);
+        film += (size_t)pl->settings.width * pl->settings.height;
+        b->host_scenes.push_back(sc);
+    }
+    b->film_elems = film;
+    b->total_paths = path;
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->films, sizeof(float4) * film)) || (e = cudaMalloc(&b->scenes, sizeof(BatchScene) * count)) ||
+        (e = cudaMalloc(&b->remaining, sizeof(uint32_t) * count)) ||
+        (e = cudaMalloc(&b->done_ns, sizeof(unsigned long long) * count)) ||
+        (e = cudaMalloc(&b->state, sizeof(BatchState))) || (e = cudaMalloc(&b->work, sizeof(uint32_t) * 4)))
+        return cleanup(cuda_fail(e, "pb2_batch_create"));
+    for (uint32_t i = 0; i < count; ++i) b->host_scenes[i].film = b->films + b->film_offset[i];
+    if ((e = cudaMemcpyAsync(b->scenes, b->host_scenes.data(), sizeof(BatchScene) * count, cudaMemcpyHostToDevice,
+                             stream)) ||
+        (e = cudaStreamSynchronize(stream)))
+        return cleanup(cuda_fail(e, "upload batch scenes"));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND, BatchCtx>, kQThreads, 0);
+    b->trace_blocks_max = per > 0 ? per : 1;
+    b->config.capacity = (uint32_t)std::max<unsigned long long>(1024ull, std::min<unsigned long long>(path, 1ull << 22));
+    b->config.shade_block = 128;
+    b->config.trace_blocks_per_sm = (uint32_t)b->trace_blocks_max;
+    b->config.use_graph = 1;
+    b->scene_ms.assign(count, 0.0f);
+    *out = b;
+    return PB2_OK;
+}
+
+int pb2_batch_destroy(pb2_batch* b) {
+    if (!b) return PB2_OK;
+    batch_release_graph(b);
+    if (b->own) {
+        cudaStreamSynchronize(b->own);
+        cudaStreamDestroy(b->own);
+    }
+    for (auto* p : b->pipes) pb2_pipeline_destroy(p);
+    cudaFree(b->films);
+    cudaFree(b->scenes);
+    cudaFree(b->remaining);
+    cudaFree(b->done_ns);
+    cudaFree(b->state);
+    cudaFree(b->work);
+    cudaFree(b->mem);
+    delete b;
+    return PB2_OK;
+}
+
+int pb2_batch_get_config(const pb2_batch* b, pb2_batch_config* config) {
+    if (!b || !config) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_get_config: null argument");
+    *config = b->config;
+    return PB2_OK;
+}
+
+int pb2_batch_set_config(pb2_batch* b, const pb2_batch_config* c) {
+    if (!b || !c) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_set_config: null argument");
+    if (c->capacity < 1024 || c->capacity > (1u << 26))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "capacity must lie in [1024, 2^26] paths");
+    if (c->shade_block != 64 && c->shade_block != 128 && c->shade_block != 256 && c->shade_block != 512)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "shade_block must be 64, 128, 256 or 512");
+    if (c->trace_blocks_per_sm < 1 || c->trace_blocks_per_sm > (uint32_t)b->trace_blocks_max)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "trace_blocks_per_sm must lie in [1, resident blocks per SM]");
+    b->config = *c;
+    return PB2_OK;
+}
+
+int pb2_batch_render(pb2_batch* b, void* stream_ptr) {
+    if (!b) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_render: null batch");
+    cudaStream_t stream;
+    int rc = batch_stream(b, stream_ptr, &stream);
+    if (rc) return rc;
+    if ((rc = batch_reset(b, stream))) return rc;
+    float ms = 0.0f;
+    if ((rc = batch_run(b, stream, 0, &ms))) return rc;
+    std::vector<unsigned long long> done(b->pipes.size());
+    BatchState st{};
+    cudaError_t e;
+    if ((e = cudaMemcpy(done.data(), b->done_ns, sizeof(unsigned long long) * done.size(), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(&st, b->state, sizeof(st), cudaMemcpyDeviceToHost)))
+        return cuda_fail(e, "batch timing");
+    for (size_t i = 0; i < done.size(); ++i)
+        b->scene_ms[i] = done[i] >= st.t_start ? (float)((double)(done[i] - st.t_start) * 1e-6) : -1.0f;
+    b->total_ms = ms;
+    b->stats.paths = b->total_paths;
+    return PB2_OK;
+}
+
+int pb2_batch_autotune(pb2_batch* b, void* stream_ptr, pb2_batch_config* chosen, float* tune_ms) {
+    if (!b) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_autotune: null batch");
+    cudaStream_t stream;
+    if (const int rc = batch_stream(b, stream_ptr, &stream)) return rc;
+    const pb2_batch_config base = b->config;
+    // Candidates are scored by path vertices shaded per ms over a fixed number of iterations from a fresh
+    // start (the fill phase included, as in a real render): capacity first, then the launch shapes.
+    auto score = [&](const pb2_batch_config& c, double* out) -> int {
+        b->config = c;
+        int rc = batch_reset(b, stream);
+        if (rc) return rc;
+        float ms = 0.0f;
+        if ((rc = batch_run(b, stream, 24, &ms))) return rc;
+        *out = ms > 0.0f ? (double)b->stats.path_vertices / ms : 0.0;
+        return PB2_OK;
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    pb2_batch_config best = base;
+    double best_s = -1.0;
+    auto consider = [&](const pb2_batch_config& c) -> int {
+        double s = 0.0;
+        const int rc = score(c, &s);
+        if (rc) return rc;
+        if (s > best_s) {
+            best_s = s;
+            best = c;
+        }
+        return PB2_OK;
+    };
+    const uint32_t caps[] = { 1u << 20, 1u << 21, 1u << 22, 1u << 23 };
+    for (uint32_t cap : caps) {
+        if (cap > std::max<unsigned long long>(b->total_paths, 1u << 20)) break;
+        pb2_batch_config c = base;
+        c.capacity = cap;
+        if (const int rc = consider(c)) return rc;
+    }
+    for (uint32_t sb : { 64u, 256u }) {
+        pb2_batch_config c = best;
+        c.shade_block = sb;
+        if (const int rc = consider(c)) return rc;
+    }
+    for (uint32_t tb = (uint32_t)b->trace_blocks_max / 2; tb >= 1; tb /= 2) {
+        pb2_batch_config c = best;
+        c.trace_blocks_per_sm = tb;
+        if (const int rc = consider(c)) return rc;
+    }
+    b->config = best;
+    batch_release_graph(b);
+    if (chosen) *chosen = best;
+    if (tune_ms)
+        *tune_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return PB2_OK;
+}
+
+int pb2_batch_film(const pb2_batch* b, uint32_t scene, float** rgbw_dev, uint32_t* width, uint32_t* height) {
+    if (!b || scene >= b->pipes.size()) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_film: bad scene index");
+    if (rgbw_dev) *rgbw_dev = reinterpret_cast<float*>(b->films + b->film_offset[scene]);
+    if (width) *width = b->pipes[scene]->settings.width;
+    if (height) *height = b->pipes[scene]->settings.height;
+    return PB2_OK;
+}
+
+int pb2_batch_timing(const pb2_batch* b, float* scene_ms, uint32_t count, float* total_ms, uint32_t* iterations) {
+    if (!b || (scene_ms && count != b->pipes.size()))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_timing: count must equal the scene count");
+    if (scene_ms) std::memcpy(scene_ms, b->scene_ms.data(), sizeof(float) * count);
+    if (total_ms) *total_ms = b->total_ms;
+    if (iterations) *iterations = b->iterations;
+    return PB2_OK;
+}
+
+int pb2_batch_get_stats(const pb2_batch* b, pb2_launch_stats* stats) {
+    if (!b || !stats) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_batch_get_stats: null argument");
+    *stats = b->stats;
     return PB2_OK;
 }
 
