@@ -284,6 +284,53 @@ def _render_rate(pl, rect, spp, chunk, frames=1):
             "ms_per_frame": round(ms / frames, 3), "rays_per_sample": round(rays / samples, 3)}
 
 
+def batch_bench():
+    """64 scenes of uneven size (10k-2M triangles, 128-1024 px film side, 4-64 spp) through one batched
+    render: autotuned configuration, aggregate samples/s, per-scene completion percentiles; beside it the
+    same scenes rendered one after another through single-scene pipelines (device time of the launches)."""
+    import numpy as np
+    import torch
+
+    from piper2_b200 import api, scenes
+
+    sds = scenes.batch_workload(seed=0)
+    samples = sum(sd.settings.width * sd.settings.height * sd.settings.samples_per_pixel for sd in sds)
+    with api.Batch(sds) as b:
+        cfg, tune_ms = b.autotune()
+        b.render()  # warm-up
+        b.render()
+        ms, total, iters = b.timing()
+        st = b.stats()
+    out = {"workload": "64 scenes: mixed-materials generator, triangles log-uniform 10k-2M, film side log-uniform "
+                       "128-1024 (16:9), spp uniform 4-64 rounded up to a power of two, depth 16",
+           "triangles": sum(sum(len(m.indices) for m in sd.meshes) for sd in sds), "samples": samples,
+           "samples_per_s": round(samples / (total * 1e-3), 1), "ms": round(total, 2),
+           "mrays_per_s": round((st.closest_rays + st.shadow_rays) / (total * 1e-3) / 1e6, 2),
+           "scene_ms_p50": round(float(np.percentile(ms, 50)), 2), "scene_ms_p90": round(float(np.percentile(ms, 90)), 2),
+           "scene_ms_p99": round(float(np.percentile(ms, 99)), 2), "iterations": iters,
+           "config": {"capacity": cfg.capacity, "shade_block": cfg.shade_block,
+                      "trace_blocks_per_sm": cfg.trace_blocks_per_sm, "graph": bool(cfg.use_graph)},
+           "autotune_ms": round(tune_ms, 1)}
+    seq = 0.0
+    for sd in sds:
+        with api.Pipeline(sd) as pl:
+            spp = sd.settings.samples_per_pixel
+            film = pl.new_film()
+            pl.launch(film, pl.rect, 0, min(spp, 16))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for s0 in range(0, spp, 16):
+                pl.launch(film, pl.rect, s0, min(16, spp - s0))
+            e1.record()
+            torch.cuda.synchronize()
+            seq += e0.elapsed_time(e1)
+        torch.cuda.empty_cache()
+    out["sequential_single_scene_ms"] = round(seq, 2)
+    out["sequential_samples_per_s"] = round(samples / (seq * 1e-3), 1)
+    return out
+
+
 def render_bench(args):
     """The render path: the Cornell-box configuration (256 x 256, 16 spp, depth 8) against the reference's own
     kernels compiled natively (oracle/_ref) on all host cores over a bounded crop; the mixed-materials
@@ -318,6 +365,8 @@ def render_bench(args):
                           "icospheres: Lambert / smooth dielectric / GGX conductor), env 0.5 + sun"}
         mm.update(_render_rate(pl, pl.rect, md.settings.samples_per_pixel, 8))
     result["mixed_materials"] = mm
+    torch.cuda.empty_cache()
+    result["batch"] = batch_bench()
     torch.cuda.empty_cache()
     g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512)
     result["guiding"] = g

@@ -398,3 +398,25 @@ def mixed_materials(seed: int = 0, width: int = 1920, height: int = 1080, spp: i
     cam = camera_from_config((0.0, 8.0, -24.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), (36.0, 20.25), 28.0, 1e30)
     sd.settings = render_settings(width, height, spp, max_depth, min_rr_depth, cam)
     return sd
+
+
+def batch_workload(seed: int = 0, count: int = 64, max_depth: int = 16) -> list:
+    """The batching workload: `count` scenes from the mixed-materials generator, each with its own seed,
+    triangle count log-uniform in [10k, 2M] (terrain grid and icosphere count chosen to match), film side
+    log-uniform in [128, 1024] (16:9, the generator's sensor), and spp uniform in [4, 64] rounded up to a
+    power of two (the reference's sampler rounds the same way, ScrambledSobolSampler.cpp:43-50)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        tris = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        n_spheres = int(min(200, (0.3 * tris) // 5120))
+        grid = max(8, int(np.sqrt(max(tris - 5120 * n_spheres, 128) / 2)))
+        side = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        width, height = side, max(8, int(round(side * 9 / 16)))
+        spp = 1 << int(np.ceil(np.log2(rng.integers(4, 65))))
+        sd = mixed_materials(seed=seed * 1000 + k + 1, width=width, height=height, spp=spp, max_depth=max_depth,
+                             grid=grid, n_spheres=n_spheres)
+        sd.name = f"batch[{k}] {2 * grid * grid + 5120 * n_spheres} tris {width}x{height} {spp} spp"
+        out.append(sd)
+    return out
+
