@@ -10,9 +10,24 @@
 namespace pb2 {
 
 constexpr int kTraceThreads = 128;
-constexpr int kRefill = 4;
-constexpr int kSteps = 4;
-constexpr int kMinBlocks = 10;
+#ifndef PB2_TRACE_REFILL
+#define PB2_TRACE_REFILL 4
+#endif
+#ifndef PB2_TRACE_STEPS
+#define PB2_TRACE_STEPS 4
+#endif
+constexpr int kRefill = PB2_TRACE_REFILL;
+constexpr int kSteps = PB2_TRACE_STEPS;
+// Resident blocks per SM the register budget is sized for, closest hit / any hit (tuned on a B200:
+// 10 / 9 of 8-12 tried).
+#ifndef PB2_TRACE_MIN_BLOCKS
+#define PB2_TRACE_MIN_BLOCKS 10
+#endif
+#ifndef PB2_TRACE_MIN_BLOCKS_ANY
+#define PB2_TRACE_MIN_BLOCKS_ANY 9
+#endif
+constexpr int kMinBlocks = PB2_TRACE_MIN_BLOCKS;
+constexpr int kMinBlocksAny = PB2_TRACE_MIN_BLOCKS_ANY;
 
 struct ApiRays {
     const float4* rays;
@@ -25,7 +40,7 @@ struct ApiRays {
 };
 
 template <bool kClosest, bool kCount>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_trace_api(BvhView bvh, ApiRays io, uint32_t n, uint32_t* work,
+__global__ void __launch_bounds__(kTraceThreads, kClosest ? kMinBlocks : kMinBlocksAny) k_trace_api(BvhView bvh, ApiRays io, uint32_t n, uint32_t* work,
                                                               unsigned long long* counters, uint32_t* error_flag) {
     __shared__ uint2 stack_smem[kSharedStack * kTraceThreads];
     Traverser<kClosest, kCount, kTraceThreads> tr;
