@@ -311,6 +311,8 @@ typedef struct pb2_guide_settings {
     uint32_t record_capacity;  /* training records kept between two training calls (e.g. 2^20) */
     float weight_quantile;     /* training weights are clamped at this quantile of the call's records
                                   (e.g. 0.99; 0 or 1 = no clamp) */
+    uint32_t spatial_cells;    /* before clamping, each record's weight is divided by the mean weight of its
+                                  cell in a spatial_cells^3 grid over the scene box (0 = off, at most 16) */
 } pb2_guide_settings;
 
 /* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */

@@ -109,7 +109,8 @@ class BatchConfig(C.Structure):
 
 
 class GuideSettings(C.Structure):
-    _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32), ("weight_quantile", C.c_float)]
+    _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32), ("weight_quantile", C.c_float),
+                ("spatial_cells", C.c_uint32)]
 
 
 SIGNATURES = [

@@ -148,6 +148,7 @@ struct SceneView {
 
 // Guided sampling state of a launch (all pointers device memory, indexed by path slot unless noted).
 constexpr int kMaxRecords = 3;  // pending training records per path (its first guided vertices)
+constexpr uint32_t kMaxCells = 16 * 16 * 16;  // spatial cells of the training-weight normalisation
 struct GuideState {
     uint32_t enabled;
     float sel_prob;
@@ -913,6 +914,33 @@ __global__ void __launch_bounds__(guide::kThreads) k_guide_infer(SceneView sv, P
     (void)slots16;
 }
 
+// Per spatial cell (res^3 cells over the scene box) sum and count of the records' weights.
+__global__ void k_cell_sums(const float* __restrict__ rec, uint32_t count, uint32_t res, float* __restrict__ sum,
+                            uint32_t* __restrict__ cnt) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float* r = rec + 16 * (size_t)i;
+        uint32_t c[3];
+        for (int k = 0; k < 3; ++k) c[k] = min((uint32_t)fmaxf(r[k] * (float)res, 0.0f), res - 1u);
+        const uint32_t cell = (c[2] * res + c[1]) * res + c[0];
+        atomicAdd(&sum[cell], r[12]);
+        atomicAdd(&cnt[cell], 1u);
+    }
+}
+
+// Divides each record's weight by its cell's mean weight, so every region of the scene has a comparable
+// share of the loss however bright it is.
+__global__ void k_cell_normalize(float* __restrict__ rec, uint32_t count, uint32_t res, const float* __restrict__ sum,
+                                 const uint32_t* __restrict__ cnt) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        float* r = rec + 16 * (size_t)i;
+        uint32_t c[3];
+        for (int k = 0; k < 3; ++k) c[k] = min((uint32_t)fmaxf(r[k] * (float)res, 0.0f), res - 1u);
+        const uint32_t cell = (c[2] * res + c[1]) * res + c[0];
+        const float mean = sum[cell] / (float)cnt[cell];
+        if (mean > 0.0f) r[12] = r[12] / mean;
+    }
+}
+
 // log2 histogram of the training records' weights (64 bins, exponent -32 .. 31)
 __global__ void k_weight_hist(const float* __restrict__ rec, uint32_t count, uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[64];
@@ -1637,6 +1665,8 @@ int pb2_pipeline_set_guide(pb2_pipeline* pl, pb2_guide* guide, const pb2_guide_s
         return fail(PB2_ERR_INVALID_ARGUMENT, "record_capacity must lie in [1, 2^26]");
     if (!(settings->weight_quantile >= 0.0f && settings->weight_quantile <= 1.0f))
         return fail(PB2_ERR_INVALID_ARGUMENT, "weight_quantile must lie in [0, 1]");
+    if (settings->spatial_cells > 16)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "spatial_cells must lie in [0, 16] per axis");
     if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
         return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
     cudaError_t e;
@@ -1674,9 +1704,18 @@ int pb2_pipeline_train_guide(pb2_pipeline* pl, uint32_t steps, uint32_t batch, f
             cudaFree(pl->g_batch);
             pl->g_batch = nullptr;
             pl->g_batch_capacity = 0;
-            if ((e = cudaMalloc(&pl->g_batch, (size_t)batch * 64 + 64 * sizeof(uint32_t))))
+            if ((e = cudaMalloc(&pl->g_batch, (size_t)batch * 64 + 64 * sizeof(uint32_t) + kMaxCells * 8)))
                 return cuda_fail(e, "cudaMalloc batch");
             pl->g_batch_capacity = batch;
+        }
+        const uint32_t res = pl->guide_settings.spatial_cells;
+        if (res > 0) {
+            float* csum = reinterpret_cast<float*>(pl->g_batch + (size_t)batch * 16 + 64);
+            uint32_t* ccnt = reinterpret_cast<uint32_t*>(csum + kMaxCells);
+            if ((e = cudaMemsetAsync(csum, 0, kMaxCells * 8, stream))) return cuda_fail(e, "memset cells");
+            k_cell_sums<<<pl->sms * 4, 256, 0, stream>>>(pl->g_train, count, res, csum, ccnt);
+            k_cell_normalize<<<pl->sms * 4, 256, 0, stream>>>(pl->g_train, count, res, csum, ccnt);
+            if ((e = cudaGetLastError())) return cuda_fail(e, "cell normalisation");
         }
         // weight clamp at the configured quantile of this call's records (log2 bins): a few extreme
         // radiance samples must not dominate a batch's self-normalised loss

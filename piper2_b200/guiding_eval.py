@@ -36,7 +36,7 @@ def rel_mse(img, ref):
 
 def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
-             weight_quantile=0.99):
+             weight_quantile=0.99, spatial_cells=0):
     import torch
 
     from . import api, scenes
@@ -56,7 +56,8 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
         plain = pl.resolve(film).cpu().numpy().astype(np.float64)
         # guided: fresh network, progressive passes with online training
         guide = api.Guide(seed=seed + 1)
-        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile)
+        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile,
+                     spatial_cells=spatial_cells)
         film = pl.new_film()
         t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
                                                                  learning_rate, train_passes))
@@ -68,6 +69,7 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
                    "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,
                    "train_passes": train_passes, "learning_rate": learning_rate, "weight_quantile": weight_quantile,
+                   "spatial_cells": spatial_cells,
                    "first_loss": losses[0] if losses else None, "last_loss": losses[-1] if losses else None},
         "reference_mean": float(ref.mean()),
         "relmse_ratio": e_plain / e_guided if e_guided > 0 else None,
@@ -89,11 +91,12 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-2)
     ap.add_argument("--selection-prob", type=float, default=0.5)
     ap.add_argument("--weight-quantile", type=float, default=0.99)
+    ap.add_argument("--spatial-cells", type=int, default=0)
     ap.add_argument("--tess", type=int, default=15)
     a = ap.parse_args()
     print(json.dumps(evaluate(a.width, a.height, a.spp, a.ref_spp, a.spp_per_pass, a.train_steps, a.batch, a.lr,
                               a.selection_prob, tess=a.tess, train_passes=a.train_passes,
-                              weight_quantile=a.weight_quantile)))
+                              weight_quantile=a.weight_quantile, spatial_cells=a.spatial_cells)))
 
 
 if __name__ == "__main__":
