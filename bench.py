@@ -50,6 +50,70 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def mlp_bench():
+    """The guiding network's kernels against the tensor-pipe peak: one Adam step on 2^16 records (forward +
+    backward + update; 3 x 43,008 FLOP per record by the dense-layer count) and one forward pass over 2^20
+    vertices (43,008 FLOP each: 2 (96x64 + 3 x 64x64 + 64x48))."""
+    import numpy as np
+    import torch
+
+    from piper2_b200 import api
+
+    g = api.Guide(seed=0)
+    rng = np.random.default_rng(0)
+    b = 1 << 16
+    rec = np.zeros((b, 16), np.float32)
+    rec[:, 0:3] = rng.uniform(0, 1, (b, 3))
+    for k in (3, 6, 9):
+        v = rng.normal(size=(b, 3))
+        rec[:, k:k + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    rec[:, 12] = rng.exponential(1.0, b)
+    drec = torch.from_numpy(rec).cuda()
+    n = 1 << 20
+    feat = torch.from_numpy(np.concatenate([rec] * 16)[:, :12].copy()).cuda()
+    out = torch.empty((n, 48), device="cuda")
+    import ctypes as C
+
+    from piper2_b200 import capi
+
+    lib = capi.lib()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def train():
+        capi.check(lib.pb2_guide_train(g.h, C.c_void_p(drec.data_ptr()), b, C.c_float(1e-3), None, sp))
+
+    def fwd():
+        capi.check(lib.pb2_guide_forward(g.h, C.c_void_p(feat.data_ptr()), n, C.c_void_p(out.data_ptr()), sp))
+
+    res = {}
+    peak, kind = _bf16_peak()
+    for name, fn, flops in (("train_step_2^16", train, 3 * 43008 * b), ("forward_2^20", fwd, 43008 * n)):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        tf = flops / (ms * 1e-3) / 1e12
+        res[name] = {"ms": round(ms, 4), "tflops": round(tf, 2), "frac": round(tf / peak, 4)}
+    res["peak_tflops"] = peak
+    res["peak_source"] = kind
+    res["note"] = "mma.sync m16n8k16 bf16 tiles, 16 rows per warp; the network is 64 wide"
+    return res
+
+
 def _profile_traffic():
     """DRAM bytes per closest-hit launch from the committed ncu summary (None if absent)."""
     path = os.path.join(ROOT, "profiles", "trace_closest_soup1M.md")
@@ -370,6 +434,7 @@ def render_bench(args):
     torch.cuda.empty_cache()
     g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512)
     result["guiding"] = g
+    result["guiding_mlp"] = mlp_bench()
     return result
 
 
