@@ -140,12 +140,15 @@ typedef struct pb2_render_settings {
     uint32_t fit_mode;        /* pb2_fit_mode, Src/Interface/BuiltinComponent/Sensor.hpp:36-75 */
     uint32_t samples_per_pixel;/* ScrambledSobolSampler "SamplesPerPixel": rounded up to a power of 2
                                   (ScrambledSobolSampler.cpp:43-50) */
-    uint32_t scramble;        /* must be 0: "Scramble" is notImplemented in the reference (:51-53) */
+    uint32_t scramble;        /* 0: unscrambled, the reference's only mode ("Scramble" is notImplemented,
+                                  :51-53).  1: Owen scrambling of dimensions >= 2 (extension, see
+                                  scramble_seed); dimensions 0/1 place the sample in its pixel and stay */
     uint32_t max_depth;       /* PathTracing "MaxTraceDepth" (PathTracing.cpp:38) */
     uint32_t min_rr_depth;    /* PathTracing "MinRussianRouletteDepth" (PathTracing.cpp:39) */
     uint32_t filter;          /* pb2_filter_type (FixedSampler.cpp:38-45) */
     float gaussian_alpha;     /* "Alpha" of the gaussian filter */
     pb2_camera camera;
+    uint32_t scramble_seed;   /* seed of the Owen scrambling (scramble = 1) */
 } pb2_render_settings;
 
 /* Render rectangle (Tracer.hpp:96-98 RenderRECT). */

@@ -37,6 +37,8 @@ def oracle():
         h = C.CDLL(ORACLE_SO)
         h.or_sobol_sample.restype = C.c_float
         h.or_sobol_sample.argtypes = [C.c_uint64, C.c_uint32]
+        h.or_sobol_sample_scrambled.restype = C.c_float
+        h.or_sobol_sample_scrambled.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
         h.or_sobol_interval_to_index.restype = C.c_uint64
         h.or_sobol_interval_to_index.argtypes = [C.c_uint32] * 4
         h.or_sobol_start.argtypes = [C.c_uint32] * 5 + [C.POINTER(C.c_uint64), C.POINTER(C.c_float)]

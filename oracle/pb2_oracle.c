@@ -1413,15 +1413,27 @@ typedef struct path_ctx {
     const or_scene* s;
     uint64_t index;
     uint32_t dim;
+    uint32_t scramble, seed; /* Owen scrambling of dimensions >= 2 (extension, pb2_math.h) */
     int overflow;
     uint64_t closest_rays, shadow_rays;
 } path_ctx;
 
 /* piperSample (Tracer/Embree/Kernel.cpp:37-45); the mt19937_64 tail past dimension 1023 is not
  * reproduced (settings that could reach it are rejected up front). */
+/* Dimension `dim` (>= 2) of a sample, Owen-scrambled when asked for (extension: the reference's Scramble
+ * is notImplemented, ScrambledSobolSampler.cpp:51-53). */
+float or_sobol_sample_scrambled(uint64_t index, uint32_t dim, uint32_t scramble, uint32_t seed) {
+    uint32_t v = 0;
+    for (uint32_t i = dim * PB2_SOBOL_MATRIX_SIZE; index; index >>= 1, i++)
+        if (index & 1) v ^= pb2_sobol_matrices32[i];
+    if (scramble) v = pb2_owen_scramble(v, pb2_owen_dim_seed(seed, dim));
+    return (float)v * 0x1p-32f;
+}
+
 static inline float next_sample(path_ctx* c) {
     if (c->dim >= PB2_SOBOL_DIMS) { c->overflow = 1; return 0.5f; }
-    return or_sobol_sample(c->index, c->dim++);
+    const uint32_t d = c->dim++;
+    return or_sobol_sample_scrambled(c->index, d, c->scramble, c->seed);
 }
 
 /* The two uniform numbers of piperSurfaceSample / piperLightSample are the two `piperSample(context)`
@@ -1626,7 +1638,7 @@ void or_bsdf_eval(const or_scene* s, uint32_t mat, int front, const float wo_in[
 
 int or_render(const or_scene* s, const pb2_render_settings* st, const pb2_rect* rect, uint32_t sample_begin,
               uint32_t sample_count, float* rgbw, float* sample_out, int threads) {
-    if (st->scramble) return -1;
+    if (st->scramble > 1) return -1;
     if (5u + 8u * (uint64_t)st->max_depth > PB2_SOBOL_DIMS) return -2;
     pb2_ndc_transform tr;
     pb2_rect full;
@@ -1650,14 +1662,16 @@ int or_render(const or_scene* s, const pb2_render_settings* st, const pb2_rect* 
                 memset(&c, 0, sizeof(c));
                 c.s = s;
                 c.dim = 5;
+                c.scramble = st->scramble;
+                c.seed = st->scramble_seed;
                 float off[2];
                 or_sobol_start(res, log2res, sx, sy, sidx, &c.index, off);
                 const float px = off[0] + (float)(full.left + sx);
                 const float py = off[1] + (float)(full.top + sy);
                 const float ndc_x = tr.ox + tr.sx * px / (float)st->width;
                 const float ndc_y = tr.oy + tr.sy * py / (float)st->height;
-                const float u1 = or_sobol_sample(c.index, 3);
-                const float u2 = or_sobol_sample(c.index, 4);
+                const float u1 = or_sobol_sample_scrambled(c.index, 3, st->scramble, st->scramble_seed);
+                const float u2 = or_sobol_sample_scrambled(c.index, 4, st->scramble, st->scramble_seed);
                 pb2_ray ray;
                 or_camera_ray(&st->camera, ndc_x, ndc_y, u1, u2, &ray);
                 uint32_t depth;

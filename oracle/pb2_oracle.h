@@ -24,6 +24,8 @@ extern "C" {
 typedef struct or_scene or_scene;
 
 float or_sobol_sample(uint64_t index, uint32_t dim);
+/* Dimension `dim` of a sample with optional Owen scrambling (scramble = 1, extension). */
+float or_sobol_sample_scrambled(uint64_t index, uint32_t dim, uint32_t scramble, uint32_t seed);
 uint64_t or_sobol_interval_to_index(uint32_t m, uint32_t sample, uint32_t px, uint32_t py);
 void or_sobol_start(uint32_t resolution, uint32_t log2_resolution, uint32_t px, uint32_t py,
                     uint32_t sample, uint64_t* index, float offset[2]);

@@ -72,7 +72,7 @@ class RenderSettings(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fit_mode", C.c_uint32),
                 ("samples_per_pixel", C.c_uint32), ("scramble", C.c_uint32), ("max_depth", C.c_uint32),
                 ("min_rr_depth", C.c_uint32), ("filter", C.c_uint32), ("gaussian_alpha", C.c_float),
-                ("camera", Camera)]
+                ("camera", Camera), ("scramble_seed", C.c_uint32)]
 
 
 class Rect(C.Structure):

@@ -147,3 +147,43 @@ PB2_HD float pb2_acosf(float x) {
     }
     return r;
 }
+
+/* ---- Owen scrambling of Sobol values (an extension: the reference's "Scramble" is notImplemented,
+ * ScrambledSobolSampler.cpp:51-53) -----------------------------------------------------------------
+ * Nested uniform scrambling by hashing (Burley, "Practical Hash-based Owen Scrambling", JCGT 9(4), 2020):
+ * reverse the bits, apply the Laine-Karras style permutation (an added seed, then x ^= x * c with even
+ * constants -- each output bit depends only on the same and lower bits of the reversed value), reverse
+ * back.  Every elementary interval of the input maps to one of the output, so a Sobol dimension stays
+ * stratified.  The per-dimension seed is the MurmurHash3 finaliser of (seed, dimension). */
+PB2_HD uint32_t pb2_reverse_bits(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __brev(x);
+#else
+    x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
+    x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
+    x = ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4);
+    x = ((x >> 8) & 0x00FF00FFu) | ((x & 0x00FF00FFu) << 8);
+    return (x >> 16) | (x << 16);
+#endif
+}
+
+PB2_HD uint32_t pb2_owen_dim_seed(uint32_t seed, uint32_t dim) {
+    uint32_t h = seed ^ (dim * 0x9E3779B9u + 0x632BE5ABu);
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+PB2_HD uint32_t pb2_owen_scramble(uint32_t v, uint32_t seed) {
+    uint32_t x = pb2_reverse_bits(v);
+    x += seed;
+    x ^= x * 0x6C50B47Cu;
+    x ^= x * 0xB82F1E52u;
+    x ^= x * 0xC7AFE638u;
+    x ^= x * 0x8D22F6E6u;
+    return pb2_reverse_bits(x);
+}
+

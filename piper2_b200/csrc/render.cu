@@ -26,10 +26,19 @@
 
 namespace pb2 {
 
-__device__ __forceinline__ float sobol_sample(uint64_t index, uint32_t dim) {
+__device__ __forceinline__ uint32_t sobol_bits(uint64_t index, uint32_t dim) {
     uint32_t v = 0;
     for (uint32_t i = dim * PB2_SOBOL_MATRIX_SIZE; index; index >>= 1, i++)
         if (index & 1) v ^= __ldg(&pb2_sobol_matrices32[i]);
+    return v;
+}
+__device__ __forceinline__ float sobol_sample(uint64_t index, uint32_t dim) {
+    return (float)sobol_bits(index, dim) * 0x1p-32f;
+}
+// A dimension >= 2 of a launch, Owen-scrambled when the settings ask for it (extension; see pb2_math.h).
+__device__ __forceinline__ float sobol_sample_s(uint64_t index, uint32_t dim, uint32_t scramble, uint32_t seed) {
+    uint32_t v = sobol_bits(index, dim);
+    if (scramble) v = pb2_owen_scramble(v, pb2_owen_dim_seed(seed, dim));
     return (float)v * 0x1p-32f;
 }
 
@@ -134,6 +143,7 @@ struct LaunchParams {
     float env[3];
     uint32_t path_count;
     uint32_t checks;      // PB2_DEBUG_CHECKS: verify indices, record the first violation, skip the path
+    uint32_t scramble, scramble_seed;  // Owen scrambling of dimensions >= 2 (extension)
 };
 
 struct SceneView {
@@ -298,8 +308,8 @@ __device__ __forceinline__ void primary_ray(const LaunchParams& lp, uint32_t sx,
     py = offy + (float)(lp.full.top + sy);
     const float ndc_x = lp.ndc.ox + lp.ndc.sx * px / (float)lp.width;
     const float ndc_y = lp.ndc.oy + lp.ndc.sy * py / (float)lp.height;
-    const float u1 = sobol_sample(index, 3);
-    const float u2 = sobol_sample(index, 4);
+    const float u1 = sobol_sample_s(index, 3, lp.scramble, lp.scramble_seed);
+    const float u2 = sobol_sample_s(index, 4, lp.scramble, lp.scramble_seed);
     camera_ray(lp.cam, ndc_x, ndc_y, u1, u2, org, dir);
 }
 
@@ -575,9 +585,10 @@ __global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState
 struct SampleCursor {
     uint64_t index;
     uint32_t dim;
+    uint32_t scramble, seed;
     __device__ __forceinline__ float next() {
         if (dim >= PB2_SOBOL_DIMS) return 0.5f;  // unreachable: the pipeline rejects depths that could get here
-        return sobol_sample(index, dim++);
+        return sobol_sample_s(index, dim++, scramble, seed);
     }
     // the two piperSample() arguments of one call are evaluated right to left (u2 first)
     __device__ __forceinline__ void pair(float& u1, float& u2) {
@@ -684,7 +695,7 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
         const v3 o = mk3(o4.x, o4.y, o4.z), d = mk3(d4.x, d4.y, d4.z);
         spec pf = mksp(pf4.x, pf4.y, pf4.z);
         uint32_t depth = ps.depth[slot];
-        SampleCursor sc{ ps.sidx[slot], ps.dim[slot] };
+        SampleCursor sc{ ps.sidx[slot], ps.dim[slot], lp.scramble, lp.scramble_seed };
         // calcTriangleMeshSurface (Tracer/Embree/Kernel.cpp:170-192) with face from Embree.cpp:336
         const uint32_t hs = ps.hit_slot[slot];
         const float4* t4 = reinterpret_cast<const float4*>(sv.bvh.tris + hs);
@@ -1290,7 +1301,8 @@ int pb2_sobol_start(uint32_t log2_resolution, const uint32_t* pixel_sample, uint
 int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, void* stream_ptr, pb2_pipeline** out) {
     if (!scene || !st || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_create: null argument");
     *out = nullptr;
-    if (st->scramble) return fail(PB2_ERR_NOT_SUPPORTED, "Scramble is not implemented by the reference sampler");
+    if (st->scramble > 1)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "scramble must be 0 (none, the reference's sampler) or 1 (Owen)");
     if (st->width == 0 || st->height == 0) return fail(PB2_ERR_INVALID_ARGUMENT, "empty film");
     if (st->samples_per_pixel == 0 || (st->samples_per_pixel & (st->samples_per_pixel - 1)))
         return fail(PB2_ERR_INVALID_ARGUMENT, "samples_per_pixel must be a power of two (the sampler rounds it up)");
@@ -1466,6 +1478,8 @@ static LaunchParams make_params(const pb2_pipeline* pl, const pb2_rect& rect, ui
     lp.num_lights = pl->num_lights;
     for (int k = 0; k < 3; ++k) lp.env[k] = pl->env[k];
     lp.path_count = rect.width * rect.height * sc;
+    lp.scramble = pl->settings.scramble;
+    lp.scramble_seed = pl->settings.scramble_seed;
     static const bool checks = [] {
         const char* v = std::getenv("PB2_DEBUG_CHECKS");
         return v && v[0] == '1';

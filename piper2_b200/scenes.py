@@ -161,14 +161,15 @@ def _box(center, size, angle):
 
 
 def render_settings(width, height, spp, max_depth, min_rr_depth, camera, filt="box", alpha=2.0,
-                    fit="Fill") -> capi.RenderSettings:
+                    fit="Fill", scramble=0, scramble_seed=0) -> capi.RenderSettings:
     st = capi.RenderSettings()
     st.width, st.height = width, height
     st.fit_mode = capi.FIT[fit]
     if spp & (spp - 1):
         spp = 1 << int(math.ceil(math.log2(spp)))  # ScrambledSobolSampler.cpp:43-50
     st.samples_per_pixel = spp
-    st.scramble = 0
+    st.scramble = scramble  # 1: Owen scrambling of dimensions >= 2 (extension; the reference has none)
+    st.scramble_seed = scramble_seed
     st.max_depth = max_depth
     st.min_rr_depth = min_rr_depth
     st.filter = capi.FILTER[filt]

@@ -141,6 +141,29 @@ def test_mixed_materials_crops_bitexact(oracle):
             assert not diff.any(), f"{diff.sum()} of {diff.size} samples differ"
 
 
+def test_owen_scrambled_render_bitexact_and_unbiased(oracle):
+    """Owen-scrambled sampling (extension; the reference's Scramble is notImplemented): every sample equals
+    the oracle's, and the image mean agrees with the unscrambled render within 4 standard errors."""
+    sd = scenes.cornell_box(seed=1, width=48, height=48, spp=8)
+    sd.settings.scramble, sd.settings.scramble_seed = 1, 12345
+    with _api().Pipeline(sd) as pl:
+        film, samples = pl.render(samples=True)
+    _, osamples = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
+    diff = np.any(samples.view(np.uint32) != osamples.view(np.uint32), axis=-1)
+    assert not diff.any(), f"{diff.sum()} of {diff.size} samples differ"
+    big = scenes.cornell_box(seed=1, width=128, height=128, spp=16)
+    with _api().Pipeline(big) as pl:
+        _, s0 = pl.render(samples=True)
+    big.settings.scramble, big.settings.scramble_seed = 1, 99
+    with _api().Pipeline(big) as pl:
+        _, s1 = pl.render(samples=True)
+    r0 = s0[..., 2:5].reshape(-1, 3).astype(np.float64)
+    r1 = s1[..., 2:5].reshape(-1, 3).astype(np.float64)
+    se = np.sqrt(r0.var(axis=0) / len(r0) + r1.var(axis=0) / len(r1))
+    assert np.all(np.abs(r0.mean(axis=0) - r1.mean(axis=0)) <= 4 * se)
+    assert not np.array_equal(r0, r1)
+
+
 def test_tiled_launches_sum_to_full(oracle):
     """Launching 8 x 8 tiles (the reference's FixedSampler launch shape) gives the same film."""
     import torch
@@ -165,8 +188,8 @@ def test_invalid_settings_rejected():
 
     sd = scenes.cornell_box(seed=0, width=8, height=8)
     st = sd.settings
-    st.scramble = 1
-    with pytest.raises(capi.PB2Error, match="Scramble"):
+    st.scramble = 2
+    with pytest.raises(capi.PB2Error, match="scramble"):
         _api().Pipeline(sd, st)
     st.scramble = 0
     st.max_depth = 200

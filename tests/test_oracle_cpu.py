@@ -193,3 +193,23 @@ def test_oracle_vs_reference_materials(oracle):
     _, osamp = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
     _, rsamp = oracle.RefScene(sd, use_bvh=False).render(threads=1)
     _compare_to_reference(osamp, rsamp)
+
+
+def test_owen_scrambling_keeps_stratification(oracle):
+    """Owen-scrambled dimensions (extension: the reference's Scramble is notImplemented) stay stratified:
+    the first 2^m indices of every dimension fall one per interval of width 2^-m, as unscrambled Sobol
+    points do; the values differ from the unscrambled ones, and seeds give different scrambles."""
+    lib = oracle.oracle()
+    m = 10
+    for dim in (2, 3, 5, 11, 100, 1023):
+        for seed in (0, 7):
+            v = np.array([lib.or_sobol_sample_scrambled(i, dim, 1, seed) for i in range(1 << m)])
+            cells = np.floor(v * (1 << m)).astype(int)
+            assert np.array_equal(np.sort(cells), np.arange(1 << m)), (dim, seed)
+            plain = np.array([lib.or_sobol_sample(i, dim) for i in range(1 << m)])
+            assert np.mean(v != plain) > 0.9
+        a = np.array([lib.or_sobol_sample_scrambled(i, dim, 1, 1) for i in range(64)])
+        b = np.array([lib.or_sobol_sample_scrambled(i, dim, 1, 2) for i in range(64)])
+        assert np.mean(a != b) > 0.9
+    # scramble = 0 is the unscrambled sampler
+    assert all(lib.or_sobol_sample_scrambled(i, 9, 0, 5) == lib.or_sobol_sample(i, 9) for i in range(200))
