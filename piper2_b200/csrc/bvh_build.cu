@@ -6,12 +6,16 @@
 //   4. binary radix tree over the sorted codes (Karras, "Maximizing Parallelism in the Construction of
 //      BVHs, Octrees, and k-d Trees", HPG 2012), equal codes ordered by index,
 //   5. bottom-up box refit (the second child to arrive at a node computes its box),
-//   6. top-down collapse into 8-wide nodes, one frontier level per launch: each wide node greedily
-//      opens its largest-area binary descendant with more than 3 triangles until it has 8 children,
-//      then, while slots remain, the largest smaller subtrees; subtrees of at most 3 triangles become
-//      leaves; child boxes are quantised to 8 bits relative to the node box
-//      (rounded outward) and children are placed in the slot of the ray octant they are nearest
-//      for (greedy assignment on the projected centroid offsets).
+//   6. SAH costs of the collapse, bottom-up over the binary tree (Ylitie, Karras, Laine, "Efficient
+//      Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017, Sec. 4.1): for every
+//      binary node n and i = 1..8, C(n, i) = the least SAH cost of representing n's subtree with at most
+//      i children of the enclosing wide node, where one child is either a leaf of <= 3 triangles
+//      (cost kCostTri x triangles x area) or a wide node (kCostNode x area + the best distribution of 8
+//      children below it); distributions split i between n's two binary children,
+//   7. top-down collapse into 8-wide nodes, one frontier level per launch, each wide node taking the
+//      children of its optimal distribution; child boxes are quantised to 8 bits relative to the node
+//      box (rounded outward) and children are placed in the slot of the ray octant they are nearest for
+//      (greedy assignment on the projected centroid offsets).
 #include <cub/device/device_radix_sort.cuh>
 
 #include <cfloat>
@@ -23,6 +27,15 @@ namespace pb2 {
 namespace {
 
 constexpr int kLeafMax = 3;
+// SAH weights of the collapse, per unit of surface area: a wide node against a leaf triangle.  Measured on a
+// B200 (1M-triangle soup, closest hit): 0.15 -> 783, 0.3 -> 883, 0.8 -> 964, 1.2 -> 1017, 2.0 -> 1021,
+// 3.0 -> 1020 Mrays/s; a triangle weighted above a node makes the collapse favour small leaves, which the
+// traversal's per-triangle divergence rewards more than the box count predicts.
+#ifndef PB2_SAH_COST_TRI
+#define PB2_SAH_COST_TRI 2.0f
+#endif
+constexpr float kCostNode = 1.0f;
+constexpr float kCostTri = PB2_SAH_COST_TRI;
 
 __device__ __forceinline__ int f2key(float f) {
     const int i = __float_as_int(f);
@@ -178,6 +191,72 @@ __global__ void k_refit(const Internal* __restrict__ nodes, const int* __restric
     }
 }
 
+__device__ __forceinline__ float box_area(float4 l, float4 h) {
+    const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// SAH collapse costs (step 6).  cost[8 n + i - 1] = C(n, i); split[8 n + i - 1] = how many of i children go
+// to the left binary child in the best distribution D(n, i) (i >= 2); dist[n] bit i set when D(n, i) beats a
+// single child for C(n, i); leafy[n] = 1 when that single child is a leaf (possible for <= 3 triangles).
+// Bottom-up like the refit.
+__global__ void k_sah_costs(const Internal* __restrict__ nodes, const int* __restrict__ iparent,
+                            const int* __restrict__ lparent, const float4* __restrict__ slo, const float4* __restrict__ shi,
+                            const float4* __restrict__ ilo, const float4* __restrict__ ihi, uint32_t* flags, float* cost,
+                            uint8_t* split, uint8_t* dist, uint8_t* leafy, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int node = lparent[k];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1u) == 0) return;
+        __threadfence();
+        const Internal nd = nodes[node];
+        float cl[8], cr[8];
+        if (is_leaf(nd.left)) {
+            const float c = kCostTri * box_area(slo[~nd.left], shi[~nd.left]);
+            for (int i = 0; i < 8; ++i) cl[i] = c;
+        } else {
+            for (int i = 0; i < 8; ++i) cl[i] = __ldcg(&cost[8 * (size_t)nd.left + i]);
+        }
+        if (is_leaf(nd.right)) {
+            const float c = kCostTri * box_area(slo[~nd.right], shi[~nd.right]);
+            for (int i = 0; i < 8; ++i) cr[i] = c;
+        } else {
+            for (int i = 0; i < 8; ++i) cr[i] = __ldcg(&cost[8 * (size_t)nd.right + i]);
+        }
+        float d[9];
+        uint8_t sp[9];
+        for (int i = 2; i <= 8; ++i) {
+            float best = FLT_MAX;
+            int arg = 1;
+            for (int j = 1; j < i; ++j) {
+                const float c = cl[j - 1] + cr[i - j - 1];
+                if (c < best) { best = c; arg = j; }
+            }
+            d[i] = best;
+            sp[i] = (uint8_t)arg;
+        }
+        const float area = box_area(__ldcg(&ilo[node]), __ldcg(&ihi[node]));
+        const uint32_t tris = nd.last - nd.first + 1;
+        const float c_wide = kCostNode * area + d[8];
+        const float c_leaf = tris <= (uint32_t)kLeafMax ? kCostTri * (float)tris * area : FLT_MAX;
+        const bool leaf = c_leaf <= c_wide;
+        const float c1 = leaf ? c_leaf : c_wide;
+        uint8_t dm = 0;
+        __stcg(&cost[8 * (size_t)node], c1);
+        for (int i = 2; i <= 8; ++i) {
+            const bool use = d[i] < c1;
+            if (use) dm |= (uint8_t)(1u << i);
+            __stcg(&cost[8 * (size_t)node + i - 1], use ? d[i] : c1);
+            split[8 * (size_t)node + i - 1] = sp[i];
+        }
+        dist[node] = dm;
+        leafy[node] = leaf ? 1 : 0;
+        node = iparent[node];
+    }
+}
+
 struct Frontier {
     int ref;
     uint32_t wide;
@@ -207,7 +286,8 @@ __global__ void k_collapse(const Frontier* __restrict__ in, uint32_t count, Fron
                            const float4* __restrict__ shi, const float4* __restrict__ ilo,
                            const float4* __restrict__ ihi, const uint32_t* __restrict__ vals,
                            const TriSlot* __restrict__ tris_in, WideNode* __restrict__ wnodes,
-                           TriSlot* __restrict__ tris_out) {
+                           TriSlot* __restrict__ tris_out, const uint8_t* __restrict__ split,
+                           const uint8_t* __restrict__ dist, const uint8_t* __restrict__ leafy) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int ref = in[i].ref;
@@ -217,39 +297,33 @@ __global__ void k_collapse(const Frontier* __restrict__ in, uint32_t count, Fron
     if (is_leaf(ref)) {
         ch[nch++] = ref;
     } else {
+        // the children of the best distribution of 8 below `ref` (step 6): expand (binary node, slots) pairs
+        // until each is one child (a binary leaf, a single-child decision, or a subtree that is a leaf)
+        int st_ref[8];
+        int st_n[8];
+        int sp = 0;
         const Internal nd = nodes[ref];
-        ch[nch++] = nd.left;
-        ch[nch++] = nd.right;
-        while (nch < 8) {
-            int best = -1;
-            float best_area = -1.0f;
-            for (int k = 0; k < nch; ++k) {
-                if (is_leaf(ch[k]) || ref_count(ch[k], nodes) <= (uint32_t)kLeafMax) continue;
-                const float4 l = ilo[ch[k]], h = ihi[ch[k]];
-                const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
-                const float area = dx * dy + dy * dz + dz * dx;
-                if (area > best_area) { best_area = area; best = k; }
+        const int k8 = split[8 * (size_t)ref + 7];
+        st_ref[sp] = nd.right; st_n[sp] = 8 - k8; ++sp;
+        st_ref[sp] = nd.left; st_n[sp] = k8; ++sp;
+        while (sp > 0 && nch < 8) {
+            --sp;
+            const int r = st_ref[sp];
+            const int slots = st_n[sp];
+            if (is_leaf(r) || slots == 1 || !((dist[r] >> slots) & 1u)) {
+                ch[nch++] = r;
+            } else {
+                const Internal c = nodes[r];
+                const int k = split[8 * (size_t)r + slots - 1];
+                st_ref[sp] = c.right; st_n[sp] = slots - k; ++sp;
+                st_ref[sp] = c.left; st_n[sp] = k; ++sp;
             }
-            if (best < 0) {
-                // room left: also open small subtrees (tighter leaves, fewer triangle tests)
-                for (int k = 0; k < nch; ++k) {
-                    if (is_leaf(ch[k])) continue;
-                    const float4 l = ilo[ch[k]], h = ihi[ch[k]];
-                    const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
-                    const float area = dx * dy + dy * dz + dz * dx;
-                    if (area > best_area) { best_area = area; best = k; }
-                }
-            }
-            if (best < 0) break;
-            const Internal c = nodes[ch[best]];
-            ch[best] = c.left;
-            ch[nch++] = c.right;
         }
     }
     float4 cl[8], chh[8];
     float4 nlo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.0f), nhi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.0f);
     for (int k = 0; k < nch; ++k) {
-        if (is_leaf(ch[k]) || ref_count(ch[k], nodes) > (uint32_t)kLeafMax) {
+        if (is_leaf(ch[k]) || !leafy[ch[k]]) {
             if (is_leaf(ch[k])) { cl[k] = slo[~ch[k]]; chh[k] = shi[~ch[k]]; }
             else { cl[k] = ilo[ch[k]]; chh[k] = ihi[ch[k]]; }
         } else {
@@ -288,7 +362,7 @@ __global__ void k_collapse(const Frontier* __restrict__ in, uint32_t count, Fron
     uint32_t n_internal = 0, n_tris = 0;
     for (int k = 0; k < nch; ++k) {
         const uint32_t c = ref_count(ch[k], nodes);
-        if (c > (uint32_t)kLeafMax) ++n_internal;
+        if (!is_leaf(ch[k]) && !leafy[ch[k]]) ++n_internal;
         else n_tris += c;
     }
     const uint32_t child_base = n_internal ? atomicAdd(node_counter, n_internal) : 0u;
@@ -320,7 +394,7 @@ __global__ void k_collapse(const Frontier* __restrict__ in, uint32_t count, Fron
             qhi[a][s] = (uint8_t)qh;
         }
         const uint32_t c = ref_count(ch[k], nodes);
-        if (c > (uint32_t)kLeafMax) {
+        if (!is_leaf(ch[k]) && !leafy[ch[k]]) {
             imask |= 1u << s;
             meta[s] = (uint8_t)((1u << 5) | (24u + s));
             out[out_base + int_idx] = Frontier{ ch[k], child_base + int_idx };
@@ -371,6 +445,8 @@ struct ScratchLayout {
     int *iparent, *lparent;
     uint32_t* flags;
     Frontier *fa, *fb;
+    float* cost;
+    uint8_t *split, *dist, *leafy;
     int* cbounds;
     uint32_t* counters;
     void* cub_tmp;
@@ -399,6 +475,10 @@ static ScratchLayout layout(char* base, uint32_t n) {
     L.flags = carve<uint32_t>(p, m);
     L.fa = carve<Frontier>(p, m);
     L.fb = carve<Frontier>(p, m);
+    L.cost = carve<float>(p, 8 * m);
+    L.split = carve<uint8_t>(p, 8 * m);
+    L.dist = carve<uint8_t>(p, m);
+    L.leafy = carve<uint8_t>(p, m);
     L.cbounds = carve<int>(p, 8);
     L.counters = carve<uint32_t>(p, 8);
     L.cub_bytes = cub_bytes((uint32_t)m);
@@ -449,6 +529,9 @@ cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* wnodes,
         if ((err = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * m, stream))) return err;
         k_karras<<<(unsigned)((n - 1 + T - 1) / T), T, 0, stream>>>(keys2, n, nodes, iparent, lparent);
         k_refit<<<G, T, 0, stream>>>(nodes, iparent, lparent, slo, shi, ilo, ihi, flags, n);
+        if ((err = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * m, stream))) return err;
+        k_sah_costs<<<G, T, 0, stream>>>(nodes, iparent, lparent, slo, shi, ilo, ihi, flags, L.cost, L.split, L.dist,
+                                         L.leafy, n);
     }
     // collapse, one frontier level per launch
     const uint32_t init_counters[8] = { 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u };  // node_counter, tri_counter, out_count
@@ -460,7 +543,8 @@ cudaError_t build_wide_bvh(const TriSlot* tris_in, uint32_t n, WideNode* wnodes,
     while (count > 0) {
         if ((err = cudaMemsetAsync(counters + 2, 0, sizeof(uint32_t), stream))) return err;
         k_collapse<<<(count + 127) / 128, 128, 0, stream>>>(fa, count, fb, counters + 2, counters + 0, counters + 1,
-                                                           nodes, slo, shi, ilo, ihi, vals2, tris_in, wnodes, tris_out);
+                                                           nodes, slo, shi, ilo, ihi, vals2, tris_in, wnodes, tris_out,
+                                                           L.split, L.dist, L.leafy);
         if ((err = cudaMemcpyAsync(&count, counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream))) return err;
         if ((err = cudaStreamSynchronize(stream))) return err;
         Frontier* t = fa; fa = fb; fb = t;
@@ -504,6 +588,9 @@ cudaError_t build_wide_bvh_prealloc(const TriSlot* tris_in, uint32_t n, WideNode
         if ((err = cudaMemsetAsync(L.flags, 0, sizeof(uint32_t) * m, stream))) return err;
         k_karras<<<(unsigned)((n - 1 + T - 1) / T), T, 0, stream>>>(L.keys2, n, L.nodes, L.iparent, L.lparent);
         k_refit<<<G, T, 0, stream>>>(L.nodes, L.iparent, L.lparent, L.slo, L.shi, L.ilo, L.ihi, L.flags, n);
+        if ((err = cudaMemsetAsync(L.flags, 0, sizeof(uint32_t) * m, stream))) return err;
+        k_sah_costs<<<G, T, 0, stream>>>(L.nodes, L.iparent, L.lparent, L.slo, L.shi, L.ilo, L.ihi, L.flags, L.cost,
+                                         L.split, L.dist, L.leafy, n);
     }
     const uint32_t init_counters[8] = { 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u };
     if ((err = cudaMemcpyAsync(L.counters, init_counters, sizeof(init_counters), cudaMemcpyHostToDevice, stream)))
@@ -516,7 +603,7 @@ cudaError_t build_wide_bvh_prealloc(const TriSlot* tris_in, uint32_t n, WideNode
         if ((err = cudaMemsetAsync(L.counters + 2, 0, sizeof(uint32_t), stream))) return err;
         k_collapse<<<(count + 127) / 128, 128, 0, stream>>>(fa, count, fb, L.counters + 2, L.counters + 0, L.counters + 1,
                                                            L.nodes, L.slo, L.shi, L.ilo, L.ihi, L.vals2, tris_in, wnodes,
-                                                           tris_out);
+                                                           tris_out, L.split, L.dist, L.leafy);
         if ((err = cudaMemcpyAsync(&count, L.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream))) return err;
         if ((err = cudaStreamSynchronize(stream))) return err;
         Frontier* t = fa;
