@@ -49,25 +49,57 @@ __global__ void k_weight_sum(const float* __restrict__ rec, uint32_t n, float* s
     if ((threadIdx.x & 31) == 0) atomicAdd(&scalars[0], s);
 }
 
-// records: n rows of 16 floats (pos01 xyz, normal xyz, wo xyz, wi xyz, weight, unused x3)
-__global__ void __launch_bounds__(kThreads) k_gradient(GuideView gv, const float* __restrict__ rec, uint32_t n,
-                                                       const float* __restrict__ scalars, float* __restrict__ grad,
-                                                       float* __restrict__ loss) {
+// ---- loss gradient over a batch, in three passes ------------------------------------------------------
+// The weight gradient dW_l = sum over records of dZ_l^T x input_l is a GEMM whose reduction runs over the
+// batch.  Pass 1 runs forward and backward-data per 16-record tile and stages the bf16 layer inputs and
+// deltas (1.3 KB per record); pass 2 runs the weight-gradient GEMMs with the batch as K, each block
+// accumulating all 168 16x8 output tiles in registers over its records; pass 3 sums the blocks' partials.
+// The bias gradients (column sums of the deltas) are reduced per block in pass 1.
+constexpr int kStageX = kIn + 4 * kHid;   // 352: input X | H1 | H2 | H3 | H4 (the input of layer l)
+constexpr int kStageD = 4 * kHid + kOut;  // 304: dZ0 | dZ1 | dZ2 | dZ3 | dY (the delta of layer l)
+constexpr uint32_t kChunkRows = 1u << 16; // records staged per pass
+constexpr int kGwThreads = 256;           // pass 2: 8 warps x 21 output tiles
+constexpr int kGwRows = 64;               // pass 2: records per shared-memory chunk
+constexpr int kGwXs = kStageX + 8, kGwDs = kStageD + 8;  // padded rows (conflict-free ldmatrix)
+constexpr int kOutTiles = 48 + 3 * 32 + 24;
+constexpr uint32_t kGwMaxBlocks = 128;
+constexpr int kGrWarps = 8;  // pass 1: warps per block (one 16-record tile each at a time)
+constexpr int kGrThreads = kGrWarps * 32;
+__host__ __device__ constexpr int stage_x_offset(int l) { return l == 0 ? 0 : kIn + (l - 1) * kHid; }
+__host__ __device__ constexpr int stage_d_offset(int l) { return l * kHid; }
+
+// Pass 1.  records: n rows of 16 floats (pos01 xyz, normal xyz, wo xyz, wi xyz, weight, unused x3); `total`
+// is the batch size the loss is normalised by.  Writes staged rows (all 16 rows of every tile; rows past n
+// carry zero deltas), adds bias gradients to grad and the loss to *loss.
+__global__ void __launch_bounds__(kGrThreads) k_grad_rows(GuideView gv, const float* __restrict__ rec, uint32_t n,
+                                                        uint32_t total, const float* __restrict__ scalars,
+                                                        __nv_bfloat16* __restrict__ sx, __nv_bfloat16* __restrict__ sd,
+                                                        float* __restrict__ grad, float* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* w_s = reinterpret_cast<__nv_bfloat16*>(smem);
     float* b_s = reinterpret_cast<float*>(smem + kW16Elems * 2);
-    float* g_s = b_s + kBiasElems;  // kParams floats, flat parameter layout
-    TrainTile* tiles = reinterpret_cast<TrainTile*>(g_s + kParams);
+    float* gb_s = b_s + kBiasElems;  // bias gradients, bias_offset layout
+    TrainTile* tiles = reinterpret_cast<TrainTile*>(gb_s + kBiasElems);
     load_weights(gv, w_s, b_s);
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) g_s[i] = 0.f;
+    for (int i = threadIdx.x; i < kBiasElems; i += blockDim.x) gb_s[i] = 0.f;
     __syncthreads();
     const float wsum = scalars[0];
-    const float gscale = -(wsum > 0.f ? (float)n / wsum : 1.f) / (float)n;  // -(w / mean w) / B = -w * gscale'
+    const float gscale = -(wsum > 0.f ? (float)total / wsum : 1.f) / (float)total;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     TrainTile& T = tiles[warp];
     float loss_acc = 0.f;
     const uint32_t tiles_total = (n + 15) / 16;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles_total; tile += gridDim.x * kWarps) {
+    auto stage = [&](const __nv_bfloat16* src, int src_stride, int cols, __nv_bfloat16* dst, int dst_stride,
+                     uint32_t row0) {
+        // 16 rows x cols bf16 (cols a multiple of 8) in 16-byte pieces
+        const int pieces = cols / 8;
+        for (int i = lane; i < 16 * pieces; i += 32) {
+            const int r = i / pieces, c = (i % pieces) * 8;
+            *reinterpret_cast<int4*>(dst + (size_t)(row0 + r) * dst_stride + c) =
+                *reinterpret_cast<const int4*>(src + r * src_stride + c);
+        }
+    };
+    for (uint32_t tile = blockIdx.x * kGrWarps + warp; tile < tiles_total; tile += gridDim.x * kGrWarps) {
         const uint32_t row0 = tile * 16;
         if (lane < 16) {
             float* f = T.feat + lane * 16;
@@ -80,8 +112,7 @@ __global__ void __launch_bounds__(kThreads) k_gradient(GuideView gv, const float
             encode_row(f, T.x + lane * kXStride);
         }
         __syncwarp();
-        const __nv_bfloat16* x = T.x;
-        dense_forward<kIn, kHid, true>(x, kXStride, w_s + w16_offset(0), layer_stride(0), b_s + bias_offset(0), T.h[0],
+        dense_forward<kIn, kHid, true>(T.x, kXStride, w_s + w16_offset(0), layer_stride(0), b_s + bias_offset(0), T.h[0],
                                        kHStride, nullptr, 0);
         __syncwarp();
         for (int l = 1; l < 4; ++l) {
@@ -92,7 +123,9 @@ __global__ void __launch_bounds__(kThreads) k_gradient(GuideView gv, const float
         dense_forward<kHid, kOut, false>(T.h[3], kHStride, w_s + w16_offset(4), layer_stride(4), b_s + bias_offset(4),
                                          nullptr, 0, T.y, kOut);
         __syncwarp();
-        // loss gradient per row: dY (bf16, 16 x 48 in dz[0]) and the output-layer bias gradient
+        stage(T.x, kXStride, kIn, sx + stage_x_offset(0), kStageX, row0);
+        for (int l = 1; l <= 4; ++l) stage(T.h[l - 1], kHStride, kHid, sx + stage_x_offset(l), kStageX, row0);
+        // loss gradient per row: dY (bf16) and the output-layer bias gradient (from the fp32 dY)
         if (lane < 16) {
             const float* f = T.feat + lane * 16;
             const float g = f[12] * gscale;
@@ -102,29 +135,23 @@ __global__ void __launch_bounds__(kThreads) k_gradient(GuideView gv, const float
             __nv_bfloat16* d = T.dz[0] + lane * kHStride;
             for (int i = 0; i < kOut; ++i) {
                 d[i] = __float2bfloat16_rn(dy[i]);
-                if (dy[i] != 0.f) atomicAdd(&g_s[param_offset(4) + kOut * kHid + i], dy[i]);
+                if (dy[i] != 0.f) atomicAdd(&gb_s[bias_offset(4) + i], dy[i]);
             }
         }
         __syncwarp();
-        // output layer
-        dense_backward_weight<kHid, kOut>(T.dz[0], kHStride, T.h[3], kHStride, g_s + param_offset(4));
+        stage(T.dz[0], kHStride, kOut, sd + stage_d_offset(4), kStageD, row0);
         dense_backward_data<kHid, kOut>(T.dz[0], kHStride, w_s + w16_offset(4), layer_stride(4), T.h[3], kHStride,
                                         T.dz[1], kHStride);
         __syncwarp();
         int cur = 1;
         for (int l = 3; l >= 0; --l) {
-            // bias gradient of layer l: column sums of dZ_l
             for (int c = lane; c < kHid; c += 32) {
-                float s = 0.f;
-                for (int r = 0; r < 16; ++r) s += __bfloat162float(T.dz[cur][r * kHStride + c]);
-                atomicAdd(&g_s[param_offset(l) + layer_out(l) * layer_in(l) + c], s);
+                float sum = 0.f;
+                for (int r = 0; r < 16; ++r) sum += __bfloat162float(T.dz[cur][r * kHStride + c]);
+                atomicAdd(&gb_s[bias_offset(l) + c], sum);
             }
-            const __nv_bfloat16* in = l == 0 ? T.x : T.h[l - 1];
-            const int ins = l == 0 ? kXStride : kHStride;
-            if (l == 0) {
-                dense_backward_weight<kIn, kHid>(T.dz[cur], kHStride, in, ins, g_s + param_offset(0));
-            } else {
-                dense_backward_weight<kHid, kHid>(T.dz[cur], kHStride, in, ins, g_s + param_offset(l));
+            stage(T.dz[cur], kHStride, kHid, sd + stage_d_offset(l), kStageD, row0);
+            if (l > 0) {
                 dense_backward_data<kHid, kHid>(T.dz[cur], kHStride, w_s + w16_offset(l), layer_stride(l), T.h[l - 1],
                                                 kHStride, T.dz[cur ^ 1], kHStride);
             }
@@ -135,8 +162,97 @@ __global__ void __launch_bounds__(kThreads) k_gradient(GuideView gv, const float
     for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xFFFFFFFFu, loss_acc, o);
     if (lane == 0 && loss_acc != 0.f) atomicAdd(loss, loss_acc);
     __syncthreads();
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x)
-        if (g_s[i] != 0.f) atomicAdd(&grad[i], g_s[i]);
+    for (int i = threadIdx.x; i < kBiasElems; i += blockDim.x) {
+        const int l = i < 4 * kHid ? i / kHid : 4;
+        const int c = i - bias_offset(l);
+        if (gb_s[i] != 0.f) atomicAdd(&grad[param_offset(l) + layer_out(l) * layer_in(l) + c], gb_s[i]);
+    }
+}
+
+// (layer, output row tile, input column tile) of output tile t (48 tiles of layer 0, 32 of layers 1-3,
+// 24 of layer 4)
+__device__ __forceinline__ void out_tile(int t, int& l, int& mt, int& nt) {
+    if (t < 48) {
+        l = 0; mt = t / 12; nt = t % 12;
+    } else if (t < 144) {
+        const int r = t - 48;
+        l = 1 + r / 32; mt = (r % 32) / 8; nt = r % 8;
+    } else {
+        const int r = t - 144;
+        l = 4; mt = r / 8; nt = r % 8;
+    }
+}
+
+// Pass 2: partial[block][param] for the weight entries, over records [block * per, (block + 1) * per).
+__global__ void __launch_bounds__(kGwThreads) k_grad_weights(const __nv_bfloat16* __restrict__ sx,
+                                                              const __nv_bfloat16* __restrict__ sd, uint32_t n,
+                                                              uint32_t per, float* __restrict__ partial) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* ds = xs + kGwRows * kGwXs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kPerWarp = kOutTiles / (kGwThreads / 32);  // 21
+    float acc[kPerWarp][4];
+#pragma unroll
+    for (int j = 0; j < kPerWarp; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    const uint32_t begin = blockIdx.x * per, end = min(n, begin + per);
+    const int jj = lane >> 3, rr = lane & 7;
+    for (uint32_t r0 = begin; r0 < end; r0 += kGwRows) {
+        // stage kGwRows records (zeros past `end`) into padded shared rows
+        constexpr int kXp = kStageX / 8, kDp = kStageD / 8;
+        for (int i = threadIdx.x; i < kGwRows * (kXp + kDp); i += kGwThreads) {
+            const int r = i / (kXp + kDp), c = i % (kXp + kDp);
+            int4 v = make_int4(0, 0, 0, 0);
+            if (r0 + r < end) {
+                v = c < kXp ? *reinterpret_cast<const int4*>(sx + (size_t)(r0 + r) * kStageX + c * 8)
+                            : *reinterpret_cast<const int4*>(sd + (size_t)(r0 + r) * kStageD + (c - kXp) * 8);
+            }
+            if (c < kXp) *reinterpret_cast<int4*>(xs + r * kGwXs + c * 8) = v;
+            else *reinterpret_cast<int4*>(ds + r * kGwDs + (c - kXp) * 8) = v;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int ks = 0; ks < kGwRows / 16; ++ks) {
+            const __nv_bfloat16* X = xs + ks * 16 * kGwXs;
+            const __nv_bfloat16* D = ds + ks * 16 * kGwDs;
+#pragma unroll
+            for (int j = 0; j < kPerWarp; ++j) {
+                int l, mt, nt;
+                out_tile(warp + j * (kGwThreads / 32), l, mt, nt);
+                uint32_t a[4], b[2];
+                // A[m = out][k = record] = D^T, B[k = record][n = in] = X
+                ldsm_x4_t(a, D + ((jj >> 1) * 8 + rr) * kGwDs + stage_d_offset(l) + mt * 16 + (jj & 1) * 8);
+                ldsm_x2_t(b, X + (lane & 15) * kGwXs + stage_x_offset(l) + nt * 8);
+                mma16816(acc[j], a, b);
+            }
+        }
+        __syncthreads();
+    }
+    float* out = partial + (size_t)blockIdx.x * kParams;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int j = 0; j < kPerWarp; ++j) {
+        int l, mt, nt;
+        out_tile(warp + j * (kGwThreads / 32), l, mt, nt);
+        const int o0 = mt * 16 + g, i0 = nt * 8 + 2 * t, in = layer_in(l);
+        float* w = out + param_offset(l);
+        w[o0 * in + i0] = acc[j][0];
+        w[o0 * in + i0 + 1] = acc[j][1];
+        w[(o0 + 8) * in + i0] = acc[j][2];
+        w[(o0 + 8) * in + i0 + 1] = acc[j][3];
+    }
+}
+
+// Pass 3: grad[weight entries] += the blocks' partials.
+__global__ void k_grad_reduce(const float* __restrict__ partial, uint32_t blocks, float* __restrict__ grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kParams) return;
+    int l = 0;
+    while (l < kLayers - 1 && i >= param_offset(l + 1)) ++l;
+    if (i - param_offset(l) >= layer_out(l) * layer_in(l)) return;  // a bias entry (pass 1)
+    float s = 0.f;
+    for (uint32_t b = 0; b < blocks; ++b) s += partial[(size_t)b * kParams + i];
+    grad[i] += s;
 }
 
 // Adam on the flat fp32 parameters; refreshes the bf16 weight image and fp32 biases.
@@ -178,7 +294,8 @@ __global__ void k_image(const float* __restrict__ p, __nv_bfloat16* __restrict__
 }
 
 size_t forward_smem() { return kW16Elems * 2 + kBiasElems * 4 + sizeof(FwdTile) * kWarps; }
-size_t gradient_smem() { return kW16Elems * 2 + kBiasElems * 4 + kParams * 4 + sizeof(TrainTile) * kWarps; }
+size_t grad_rows_smem() { return kW16Elems * 2 + 2 * kBiasElems * 4 + sizeof(TrainTile) * kGrWarps; }
+size_t grad_weights_smem() { return (size_t)kGwRows * (kGwXs + kGwDs) * 2; }
 
 }  // namespace guide
 
@@ -196,22 +313,41 @@ cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n
     return cudaGetLastError();
 }
 
+size_t guide_workspace_bytes() {
+    using namespace guide;
+    return (size_t)kChunkRows * (kStageX + kStageD) * 2 + (size_t)kGwMaxBlocks * kParams * 4;
+}
+
 cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
-                           cudaStream_t stream) {
+                           void* workspace, cudaStream_t stream) {
     using namespace guide;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gradient, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gradient_smem());
+        cudaFuncSetAttribute(k_grad_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_rows_smem());
+        cudaFuncSetAttribute(k_grad_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_weights_smem());
         attr = true;
     }
     cudaError_t e = cudaMemsetAsync(scalars, 0, 2 * sizeof(float), stream);
     if (e != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
+    __nv_bfloat16* sx = static_cast<__nv_bfloat16*>(workspace);
+    __nv_bfloat16* sd = sx + (size_t)kChunkRows * kStageX;
+    float* partial = reinterpret_cast<float*>(sd + (size_t)kChunkRows * kStageD);
     k_weight_sum<<<128, 256, 0, stream>>>(records, n, scalars);
-    const uint32_t tiles = (n + 15) / 16;
-    const int grid = (int)std::min<uint32_t>((tiles + kWarps - 1) / kWarps, 148u);
-    k_gradient<<<grid, kThreads, gradient_smem(), stream>>>(gv, records, n, scalars, grad, scalars + 1);
-    return cudaGetLastError();
+    for (uint32_t c0 = 0; c0 < n; c0 += kChunkRows) {
+        const uint32_t rows = std::min(kChunkRows, n - c0);
+        const uint32_t tiles = (rows + 15) / 16;
+        const int g1 = (int)std::min<uint32_t>((tiles + kGrWarps - 1) / kGrWarps, 148u);
+        k_grad_rows<<<g1, kGrThreads, grad_rows_smem(), stream>>>(gv, records + 16 * (size_t)c0, rows, n, scalars, sx, sd,
+                                                                grad, scalars + 1);
+        const uint32_t chunks = (rows + kGwRows - 1) / kGwRows;
+        const uint32_t blocks = std::min(kGwMaxBlocks, chunks);
+        const uint32_t per = (chunks + blocks - 1) / blocks * kGwRows;
+        k_grad_weights<<<blocks, kGwThreads, grad_weights_smem(), stream>>>(sx, sd, rows, per, partial);
+        k_grad_reduce<<<(kParams + 255) / 256, 256, 0, stream>>>(partial, blocks, grad);
+        if ((e = cudaGetLastError())) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace pb2
@@ -230,7 +366,8 @@ int pb2_guide_create(uint32_t seed, pb2_guide** out) {
     cudaError_t e;
     if ((e = cudaMalloc(&g->params, P * 4)) || (e = cudaMalloc(&g->m, P * 4)) || (e = cudaMalloc(&g->v, P * 4)) ||
         (e = cudaMalloc(&g->grad, P * 4)) || (e = cudaMalloc(&g->w16, guide::kW16Elems * 2)) ||
-        (e = cudaMalloc(&g->b32, guide::kBiasElems * 4)) || (e = cudaMalloc(&g->scalars, 16))) {
+        (e = cudaMalloc(&g->b32, guide::kBiasElems * 4)) || (e = cudaMalloc(&g->scalars, 16)) ||
+        (e = cudaMalloc(&g->workspace, guide_workspace_bytes()))) {
         pb2_guide_destroy(g);
         return cuda_fail(e, "pb2_guide_create");
     }
@@ -267,6 +404,7 @@ int pb2_guide_destroy(pb2_guide* g) {
     cudaFree(g->w16);
     cudaFree(g->b32);
     cudaFree(g->scalars);
+    cudaFree(g->workspace);
     delete g;
     return PB2_OK;
 }
@@ -304,7 +442,7 @@ int pb2_guide_gradient(pb2_guide* g, const float* records, uint32_t n, float* gr
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if ((e = cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s))) return cuda_fail(e, "memset grad");
-    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, s))) return cuda_fail(e, "guide gradient");
+    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, g->workspace, s))) return cuda_fail(e, "guide gradient");
     float sc[2] = { 0, 0 };
     if ((e = cudaMemcpyAsync(sc, g->scalars, 8, cudaMemcpyDeviceToHost, s))) return cuda_fail(e, "read loss");
     if (grad_host && (e = cudaMemcpyAsync(grad_host, g->grad, guide::kParams * 4, cudaMemcpyDeviceToHost, s)))
@@ -320,7 +458,7 @@ int pb2_guide_train(pb2_guide* g, const float* records, uint32_t n, float learni
     if (n == 0) return PB2_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
-    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, s))) return cuda_fail(e, "guide gradient");
+    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, g->workspace, s))) return cuda_fail(e, "guide gradient");
     g->step += 1;
     const float bc1 = 1.0f - std::pow(guide::kBeta1, (float)g->step);
     const float bc2 = 1.0f - std::pow(guide::kBeta2, (float)g->step);

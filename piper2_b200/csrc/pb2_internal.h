@@ -21,8 +21,10 @@ struct GuideView {
     const float* b32;
 };
 cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n, float* out, cudaStream_t stream);
+// Batch loss gradient (added to grad) and loss; `workspace` holds guide_workspace_bytes() of staging.
 cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
-                           cudaStream_t stream);
+                           void* workspace, cudaStream_t stream);
+size_t guide_workspace_bytes();
 
 cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
                              bool closest, bool count, uint32_t* work, unsigned long long* counters,
@@ -55,6 +57,7 @@ struct pb2_guide {
     __nv_bfloat16* w16 = nullptr;  // padded bf16 weight image used by the tensor-core tiles
     float* b32 = nullptr;
     float* scalars = nullptr;  // [0] weight sum of the batch, [1] loss
+    void* workspace = nullptr; // gradient staging (guide_workspace_bytes)
     uint32_t step = 0;
     pb2::GuideView view() const { return pb2::GuideView{ w16, b32 }; }
 };
