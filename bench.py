@@ -93,9 +93,13 @@ def mlp_bench():
     def fwd():
         capi.check(lib.pb2_guide_forward(g.h, C.c_void_p(feat.data_ptr()), n, C.c_void_p(out.data_ptr()), sp))
 
+    def fwd_mma():
+        capi.check(lib.pb2_guide_forward_mma(g.h, C.c_void_p(feat.data_ptr()), n, C.c_void_p(out.data_ptr()), sp))
+
     res = {}
     peak, kind = _bf16_peak()
-    for name, fn, flops in (("train_step_2^16", train, 3 * 43008 * b), ("forward_2^20", fwd, 43008 * n)):
+    for name, fn, flops in (("train_step_2^16", train, 3 * 43008 * b), ("forward_tcgen05_2^20", fwd, 43008 * n),
+                            ("forward_mma_sync_2^20", fwd_mma, 43008 * n)):
         for _ in range(3):
             fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -110,7 +114,9 @@ def mlp_bench():
         res[name] = {"ms": round(ms, 4), "tflops": round(tf, 2), "frac": round(tf / peak, 4)}
     res["peak_tflops"] = peak
     res["peak_source"] = kind
-    res["note"] = "mma.sync m16n8k16 bf16 tiles, 16 rows per warp; the network is 64 wide"
+    res["note"] = ("forward_tcgen05: tcgen05.mma kind::f16 M=128 per CTA, TMEM accumulators (one stream "
+                   "synchronisation per call included); forward_mma_sync and training: mma.sync m16n8k16 bf16 "
+                   "tiles; the network is 64 wide")
     return res
 
 

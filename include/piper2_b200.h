@@ -298,8 +298,14 @@ int pb2_guide_destroy(pb2_guide* guide);
 int pb2_guide_set_params(pb2_guide* guide, const float* params_host, uint32_t count);
 int pb2_guide_get_params(const pb2_guide* guide, float* params_host, uint32_t count);
 /* features_dev: n rows of 12 floats (position in the unit cube xyz, normal xyz, outgoing dir xyz, unused);
- * out_dev: n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused). */
+ * out_dev: n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused).  Runs on the
+ * tcgen05 tensor cores (128 rows per CTA, TMEM accumulators); synchronises `stream` to check that no
+ * tensor-core wait timed out (PB2_ERR_DEVICE_TIMEOUT). */
 int pb2_guide_forward(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev, void* stream);
+/* The same forward pass on mma.sync tiles (16 rows per warp), asynchronous; the cross-check of the tcgen05
+ * path and the form the integrator's per-bounce inference uses. */
+int pb2_guide_forward_mma(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev,
+                          void* stream);
 /* records_dev: n rows of 16 floats (position xyz, normal xyz, outgoing xyz, sampled direction xyz, weight =
  * target / sampling pdf, unused x3).  Gradient of the batch loss into grad_host (pb2_guide_param_count
  * floats, may be NULL) and the loss; parameters unchanged. */

@@ -336,14 +336,14 @@ class Guide:
         p = np.ascontiguousarray(params, dtype=np.float32)
         capi.check(capi.lib().pb2_guide_set_params(self.h, p.ctypes.data_as(C.c_void_p), len(p)))
 
-    def forward(self, features: np.ndarray) -> np.ndarray:
-        """features (n, 12) -> raw outputs (n, 48)."""
+    def forward(self, features: np.ndarray, tiles: str = "tcgen05") -> np.ndarray:
+        """features (n, 12) -> raw outputs (n, 48); tiles = "tcgen05" (default) or "mma" (mma.sync)."""
         torch = _torch()
         f = torch.from_numpy(np.ascontiguousarray(features, dtype=np.float32)).cuda()
         n = f.shape[0]
         out = torch.empty((n, 48), dtype=torch.float32, device="cuda")
-        capi.check(capi.lib().pb2_guide_forward(self.h, C.c_void_p(f.data_ptr()), n, C.c_void_p(out.data_ptr()),
-                                                _stream()))
+        fn = capi.lib().pb2_guide_forward if tiles == "tcgen05" else capi.lib().pb2_guide_forward_mma
+        capi.check(fn(self.h, C.c_void_p(f.data_ptr()), n, C.c_void_p(out.data_ptr()), _stream()))
         torch.cuda.synchronize()
         return out.cpu().numpy()
 

@@ -433,8 +433,22 @@ int pb2_guide_get_params(const pb2_guide* g, float* params, uint32_t count) {
 
 int pb2_guide_forward(const pb2_guide* g, const float* features, uint32_t n, float* out, void* stream) {
     if (!g || (n && (!features || !out))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward: null argument");
+    if (n == 0) return PB2_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t* flag = reinterpret_cast<uint32_t*>(g->scalars + 3);
+    cudaError_t e;
+    uint32_t h = 0;
+    if ((e = cudaMemsetAsync(flag, 0, 4, s)) || (e = guide_forward_tc(g->view(), features, n, out, flag, s)) ||
+        (e = cudaMemcpyAsync(&h, flag, 4, cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
+        return cuda_fail(e, "pb2_guide_forward");
+    if (h) return fail(PB2_ERR_DEVICE_TIMEOUT, "pb2_guide_forward: a tensor-core wait timed out");
+    return PB2_OK;
+}
+
+int pb2_guide_forward_mma(const pb2_guide* g, const float* features, uint32_t n, float* out, void* stream) {
+    if (!g || (n && (!features || !out))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward_mma: null argument");
     const cudaError_t e = guide_forward(g->view(), features, n, out, static_cast<cudaStream_t>(stream));
-    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "pb2_guide_forward");
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "pb2_guide_forward_mma");
 }
 
 int pb2_guide_gradient(pb2_guide* g, const float* records, uint32_t n, float* grad_host, float* loss_host, void* stream) {

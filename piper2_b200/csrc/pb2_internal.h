@@ -25,6 +25,10 @@ cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n
 cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
                            void* workspace, cudaStream_t stream);
 size_t guide_workspace_bytes();
+// The same forward pass on the tcgen05 tensor cores (guiding_tc.cu); error[0] is set if a tensor-core
+// wait timed out.
+cudaError_t guide_forward_tc(const GuideView& gv, const float* features, uint32_t n, float* out, uint32_t* error,
+                             cudaStream_t stream);
 
 cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
                              bool closest, bool count, uint32_t* work, unsigned long long* counters,
