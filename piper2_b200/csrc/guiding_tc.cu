@@ -1,237 +1,35 @@
-// guiding_tc.cu -- the guiding network's forward pass on the 5th-generation tensor cores (tcgen05).
-//
-// One CTA of 4 warps evaluates 128 rows at a time.  The encoded inputs and each hidden layer's output are
-// bf16 operands in shared memory in the canonical K-major, no-swizzle UMMA layout (8-row x 16-byte core
-// matrices; within a tile, core matrices adjacent in K are 128 bytes apart (LBO) and 8-row groups are
-// K x 16 bytes apart (SBO)); the weights of all five layers are staged once per CTA in the same layout.
-// For each layer one thread issues K/16 `tcgen05.mma.cta_group::1.kind::f16` (M = 128, N = 64 or 48,
-// BF16 x BF16 -> FP32) into a 64-column TMEM accumulator and commits them to an mbarrier; every warp then
-// reads its 32 rows back with `tcgen05.ld.32x32b`, adds the bias, applies ReLU, and writes the next layer's
-// bf16 operand (or the fp32 outputs after the last layer).  Shared-memory writes that an MMA reads are made
-// visible to the tensor core's async proxy with `fence.proxy.async.shared::cta` before the barrier.
-//
-// Every wait on the mbarrier is bounded: on time-out the kernel records an error, stops issuing work, gives
-// the tensor core a bounded time to drain, frees its TMEM and returns.
-#include <cuda_bf16.h>
-
-#include "guiding.cuh"
+// guiding_tc.cu -- the batched forward pass of the guiding network on the tcgen05 tensor cores
+// (pb2_guide_forward); the tile loop is in guiding_tc.cuh.
+#include "guiding_tc.cuh"
 #include "pb2_internal.h"
 
 namespace pb2 {
 namespace guide {
 namespace {
 
-constexpr int kTcRows = 128;
-constexpr int kTcThreads = 128;
-constexpr uint32_t kTmemCols = 64;
-constexpr uint32_t kWaitLimit = 1u << 20;  // mbarrier polls before a wait counts as failed
-
-__host__ __device__ constexpr int tc_w_offset(int l) {  // bytes of layer l's weights in the staged image
-    return l == 0 ? 0 : tc_w_offset(l - 1) + layer_out(l - 1) * layer_in(l - 1) * 2;
-}
-constexpr int kTcWBytes = tc_w_offset(kLayers);                        // 43,008
-constexpr int kTcXBytes = kTcRows * kIn * 2;                           // 24,576
-constexpr int kTcHBytes = kTcRows * kHid * 2;                          // 16,384
-constexpr int kTcOffW = 0;
-constexpr int kTcOffX = kTcWBytes;                                     // 1024-aligned below
-constexpr int kTcOffH0 = kTcOffX + kTcXBytes;
-constexpr int kTcOffH1 = kTcOffH0 + kTcHBytes;
-constexpr int kTcOffBias = kTcOffH1 + kTcHBytes;
-constexpr int kTcOffBar = kTcOffBias + kBiasElems * 4;
-constexpr int kTcSmem = kTcOffBar + 16;
-static_assert(kTcOffX % 1024 == 0 && kTcOffH0 % 1024 == 0 && kTcOffH1 % 1024 == 0, "operand alignment");
-
-// Byte offset of element (row, k) of a K-major operand with `kdim` columns in the core-matrix layout.
-__host__ __device__ constexpr uint32_t core_offset(uint32_t row, uint32_t k, uint32_t kdim) {
-    return (row >> 3) * (kdim * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version of sm_100; base offset 0, no swizzle
-    return d;
-}
-
-// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M = 128, N = n.
-__device__ __forceinline__ uint32_t instr_desc(uint32_t n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+// features: n rows of 12 floats (pos01 xyz, normal xyz, wo xyz, unused); out: n rows of 48 raw outputs
+struct FeatureRows {
+    const float* feat;
+    float* out;
+    __device__ __forceinline__ void features(uint32_t row, float (&f)[9], uint32_t& key) const {
+        for (int i = 0; i < 9; ++i) f[i] = feat[12 * (size_t)row + i];
+        key = row;
+    }
+    __device__ __forceinline__ void output(uint32_t key, const float (&y)[kOut]) const {
+        float* o = out + (size_t)key * kOut;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
+        for (int i = 0; i < kOut; i += 4) *reinterpret_cast<float4*>(o + i) = make_float4(y[i], y[i + 1], y[i + 2], y[i + 3]);
+    }
+};
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-}  // namespace
-
-// features: n rows of 12 floats (pos01 xyz, normal xyz, wo xyz, unused); out: n rows of 48 raw outputs.
-// error[0] is set when a tensor-core wait timed out.
 __global__ void __launch_bounds__(kTcThreads) k_forward_tc(GuideView gv, const float* __restrict__ features, uint32_t n,
                                                            float* __restrict__ out, uint32_t* __restrict__ error) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* w_s = smem + kTcOffW;
-    unsigned char* x_s = smem + kTcOffX;
-    unsigned char* h_s[2] = { smem + kTcOffH0, smem + kTcOffH1 };
-    float* b_s = reinterpret_cast<float*>(smem + kTcOffBias);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcOffBar);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 8);
-    uint32_t& s_fail = *reinterpret_cast<uint32_t*>(smem + kTcOffBar + 12);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time
-    for (int l = 0; l < kLayers; ++l) {
-        const int in = layer_in(l), outd = layer_out(l), chunks = outd * (in / 8);
-        for (int c = tid; c < chunks; c += kTcThreads) {
-            const int o = c / (in / 8), kc = c % (in / 8);
-            const int4 v = *reinterpret_cast<const int4*>(gv.w16 + w16_offset(l) + o * layer_stride(l) + kc * 8);
-            *reinterpret_cast<int4*>(w_s + tc_w_offset(l) + core_offset(o, kc * 8, in)) = v;
-        }
-    }
-    for (int i = tid; i < kBiasElems; i += kTcThreads) b_s[i] = gv.b32[i];
-    if (tid == 0) {
-        s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemCols));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t bar_addr = smem_u32(bar);
-    uint32_t phase = 0;
-    bool failed = false;
-
-    const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
-        const uint32_t row = tile * kTcRows + tid;
-        {
-            float f[9] = { 0, 0, 0, 0, 0, 1, 0, 0, 1 };
-            if (row < n)
-                for (int i = 0; i < 9; ++i) f[i] = features[12 * (size_t)row + i];
-            __align__(16) __nv_bfloat16 enc[kIn];
-            encode_row(f, enc);
-#pragma unroll
-            for (int kc = 0; kc < kIn / 8; ++kc)
-                *reinterpret_cast<int4*>(x_s + core_offset(tid, kc * 8, kIn)) = *reinterpret_cast<const int4*>(enc + kc * 8);
-        }
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        const unsigned char* a_buf = x_s;
-        for (int l = 0; l < kLayers; ++l) {
-            const uint32_t kdim = layer_in(l), ndim = layer_out(l);
-            if (tid == 0) {
-                const uint32_t a0 = smem_u32(a_buf), b0 = smem_u32(w_s + tc_w_offset(l));
-                for (uint32_t s = 0; s < kdim / 16; ++s)
-                    mma_bf16(tmem, smem_desc(a0 + 256 * s, 128, kdim * 16), smem_desc(b0 + 256 * s, 128, kdim * 16),
-                             instr_desc(ndim), s > 0 ? 1u : 0u);
-                mma_commit(bar_addr);
-            }
-            if (!mbar_wait_bounded(bar_addr, phase)) {
-                atomicExch(&s_fail, 1u);
-                atomicExch(error, 1u);
-            }
-            phase ^= 1u;
-            tc_fence_after();
-            __syncthreads();
-            if (s_fail) {
-                failed = true;
-                break;
-            }
-            // epilogue: this warp's 32 rows (TMEM lanes 32 warp ..), 16 columns at a time
-            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-            for (uint32_t c0 = 0; c0 < ndim; c0 += 16) {
-                float v[16];
-                tmem_ld16(lane_base + c0, v);
-                tmem_wait_ld();
-                const float* bias = b_s + bias_offset(l) + c0;
-                if (l < kLayers - 1) {
-                    __align__(16) __nv_bfloat16 hv[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) hv[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[i], 0.0f));
-                    unsigned char* dst = h_s[l & 1];
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0 + 8, kHid)) =
-                        *reinterpret_cast<const int4*>(hv + 8);
-                } else if (row < n) {
-                    float* o = out + (size_t)row * kOut + c0;
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4)
-                        *reinterpret_cast<float4*>(o + i) =
-                            make_float4(v[i] + bias[i], v[i + 1] + bias[i + 1], v[i + 2] + bias[i + 2], v[i + 3] + bias[i + 3]);
-                }
-            }
-            a_buf = h_s[l & 1];
-            fence_async_smem();
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-        }
-    }
-    if (failed && tid == 0) {
-        // give any MMA still in flight a bounded time to finish before its TMEM is freed
-        mbar_wait_bounded(bar_addr, phase);
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    forward_tc_tiles(gv, n, FeatureRows{ features, out }, error, smem);
 }
 
-size_t forward_tc_smem() { return (size_t)kTcSmem; }
-
+}  // namespace
 }  // namespace guide
-
 cudaError_t guide_forward_tc(const GuideView& gv, const float* features, uint32_t n, float* out, uint32_t* error,
                              cudaStream_t stream) {
     using namespace guide;

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "guiding.cuh"
+#include "guiding_tc.cuh"
 #include "pb2_internal.h"
 #include "shading.cuh"
 #include "traverse.cuh"
@@ -90,6 +91,7 @@ enum : int {
     C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24,
     C_CHECK = 25,  // 25..28: first failed index check (code, kernel, slot, value)
     C_FREE0 = 29,  // 29, 30: batched launches, slots freed (ping-pong with the extend queues)
+    C_TC_ERROR = 31,  // a tensor-core wait of the guide inference timed out
     C_COUNT = 32
 };
 
@@ -862,67 +864,57 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
 
 // ---- guide inference for the surface queues of the guided material types ------------------------------
 
-__global__ void __launch_bounds__(guide::kThreads) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
-    using namespace guide;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* w_s = reinterpret_cast<__nv_bfloat16*>(smem);
-    float* b_s = reinterpret_cast<float*>(smem + kW16Elems * 2);
-    FwdTile* tiles = reinterpret_cast<FwdTile*>(smem + kW16Elems * 2 + kBiasElems * 4);
-    load_weights(gs.net, w_s, b_s);
-    __syncthreads();
-    uint32_t counts[kNumSurfaceTypes], total = 0;
+// Rows of the guide's forward pass: the vertices in the guided material types' surface queues, in queue
+// order; a row's key is its path slot, whose mixture parameters the output writes.
+struct GuideRows {
+    SceneView sv;
+    Paths ps;
+    GuideState gs;
+    uint32_t counts[kNumSurfaceTypes];
+    __device__ __forceinline__ void features(uint32_t row, float (&f)[9], uint32_t& slot) const {
+        uint32_t idx = row;
+        int t = 0;
+        while (idx >= counts[t]) { idx -= counts[t]; ++t; }
+        slot = ps.surf[t][idx];
+        const float4 h = ps.hit[slot];
+        const float4 o4 = ps.o[slot], d4 = ps.d[slot];
+        const v3 d = mk3(d4.x, d4.y, d4.z);
+        const v3 hit = add3(mk3(o4.x, o4.y, o4.z), mul3s(d, h.x));
+        const float4* t4 = reinterpret_cast<const float4*>(sv.bvh.tris + ps.hit_slot[slot]);
+        const float4 a = t4[0], b = t4[1], c = t4[2];
+        const v3 ng = normalize3(cross3(sub3(mk3(b.x, b.y, b.z), mk3(a.x, a.y, a.z)),
+                                        sub3(mk3(c.x, c.y, c.z), mk3(a.x, a.y, a.z))));
+        const v3 N = dot3(d, ng) < 0.0f ? ng : neg3(ng);
+        f[0] = (hit.x - gs.bmin[0]) * gs.binv[0];
+        f[1] = (hit.y - gs.bmin[1]) * gs.binv[1];
+        f[2] = (hit.z - gs.bmin[2]) * gs.binv[2];
+        f[3] = N.x; f[4] = N.y; f[5] = N.z;
+        f[6] = -d.x; f[7] = -d.y; f[8] = -d.z;
+    }
+    __device__ __forceinline__ void output(uint32_t slot, const float (&y)[guide::kOut]) const {
+        guide::Mixture m;
+        guide::mixture_from_raw(y, m);
+        float* mp = gs.mix + 40 * (size_t)slot;
+        for (int k = 0; k < guide::kLobes; ++k) {
+            mp[k] = m.w[k];
+            mp[8 + 3 * k] = m.mu[k][0];
+            mp[9 + 3 * k] = m.mu[k][1];
+            mp[10 + 3 * k] = m.mu[k][2];
+            mp[32 + k] = m.kappa[k];
+        }
+    }
+};
+
+// The guide's mixture for every vertex of the guided material types, on the tcgen05 tensor cores.
+__global__ void __launch_bounds__(guide::kTcThreads) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    GuideRows rows{ sv, ps, gs, {} };
+    uint32_t total = 0;
     for (int t = 0; t < kNumSurfaceTypes; ++t) {
-        counts[t] = guided_type(t) ? ps.counts[C_SURF0 + t] : 0u;
-        total += counts[t];
+        rows.counts[t] = guided_type(t) ? ps.counts[C_SURF0 + t] : 0u;
+        total += rows.counts[t];
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    FwdTile& T = tiles[warp];
-    uint32_t slots16 = 0;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < (total + 15) / 16; tile += gridDim.x * kWarps) {
-        const uint32_t row = tile * 16 + lane;
-        uint32_t slot = 0xFFFFFFFFu;
-        if (lane < 16) {
-            float f[9] = { 0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f };
-            if (row < total) {
-                uint32_t idx = row;
-                int t = 0;
-                while (idx >= counts[t]) { idx -= counts[t]; ++t; }
-                slot = ps.surf[t][idx];
-                const float4 h = ps.hit[slot];
-                const float4 o4 = ps.o[slot], d4 = ps.d[slot];
-                const v3 d = mk3(d4.x, d4.y, d4.z);
-                const v3 hit = add3(mk3(o4.x, o4.y, o4.z), mul3s(d, h.x));
-                const float4* t4 = reinterpret_cast<const float4*>(sv.bvh.tris + ps.hit_slot[slot]);
-                const float4 a = t4[0], b = t4[1], c = t4[2];
-                const v3 ng = normalize3(cross3(sub3(mk3(b.x, b.y, b.z), mk3(a.x, a.y, a.z)),
-                                                sub3(mk3(c.x, c.y, c.z), mk3(a.x, a.y, a.z))));
-                const v3 N = dot3(d, ng) < 0.0f ? ng : neg3(ng);
-                f[0] = (hit.x - gs.bmin[0]) * gs.binv[0];
-                f[1] = (hit.y - gs.bmin[1]) * gs.binv[1];
-                f[2] = (hit.z - gs.bmin[2]) * gs.binv[2];
-                f[3] = N.x; f[4] = N.y; f[5] = N.z;
-                f[6] = -d.x; f[7] = -d.y; f[8] = -d.z;
-            }
-            encode_row(f, T.x + lane * kXStride);
-        }
-        __syncwarp();
-        forward_tile(w_s, b_s, T.x, T.h[0], T.h[1], T.y);
-        if (lane < 16 && slot != 0xFFFFFFFFu) {
-            Mixture m;
-            mixture_from_raw(T.y + lane * kOut, m);
-            float* mp = gs.mix + 40 * (size_t)slot;
-            for (int k = 0; k < kLobes; ++k) {
-                mp[k] = m.w[k];
-                mp[8 + 3 * k] = m.mu[k][0];
-                mp[9 + 3 * k] = m.mu[k][1];
-                mp[10 + 3 * k] = m.mu[k][2];
-                mp[32 + k] = m.kappa[k];
-            }
-            ++slots16;
-        }
-        __syncwarp();
-    }
-    (void)slots16;
+    guide::forward_tc_tiles(gs.net, total, rows, ps.counts + C_TC_ERROR, smem);
 }
 
 // Per spatial cell (res^3 cells over the scene box) sum and count of the records' weights.
@@ -1212,7 +1204,7 @@ static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
     return PB2_OK;
 }
 
-static size_t infer_smem() { return (size_t)guide::kW16Elems * 2 + guide::kBiasElems * 4 + guide::kWarps * sizeof(guide::FwdTile); }
+static size_t infer_smem() { return guide::forward_tc_smem(); }
 
 // Carves the SoA path state of `c` slots out of `base` (or only measures it when base is null); returns the
 // bytes used.  `batch` adds the per-slot scene ids and the two freed-slot queues.
@@ -1609,7 +1601,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         checked("k_trace_queue<extend>");
         k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_classify");
-        if (gs.enabled) k_guide_infer<<<pl->sms, guide::kThreads, infer_smem(), stream>>>(sv, ps, gs);
+        if (gs.enabled) k_guide_infer<<<pl->sms * 2, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
         checked("k_guide_infer");
         k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_shade<matte>");
@@ -1656,6 +1648,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
                                       std::to_string(counts[C_CHECK + 2]) + ", value " +
                                       std::to_string(counts[C_CHECK + 3]));
     if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+    if (counts[C_TC_ERROR]) return fail(PB2_ERR_DEVICE_TIMEOUT, "guide inference: a tensor-core wait timed out");
     if (gs.enabled) {
         uint32_t tc[2];
         if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
