@@ -120,6 +120,22 @@ def mlp_bench():
     return res
 
 
+def truth_rel_mse(img, name):
+    """relMSE of a resolved image (H, W, 3) against a committed ground-truth pixel set
+    (tests/golden/truth_<name>.npz: the double-precision CPU render at 4096 spp of a seeded pixel sample,
+    made by tests/golden/make_truth.py): mean over those pixels and channels of (I - R)^2 / (R^2 + 0.01).
+    None if the set is absent."""
+    import numpy as np
+
+    path = os.path.join(ROOT, "tests", "golden", f"truth_{name}.npz")
+    if not os.path.exists(path):
+        return None
+    with np.load(path) as z:
+        px, ref = z["pixels"].astype(np.int64), z["rgb"]
+    val = np.asarray(img, dtype=np.float64)[px[:, 1], px[:, 0], :3]
+    return float(np.mean((val - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
 def _profile_traffic():
     """DRAM bytes per closest-hit launch from the committed ncu summary (None if absent)."""
     path = os.path.join(ROOT, "profiles", "trace_closest_soup1M.md")
@@ -405,7 +421,8 @@ def render_bench(args):
     """The render path: the Cornell-box configuration (256 x 256, 16 spp, depth 8) against the reference's own
     kernels compiled natively (oracle/_ref) on all host cores over a bounded crop; the mixed-materials
     configuration (3.1M triangles, 1920 x 1080, 64 spp, depth 16); guided vs plain on the hard-indirect room
-    at reduced size."""
+    at reduced size.  Every image's relMSE is also taken against the double-precision CPU render at 4096 spp
+    (a committed pixel sample, tests/golden/truth_*.npz)."""
     import torch
 
     import oracle_py
@@ -417,6 +434,9 @@ def render_bench(args):
     with api.Pipeline(sd) as pl:
         out = {"workload": "Cornell box 256x256, 16 spp, max depth 8, NEE+MIS (plain BxDF sampling)"}
         out.update(_render_rate(pl, pl.rect, st.samples_per_pixel, st.samples_per_pixel, frames=max(3, args.steps // 2)))
+        film = pl.new_film()
+        pl.launch(film, sample_begin=0, sample_count=st.samples_per_pixel)
+        out["relmse_vs_fp64_4096spp"] = truth_rel_mse(pl.resolve(film).cpu().numpy(), "cornell_256x256")
     if oracle_py.ref_available():
         crop = capi.Rect(0, 96, 256, 16)
         rs = oracle_py.RefScene(sd, use_bvh=True)
@@ -434,11 +454,16 @@ def render_bench(args):
         mm = {"workload": "mixed materials 1920x1080, 64 spp, max depth 16, 3.1M triangles (terrain + 200 "
                           "icospheres: Lambert / smooth dielectric / GGX conductor), env 0.5 + sun"}
         mm.update(_render_rate(pl, pl.rect, md.settings.samples_per_pixel, 8))
+        film = pl.new_film()
+        for b in range(0, md.settings.samples_per_pixel, 8):
+            pl.launch(film, sample_begin=b, sample_count=8)
+        mm["relmse_vs_fp64_4096spp"] = truth_rel_mse(pl.resolve(film).cpu().numpy(), "mixed_materials_1920x1080")
     result["mixed_materials"] = mm
     torch.cuda.empty_cache()
     result["batch"] = batch_bench()
     torch.cuda.empty_cache()
-    g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512)
+    g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512,
+                              truth=lambda img: truth_rel_mse(img, "guiding_room_640x360"))
     result["guiding"] = g
     result["guiding_mlp"] = mlp_bench()
     return result

@@ -3,6 +3,7 @@
 Outputs (git-ignored):
   oracle/_build/sobol_tables.h   generated Sobol tables (same generator as the product)
   oracle/_build/liboracle.so     the C restatement (pb2_oracle.c)
+  oracle/_build/liboracle_fp64.so the same source built with -DOR_FP64: double-precision ground truth
   oracle/_ref/librefcpu.so       the reference's own device code compiled natively with a host shim,
                                  only when the reference sources are present (see oracle/ref/Makefile)
 
@@ -59,6 +60,9 @@ def build_oracle(force: bool = False) -> str:
             os.path.join(ROOT, "include", "piper2_b200.h")]
     if force or _stale(out, deps):
         _run(["gcc", *CFLAGS, "-I", BUILD, "-shared", "-o", out, src, "-lm"])
+    out64 = os.path.join(BUILD, "liboracle_fp64.so")
+    if force or _stale(out64, deps):
+        _run(["gcc", *CFLAGS, "-DOR_FP64", "-I", BUILD, "-shared", "-o", out64, src, "-lm"])
     return out
 
 

@@ -1,4 +1,5 @@
-"""ctypes binding of the CPU oracle (liboracle.so) and of the reference harness (librefcpu.so).
+"""ctypes binding of the CPU oracle (liboracle.so), its double-precision build (liboracle_fp64.so, the
+ground truth of error measurements) and of the reference harness (librefcpu.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline.
 """
@@ -18,23 +19,27 @@ if ROOT not in sys.path:
 from piper2_b200 import capi  # noqa: E402  (struct layouts of include/piper2_b200.h)
 
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+ORACLE64_SO = os.path.join(HERE, "_build", "liboracle_fp64.so")
 REF_SO = os.path.join(HERE, "_ref", "librefcpu.so")
 
 _or = None
+_or64 = None
 _ref = None
+
+
+def _load(path):
+    if not os.path.exists(path):
+        sys.path.insert(0, HERE)
+        from build_oracle import build_oracle as _b
+
+        _b()
+    return C.CDLL(path)
 
 
 def oracle():
     global _or
     if _or is None:
-        if not os.path.exists(ORACLE_SO):
-            import build_oracle  # noqa: F401
-
-            sys.path.insert(0, HERE)
-            from build_oracle import build_oracle as _b
-
-            _b()
-        h = C.CDLL(ORACLE_SO)
+        h = _load(ORACLE_SO)
         h.or_sobol_sample.restype = C.c_float
         h.or_sobol_sample.argtypes = [C.c_uint64, C.c_uint32]
         h.or_sobol_sample_scrambled.restype = C.c_float
@@ -68,8 +73,28 @@ def oracle():
         h.or_plane_make.argtypes = [C.POINTER(C.c_float)] * 3 + [C.POINTER(capi.Plane)]
         h.or_intersect_triangle.restype = C.c_int
         h.or_intersect_triangle.argtypes = [C.POINTER(C.c_float)] * 4 + [C.POINTER(C.c_float)] * 3
+        _bind_pixels(h)
         _or = h
     return _or
+
+
+def _bind_pixels(h):
+    h.or_scene_create.restype = C.c_void_p
+    h.or_scene_create.argtypes = [C.POINTER(capi.Scene), C.c_int]
+    h.or_scene_destroy.argtypes = [C.c_void_p]
+    h.or_render_pixels.restype = C.c_int
+    h.or_render_pixels.argtypes = [C.c_void_p, C.POINTER(capi.RenderSettings), C.c_void_p, C.c_uint32, C.c_uint32,
+                                   C.c_uint32, C.c_void_p, C.c_int]
+
+
+def oracle_fp64():
+    """The double-precision build of the same restatement (ground truth)."""
+    global _or64
+    if _or64 is None:
+        h = _load(ORACLE64_SO)
+        _bind_pixels(h)
+        _or64 = h
+    return _or64
 
 
 def ref_available() -> bool:
@@ -166,6 +191,41 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(f"or_render failed: {rc}")
         return film, out
+
+    def render_pixels(self, pixels, sample_begin, sample_count, threads=0):
+        """Single-precision oracle: resolved RGB of chosen pixels (same accumulation as TruthScene)."""
+        return render_pixels(oracle(), self.h, self.data.settings, pixels, sample_begin, sample_count, threads)
+
+
+def render_pixels(lib, handle, settings, pixels, sample_begin, sample_count, threads=0):
+    """Resolved (radiance / weight) RGB of the film pixels `pixels` ((n, 2) x, y) over the given samples."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    out = np.zeros((len(px), 4), dtype=np.float64)
+    rc = lib.or_render_pixels(handle, C.byref(settings), px.ctypes.data, len(px), sample_begin, sample_count,
+                              out.ctypes.data, threads or os.cpu_count())
+    if rc != 0:
+        raise RuntimeError(f"or_render_pixels failed: {rc}")
+    return out[:, :3] / np.maximum(out[:, 3:4], 1e-300)
+
+
+class TruthScene:
+    """A scene in the double-precision restatement: ground-truth pixel values for relMSE."""
+
+    def __init__(self, scene_data, use_bvh=True):
+        self.data = scene_data
+        self._sc, self._keep = scene_data.to_ctypes()
+        self.h = oracle_fp64().or_scene_create(C.byref(self._sc), 1 if use_bvh else 0)
+
+    def close(self):
+        if self.h:
+            oracle_fp64().or_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def render_pixels(self, pixels, sample_begin, sample_count, threads=0):
+        return render_pixels(oracle_fp64(), self.h, self.data.settings, pixels, sample_begin, sample_count, threads)
 
 
 class RefScene:

@@ -60,6 +60,13 @@ const float* or_triangle_vertices(const or_scene* s, uint32_t prim);
  * Returns 0, or a negative value if the settings are not supported. */
 int or_render(const or_scene* s, const pb2_render_settings* settings, const pb2_rect* rect,
               uint32_t sample_begin, uint32_t sample_count, float* rgbw, float* sample_out, int threads);
+/* Resolved film value of chosen pixels: for each (x, y) in `pixels` (npix pairs), the sums of
+ * radiance x filter weight (r, g, b) and of the weights over every sample of samples
+ * [sample_begin, sample_begin + sample_count) whose splat reaches the pixel, accumulated in double
+ * (out: npix x 4).  In liboracle_fp64.so (built with -DOR_FP64) every path is computed in double:
+ * the ground truth of the error measurements. */
+int or_render_pixels(const or_scene* s, const pb2_render_settings* settings, const uint32_t* pixels,
+                     uint32_t npix, uint32_t sample_begin, uint32_t sample_count, double* out, int threads);
 void or_calc_render_rect(uint32_t width, uint32_t height, float device_aspect, uint32_t fit_mode,
                          pb2_ndc_transform* transform, pb2_rect* rect);
 void or_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out);

@@ -10,6 +10,10 @@ proportional to time x relMSE.  `speedup` = (T_plain relMSE_plain) / (T_guided r
 time includes its online training.  The reference's own noise adds the same amount to both errors, so the
 reported speed-up is, if anything, an underestimate.
 
+`truth`, if given, is a second error measure: a function image (H, W, 3) -> relMSE against an independent
+ground truth (the bench passes the double-precision CPU render at 4096 spp over a pixel sample); its
+errors and speed-up are reported as `relmse_fp64` / `speedup_fp64`.
+
     python -m piper2_b200.guiding_eval [--width 640 --height 360 --spp 64 --ref-spp 1024]
 """
 from __future__ import annotations
@@ -36,7 +40,7 @@ def rel_mse(img, ref):
 
 def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
-             weight_quantile=0.99, spatial_cells=0):
+             weight_quantile=0.99, spatial_cells=0, truth=None):
     import torch
 
     from . import api, scenes
@@ -75,6 +79,11 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
         "relmse_ratio": e_plain / e_guided if e_guided > 0 else None,
         "speedup": (t_plain * e_plain) / (t_guided * e_guided) if e_guided > 0 else None,
     })
+    if truth is not None:
+        f_plain, f_guided = truth(plain), truth(guided)
+        out["plain"]["relmse_fp64"] = f_plain
+        out["guided"]["relmse_fp64"] = f_guided
+        out["speedup_fp64"] = (t_plain * f_plain) / (t_guided * f_guided) if f_guided > 0 else None
     return out
 
 

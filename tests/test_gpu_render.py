@@ -195,3 +195,27 @@ def test_invalid_settings_rejected():
     st.max_depth = 200
     with pytest.raises(capi.PB2Error):
         _api().Pipeline(sd, st)
+
+
+def test_cornell_converges_to_fp64_truth():
+    """The GPU estimator converges to the independent double-precision CPU render (4096 spp of disjoint
+    samples, tests/golden/truth_cornell_256x256.npz): at the truth's pixels the relMSE falls with the
+    sample count as Monte-Carlo error should (about 1/spp: 16 -> 256 spp must gain at least 8x), and the
+    256-spp mean agrees with the truth's mean within 1 %."""
+    import os
+
+    with np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                              "truth_cornell_256x256.npz")) as z:
+        px, ref = z["pixels"].astype(np.int64), z["rgb"]
+    sd = scenes.cornell_box(seed=0)
+    errs, means = {}, {}
+    with _api().Pipeline(sd) as pl:
+        for spp in (16, 256):
+            film = pl.new_film()
+            for b in range(0, spp, 16):
+                pl.launch(film, sample_begin=b, sample_count=16)
+            img = pl.resolve(film).cpu().numpy().astype(np.float64)[px[:, 1], px[:, 0]]
+            errs[spp] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+            means[spp] = float(img.mean())
+    assert errs[256] * 8 < errs[16], errs
+    assert abs(means[256] / ref.mean() - 1) < 0.01, (means, ref.mean())

@@ -213,3 +213,56 @@ def test_owen_scrambling_keeps_stratification(oracle):
         assert np.mean(a != b) > 0.9
     # scramble = 0 is the unscrambled sampler
     assert all(lib.or_sobol_sample_scrambled(i, 9, 0, 5) == lib.or_sobol_sample(i, 9) for i in range(200))
+
+
+def test_pixel_render_equals_film_resolve(oracle):
+    """or_render_pixels gathers, per pixel, exactly the samples whose 2x2 splat reaches it: its resolved
+    values equal the resolved film of or_render over the same samples (border and interior pixels)."""
+    sd = scenes.cornell_box(seed=0, width=32, height=32, spp=4)
+    o = oracle.OracleScene(sd, use_bvh=False)
+    film, _ = o.render(sd.settings, samples=False)
+    pix = np.array([(0, 0), (31, 31), (0, 17), (13, 0), (5, 9), (16, 16), (30, 2), (21, 27)], dtype=np.uint32)
+    got = o.render_pixels(pix, 0, 4)
+    want = film[pix[:, 1], pix[:, 0], :3] / film[pix[:, 1], pix[:, 0], 3:4]
+    np.testing.assert_allclose(got, want, rtol=2e-6, atol=1e-7)
+
+
+def test_fp64_truth_is_the_same_estimator(oracle):
+    """The double-precision build follows the same sample points and branches: per pixel over the same
+    samples it agrees with the single-precision oracle to float rounding (rare paths may take another
+    branch at a rounding boundary, so the bound is on the median and the mean)."""
+    sd = scenes.guiding_room(seed=0, width=64, height=36, spp=4, tess=3)
+    rng = np.random.default_rng(5)
+    pix = np.stack([rng.integers(0, 64, 96), rng.integers(0, 36, 96)], 1).astype(np.uint32)
+    a = oracle.OracleScene(sd).render_pixels(pix, 0, 16)
+    b = oracle.TruthScene(sd).render_pixels(pix, 0, 16)
+    rel = np.abs(a - b) / (np.abs(b) + 1e-4)
+    assert np.median(rel) < 1e-5, np.median(rel)
+    assert np.mean(rel) < 1e-3, np.mean(rel)
+
+
+@pytest.mark.parametrize("name", ["cornell_256x256", "guiding_room_640x360", "guiding_room_1280x720",
+                                  "mixed_materials_1920x1080"])
+def test_truth_sets_consistent(oracle, name):
+    """Each committed ground-truth set (double precision, 4096 spp over a pixel sample) names its sample
+    range, holds distinct in-film pixels, and agrees with a fresh 16-spp single-precision render of
+    disjoint samples at those pixels in the mean (within five standard errors of the difference)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_truth", os.path.join(GOLDEN, "make_truth.py"))
+    mt = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mt)
+    pixels, ref = mt.load(name)
+    with np.load(mt.path(name)) as z:
+        assert int(z["spp"]) == 4096 and int(z["sample_begin"]) == 4096
+    sd = mt.SETS[name][0]()
+    st = sd.settings
+    assert len(np.unique(pixels[:, 1] * st.width + pixels[:, 0])) == len(pixels)
+    assert pixels[:, 0].max() < st.width and pixels[:, 1].max() < st.height
+    sub = pixels[:: max(1, len(pixels) // 256)]
+    refs = ref[:: max(1, len(pixels) // 256)]
+    o = oracle.OracleScene(sd)
+    est = o.render_pixels(sub, 0, 16)
+    d = (est - refs).mean(axis=1)
+    se = d.std(ddof=1) / math.sqrt(len(d))
+    assert abs(d.mean()) < 5 * se + 1e-6, (d.mean(), se)
