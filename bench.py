@@ -421,7 +421,7 @@ def render_bench(args):
     """The render path: the Cornell-box configuration (256 x 256, 16 spp, depth 8) against the reference's own
     kernels compiled natively (oracle/_ref) on all host cores over a bounded crop; the mixed-materials
     configuration (3.1M triangles, 1920 x 1080, 64 spp, depth 16); guided vs plain on the hard-indirect room
-    at reduced size.  Every image's relMSE is also taken against the double-precision CPU render at 4096 spp
+    at its configuration (1280 x 720, 256 spp).  Every image's relMSE is also taken against the double-precision CPU render at 4096 spp
     (a committed pixel sample, tests/golden/truth_*.npz)."""
     import torch
 
@@ -462,8 +462,8 @@ def render_bench(args):
     torch.cuda.empty_cache()
     result["batch"] = batch_bench()
     torch.cuda.empty_cache()
-    g = guiding_eval.evaluate(width=640, height=360, spp=64, ref_spp=512,
-                              truth=lambda img: truth_rel_mse(img, "guiding_room_640x360"))
+    g = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0,
+                              truth=lambda img: truth_rel_mse(img, "guiding_room_1280x720"))
     result["guiding"] = g
     result["guiding_mlp"] = mlp_bench()
     return result

@@ -322,6 +322,9 @@ typedef struct pb2_guide_settings {
                                   (e.g. 0.99; 0 or 1 = no clamp) */
     uint32_t spatial_cells;    /* before clamping, each record's weight is divided by the mean weight of its
                                   cell in a spatial_cells^3 grid over the scene box (0 = off, at most 16) */
+    uint32_t guided_types;     /* bit t set: vertices of surface type t (PB2_SURFACE_*) sample the guide; only
+                                  Matte and Conductor may be set.  0 = Matte only: a glossy conductor's own
+                                  sampler is already close to the product with the incident light */
 } pb2_guide_settings;
 
 /* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */

@@ -175,6 +175,7 @@ struct GuideState {
     float accept_prob;
     uint32_t salt;
     float bmin[3], binv[3];
+    uint32_t types;         // bit t set: vertices of surface type t sample the guide
 };
 
 // Where a kernel finds the launch parameters, scene and film of a path slot.
@@ -770,7 +771,7 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
             }
         }
         // continuation (PathTracing/Kernel.cpp:164-190); guided vertices sample 0.5 BxDF + 0.5 mixture
-        const bool guided = guided_type(kType) && gs.enabled && bsdf.no_specular;
+        const bool guided = guided_type(kType) && gs.enabled && ((gs.types >> kType) & 1u) && bsdf.no_specular;
         v3 wi_sh;
         spec fval;
         float pdf;
@@ -911,7 +912,7 @@ __global__ void __launch_bounds__(guide::kTcThreads) k_guide_infer(SceneView sv,
     GuideRows rows{ sv, ps, gs, {} };
     uint32_t total = 0;
     for (int t = 0; t < kNumSurfaceTypes; ++t) {
-        rows.counts[t] = guided_type(t) ? ps.counts[C_SURF0 + t] : 0u;
+        rows.counts[t] = guided_type(t) && ((gs.types >> t) & 1u) ? ps.counts[C_SURF0 + t] : 0u;
         total += rows.counts[t];
     }
     guide::forward_tc_tiles(gs.net, total, rows, ps.counts + C_TC_ERROR, smem);
@@ -1518,6 +1519,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         if ((rc = alloc_guide_slots(pl, (uint32_t)paths))) return rc;
         gs.enabled = 1;
         gs.sel_prob = pl->guide_settings.selection_prob;
+        gs.types = pl->guide_settings.guided_types;
         gs.net = pl->guide->view();
         gs.mix = pl->g_mix;
         gs.rec = pl->g_rec;
@@ -1587,13 +1589,22 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     ctx.sv = sv;
     ctx.film = film;
     ctx.sample_out = sample_out;
+    // The bounce kernels read their queue sizes on the device, so the host checks for completion only
+    // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
+    // the bounces between checks queue up without a host round trip.
+    constexpr int kCheckEvery = 4;
+    uint32_t active = paths > 0 ? 1u : 0u;
     for (int bounce = 0; !failed; ++bounce) {
-        uint32_t active = 0;
-        if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
-            (e = cudaStreamSynchronize(stream)))
-            return cuda_fail(e, "read queue size");
-        if (active == 0) break;
+        if (bounce % kCheckEvery == 0) {
+            if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     stream)) ||
+                (e = cudaStreamSynchronize(stream)))
+                return cuda_fail(e, "read queue size");
+            if (active == 0) break;
+        }
         if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
+        // grid from the last known queue size (an upper bound: queues only shrink); the persistent trace
+        // blocks stop when the queue is drained
         const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
         cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
         k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
@@ -1674,6 +1685,14 @@ int pb2_pipeline_set_guide(pb2_pipeline* pl, pb2_guide* guide, const pb2_guide_s
         return fail(PB2_ERR_INVALID_ARGUMENT, "weight_quantile must lie in [0, 1]");
     if (settings->spatial_cells > 16)
         return fail(PB2_ERR_INVALID_ARGUMENT, "spatial_cells must lie in [0, 16] per axis");
+    {
+        uint32_t allowed = 0;
+        for (int t = 0; t < kNumSurfaceTypes; ++t)
+            if (guided_type(t)) allowed |= 1u << t;
+        if (settings->guided_types & ~allowed)
+            return fail(PB2_ERR_INVALID_ARGUMENT, "guided_types: only Matte and Conductor vertices can be guided "
+                                                  "(their BxDFs report their samplers' true density)");
+    }
     if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
         return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
     cudaError_t e;
@@ -1691,6 +1710,10 @@ int pb2_pipeline_set_guide(pb2_pipeline* pl, pb2_guide* guide, const pb2_guide_s
     pl->g_offered = 0;
     pl->guide = guide;
     pl->guide_settings = *settings;
+    // default: Matte only.  A glossy conductor's visible-normal sampler is already close to its product with
+    // the incident light, and sending half of its samples to a broad guide lobe doubles its variance
+    // (measured on the hard-indirect room: relMSE at 128 spp 0.36 guiding both types, 0.27 Matte only).
+    if (pl->guide_settings.guided_types == 0) pl->guide_settings.guided_types = 1u << PB2_SURFACE_MATTE;
     return PB2_OK;
 }
 

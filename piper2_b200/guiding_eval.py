@@ -40,19 +40,21 @@ def rel_mse(img, ref):
 
 def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
-             weight_quantile=0.99, spatial_cells=0, truth=None):
+             weight_quantile=0.99, spatial_cells=0, truth=None, guided_types=0):
     import torch
 
     from . import api, scenes
 
     sd = scenes.guiding_room(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, tess=tess)
     out = {"workload": f"guiding room {width}x{height}, {spp} spp, max depth {max_depth}",
-           "reference": f"plain, {ref_spp} spp from samples [{spp}, {spp + ref_spp})"}
+           "reference": f"plain, {ref_spp} spp from samples [{spp}, {spp + ref_spp})" if ref_spp else None}
     with api.Pipeline(sd) as pl:
-        film = pl.new_film()
-        for s in range(0, ref_spp, chunk):
-            pl.launch(film, sample_begin=spp + s, sample_count=min(chunk, ref_spp - s))
-        ref = pl.resolve(film).cpu().numpy().astype(np.float64)
+        ref = None
+        if ref_spp:
+            film = pl.new_film()
+            for s in range(0, ref_spp, chunk):
+                pl.launch(film, sample_begin=spp + s, sample_count=min(chunk, ref_spp - s))
+            ref = pl.resolve(film).cpu().numpy().astype(np.float64)
         # plain: one launch of all samples (its fastest form), after a warm-up launch
         pl.launch(pl.new_film(), sample_begin=0, sample_count=min(spp, 4))
         film = pl.new_film()
@@ -61,28 +63,31 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
         # guided: fresh network, progressive passes with online training
         guide = api.Guide(seed=seed + 1)
         pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile,
-                     spatial_cells=spatial_cells)
+                     spatial_cells=spatial_cells, guided_types=guided_types)
         film = pl.new_film()
         t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
                                                                  learning_rate, train_passes))
         guided = pl.resolve(film).cpu().numpy().astype(np.float64)
         pl.set_guide(None)
-    e_plain, e_guided = rel_mse(plain, ref), rel_mse(guided, ref)
+    e_plain = rel_mse(plain, ref) if ref is not None else None
+    e_guided = rel_mse(guided, ref) if ref is not None else None
     out.update({
         "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
+                   "guided_types": guided_types or "matte",
                    "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,
                    "train_passes": train_passes, "learning_rate": learning_rate, "weight_quantile": weight_quantile,
                    "spatial_cells": spatial_cells,
                    "first_loss": losses[0] if losses else None, "last_loss": losses[-1] if losses else None},
-        "reference_mean": float(ref.mean()),
-        "relmse_ratio": e_plain / e_guided if e_guided > 0 else None,
-        "speedup": (t_plain * e_plain) / (t_guided * e_guided) if e_guided > 0 else None,
+        "reference_mean": float(ref.mean()) if ref is not None else None,
+        "relmse_ratio": e_plain / e_guided if e_guided else None,
+        "speedup": (t_plain * e_plain) / (t_guided * e_guided) if e_guided else None,
     })
     if truth is not None:
         f_plain, f_guided = truth(plain), truth(guided)
         out["plain"]["relmse_fp64"] = f_plain
         out["guided"]["relmse_fp64"] = f_guided
+        out["relmse_ratio_fp64"] = f_plain / f_guided if f_guided > 0 else None
         out["speedup_fp64"] = (t_plain * f_plain) / (t_guided * f_guided) if f_guided > 0 else None
     return out
 
