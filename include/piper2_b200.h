@@ -325,6 +325,8 @@ typedef struct pb2_guide_settings {
     uint32_t guided_types;     /* bit t set: vertices of surface type t (PB2_SURFACE_*) sample the guide; only
                                   Matte and Conductor may be set.  0 = Matte only: a glossy conductor's own
                                   sampler is already close to the product with the incident light */
+    uint32_t max_guided_depth; /* only vertices at path depth < max_guided_depth (0 = every depth) sample the
+                                  guide; the others keep plain BxDF sampling and skip its evaluation */
 } pb2_guide_settings;
 
 /* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */

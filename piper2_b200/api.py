@@ -186,14 +186,14 @@ class Pipeline:
         return s
 
     def set_guide(self, guide, selection_prob=0.5, record_capacity=1 << 20, weight_quantile=0.99, spatial_cells=0,
-                  guided_types=0):
+                  guided_types=0, max_guided_depth=0):
         """Attach a :class:`Guide` (None detaches); later launches sample and record with it."""
         self._guide = guide
         if guide is None:
             capi.check(capi.lib().pb2_pipeline_set_guide(self.h, None, None))
             return
         st = capi.GuideSettings(float(selection_prob), int(record_capacity), float(weight_quantile), int(spatial_cells),
-                                int(guided_types))
+                                int(guided_types), int(max_guided_depth))
         capi.check(capi.lib().pb2_pipeline_set_guide(self.h, guide.h, C.byref(st)))
 
     def train_guide(self, steps, batch=1 << 16, learning_rate=1e-2) -> float:

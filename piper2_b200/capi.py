@@ -110,7 +110,8 @@ class BatchConfig(C.Structure):
 
 class GuideSettings(C.Structure):
     _fields_ = [("selection_prob", C.c_float), ("record_capacity", C.c_uint32), ("weight_quantile", C.c_float),
-                ("spatial_cells", C.c_uint32), ("guided_types", C.c_uint32)]
+                ("spatial_cells", C.c_uint32), ("guided_types", C.c_uint32),
+                ("max_guided_depth", C.c_uint32)]
 
 
 SIGNATURES = [

@@ -88,6 +88,7 @@ constexpr int kNumSurfaceTypes = 7;
 // Counter slots in Paths::counts
 enum : int {
     C_EXT_CUR = 0, C_EXT_NEXT = 1, C_SHADOW = 2, C_MIS = 3, C_SHADED = 4, C_SURF0 = 5,  // 5..11 per type
+    C_GUIDE = 12,  // vertices whose continuation samples the guide (guided launches)
     C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24,
     C_CHECK = 25,  // 25..28: first failed index check (code, kernel, slot, value)
     C_FREE0 = 29,  // 29, 30: batched launches, slots freed (ping-pong with the extend queues)
@@ -124,6 +125,7 @@ struct Paths {
     uint32_t* shadow_q;
     uint32_t* mis_q;
     uint32_t* shaded_q;
+    uint32_t* guide_q;  // slots of the vertices the guide is evaluated for (guided launches)
     uint32_t* counts;  // C_COUNT entries
     // batched launches: scene of each slot, freed-slot queues
     uint32_t* scene;
@@ -176,7 +178,14 @@ struct GuideState {
     uint32_t salt;
     float bmin[3], binv[3];
     uint32_t types;         // bit t set: vertices of surface type t sample the guide
+    uint32_t max_depth;     // only vertices at path depth < max_depth sample the guide
 };
+
+// Whether a surface vertex of type `type` at path depth `depth` samples the guide (classification and
+// shading must agree: the guide is evaluated exactly for these vertices).
+__device__ __forceinline__ bool guide_vertex(const GuideState& gs, uint32_t type, uint32_t depth) {
+    return gs.enabled && ((gs.types >> type) & 1u) && depth < gs.max_depth;
+}
 
 // Where a kernel finds the launch parameters, scene and film of a path slot.
 // One scene per launch: everything is a kernel parameter.
@@ -580,6 +589,7 @@ __global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState
         const uint32_t type = sv.materials[sv.prim_material[prim]].type;
         PB2_CHECK(type < (uint32_t)kNumSurfaceTypes, 5, K_CLASSIFY, slot, type);
         ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
+        if (guide_vertex(gs, type, ps.depth[slot])) ps.guide_q[warp_push(&ps.counts[C_GUIDE])] = slot;
     }
 }
 
@@ -771,7 +781,7 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
             }
         }
         // continuation (PathTracing/Kernel.cpp:164-190); guided vertices sample 0.5 BxDF + 0.5 mixture
-        const bool guided = guided_type(kType) && gs.enabled && ((gs.types >> kType) & 1u) && bsdf.no_specular;
+        const bool guided = guided_type(kType) && guide_vertex(gs, kType, depth) && bsdf.no_specular;
         v3 wi_sh;
         spec fval;
         float pdf;
@@ -871,12 +881,8 @@ struct GuideRows {
     SceneView sv;
     Paths ps;
     GuideState gs;
-    uint32_t counts[kNumSurfaceTypes];
     __device__ __forceinline__ void features(uint32_t row, float (&f)[9], uint32_t& slot) const {
-        uint32_t idx = row;
-        int t = 0;
-        while (idx >= counts[t]) { idx -= counts[t]; ++t; }
-        slot = ps.surf[t][idx];
+        slot = ps.guide_q[row];
         const float4 h = ps.hit[slot];
         const float4 o4 = ps.o[slot], d4 = ps.d[slot];
         const v3 d = mk3(d4.x, d4.y, d4.z);
@@ -909,13 +915,8 @@ struct GuideRows {
 // The guide's mixture for every vertex of the guided material types, on the tcgen05 tensor cores.
 __global__ void __launch_bounds__(guide::kTcThreads) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    GuideRows rows{ sv, ps, gs, {} };
-    uint32_t total = 0;
-    for (int t = 0; t < kNumSurfaceTypes; ++t) {
-        rows.counts[t] = guided_type(t) && ((gs.types >> t) & 1u) ? ps.counts[C_SURF0 + t] : 0u;
-        total += rows.counts[t];
-    }
-    guide::forward_tc_tiles(gs.net, total, rows, ps.counts + C_TC_ERROR, smem);
+    GuideRows rows{ sv, ps, gs };
+    guide::forward_tc_tiles(gs.net, ps.counts[C_GUIDE], rows, ps.counts + C_TC_ERROR, smem);
 }
 
 // Per spatial cell (res^3 cells over the scene box) sum and count of the records' weights.
@@ -1125,6 +1126,7 @@ __global__ void k_advance(uint32_t* counts) {
     counts[C_SHADOW] = 0;
     counts[C_MIS] = 0;
     counts[C_SHADED] = 0;
+    counts[C_GUIDE] = 0;
     for (int t = 0; t < kNumSurfaceTypes; ++t) counts[C_SURF0 + t] = 0;
 }
 
@@ -1235,6 +1237,7 @@ static size_t carve_paths(char* base, size_t c, bool batch, Paths& s) {
     s.shadow_q = (uint32_t*)carve(c * 4);
     s.mis_q = (uint32_t*)carve(c * 4);
     s.shaded_q = (uint32_t*)carve(c * 4);
+    s.guide_q = (uint32_t*)carve(c * 4);
     s.counts = (uint32_t*)carve(sizeof(uint32_t) * C_COUNT);
     if (batch) {
         s.scene = (uint32_t*)carve(c * 4);
@@ -1520,6 +1523,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         gs.enabled = 1;
         gs.sel_prob = pl->guide_settings.selection_prob;
         gs.types = pl->guide_settings.guided_types;
+        gs.max_depth = pl->guide_settings.max_guided_depth ? pl->guide_settings.max_guided_depth : 0xFFFFFFFFu;
         gs.net = pl->guide->view();
         gs.mix = pl->g_mix;
         gs.rec = pl->g_rec;

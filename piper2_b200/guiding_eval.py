@@ -40,7 +40,8 @@ def rel_mse(img, ref):
 
 def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
-             weight_quantile=0.99, spatial_cells=0, truth=None, guided_types=0):
+             weight_quantile=0.99, spatial_cells=0, truth=None, guided_types=0,
+             max_guided_depth=0):
     import torch
 
     from . import api, scenes
@@ -63,7 +64,8 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
         # guided: fresh network, progressive passes with online training
         guide = api.Guide(seed=seed + 1)
         pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile,
-                     spatial_cells=spatial_cells, guided_types=guided_types)
+                     spatial_cells=spatial_cells, guided_types=guided_types,
+                     max_guided_depth=max_guided_depth)
         film = pl.new_film()
         t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
                                                                  learning_rate, train_passes))
@@ -74,7 +76,7 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train
     out.update({
         "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
-                   "guided_types": guided_types or "matte",
+                   "guided_types": guided_types or "matte", "max_guided_depth": max_guided_depth or None,
                    "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,
                    "train_passes": train_passes, "learning_rate": learning_rate, "weight_quantile": weight_quantile,
                    "spatial_cells": spatial_cells,

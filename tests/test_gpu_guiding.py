@@ -219,14 +219,17 @@ def _mean_and_se(pl):
     return rad.mean(axis=0), rad.std(axis=0) / np.sqrt(len(rad))
 
 
-def test_guided_render_is_unbiased():
+@pytest.mark.parametrize("max_guided_depth", [0, 2])
+def test_guided_render_is_unbiased(max_guided_depth):
+    """Guided sampling (every depth, or only the first two vertices of each path) keeps the plain
+    estimator's expectation."""
     api = _api()
     sd = scenes.cornell_box(seed=0, width=128, height=128, spp=16, max_depth=8)
     with api.Pipeline(sd) as pl:
         m0, s0 = _mean_and_se(pl)
     g = api.Guide(seed=2)
     with api.Pipeline(sd) as pl:
-        pl.set_guide(g, selection_prob=0.5, record_capacity=1 << 17)
+        pl.set_guide(g, selection_prob=0.5, record_capacity=1 << 17, max_guided_depth=max_guided_depth)
         # a few rounds of online training so the guide is far from uniform
         for it in range(4):
             film = pl.new_film()
@@ -250,5 +253,7 @@ def test_guide_settings_are_checked():
                 pl.set_guide(g, selection_prob=bad)
         with pytest.raises(capi.PB2Error):
             pl.set_guide(g, record_capacity=0)
+        with pytest.raises(capi.PB2Error):  # Plastic reports a pdf that is not its sampler's density
+            pl.set_guide(g, guided_types=1 << 2)
         with pytest.raises(capi.PB2Error):
             pl.train_guide(steps=1)
