@@ -38,10 +38,10 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=4, train_steps=4, batch=1 << 16,
+def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
              weight_quantile=0.99, spatial_cells=0, truth=None, guided_types=0,
-             max_guided_depth=0):
+             max_guided_depth=2):
     import torch
 
     from . import api, scenes
@@ -100,7 +100,7 @@ def main():
     ap.add_argument("--height", type=int, default=720)
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--ref-spp", type=int, default=1024)
-    ap.add_argument("--spp-per-pass", type=int, default=4)
+    ap.add_argument("--spp-per-pass", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=4)
     ap.add_argument("--train-passes", type=int, default=None)
     ap.add_argument("--batch", type=int, default=1 << 16)
@@ -109,10 +109,12 @@ def main():
     ap.add_argument("--weight-quantile", type=float, default=0.99)
     ap.add_argument("--spatial-cells", type=int, default=0)
     ap.add_argument("--tess", type=int, default=15)
+    ap.add_argument("--max-guided-depth", type=int, default=2)
     a = ap.parse_args()
     print(json.dumps(evaluate(a.width, a.height, a.spp, a.ref_spp, a.spp_per_pass, a.train_steps, a.batch, a.lr,
                               a.selection_prob, tess=a.tess, train_passes=a.train_passes,
-                              weight_quantile=a.weight_quantile, spatial_cells=a.spatial_cells)))
+                              weight_quantile=a.weight_quantile, spatial_cells=a.spatial_cells,
+                              max_guided_depth=a.max_guided_depth)))
 
 
 if __name__ == "__main__":
