@@ -1164,6 +1164,7 @@ struct pb2_pipeline {
     float* plane_pdf = nullptr;
     uint32_t num_lights = 0;
     uint32_t material_count = 0;
+    uint32_t type_mask = 0;  // surface types of the scene's materials: the shading kernels launched per bounce
     float env[3] = { 0, 0, 0 };
     float gauss_sub = 0.0f;
     // path state
@@ -1411,6 +1412,8 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
     }
     pl->num_lights = scene->area_light_count;
     pl->material_count = scene->material_count;
+    for (uint32_t m = 0; m < scene->material_count; ++m) pl->type_mask |= 1u << scene->materials[m].type;
+    if (scene->material_count == 0) pl->type_mask = (1u << kNumSurfaceTypes) - 1u;
     for (int k = 0; k < 3; ++k) pl->env[k] = scene->env_radiance[k];
     cudaError_t e;
     if ((e = cudaMalloc(&pl->materials, sizeof(DevMaterial) * mats.size())) ||
@@ -1618,20 +1621,36 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         checked("k_classify");
         if (gs.enabled) k_guide_infer<<<pl->sms * 2, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
         checked("k_guide_infer");
-        k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<matte>");
-        k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<plastic>");
-        k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<glass>");
-        k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<mirror>");
-        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<substrate>");
-        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<conductor>");
-        k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_shade<blackbody>");
+        // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
+        const uint32_t tm = pl->type_mask;
+        if (tm & (1u << PB2_SURFACE_MATTE)) {
+            k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<matte>");
+        }
+        if (tm & (1u << PB2_SURFACE_PLASTIC)) {
+            k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<plastic>");
+        }
+        if (tm & (1u << PB2_SURFACE_GLASS)) {
+            k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<glass>");
+        }
+        if (tm & (1u << PB2_SURFACE_MIRROR)) {
+            k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<mirror>");
+        }
+        if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
+            k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<substrate>");
+        }
+        if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
+            k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<conductor>");
+        }
+        if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
+            k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<blackbody>");
+        }
         k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
                                                                    sstats);
         checked("k_trace_queue<shadow>");
