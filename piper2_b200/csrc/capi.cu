@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI (include/piper2_b200.h): error handling, host-side component helpers, the
 // acceleration structure and the batch trace calls.  The render pipeline lives in render.cu.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -250,6 +251,10 @@ int pb2_accel_destroy(pb2_accel* acc) {
     cudaFree(acc->counters);
     cudaFree(acc->error_flag);
     cudaFree(acc->stage);
+    for (cudaStream_t& st : acc->chunk_streams)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t& ev : acc->chunk_events)
+        if (ev) cudaEventDestroy(ev);
     delete acc;
     return PB2_OK;
 }
@@ -400,20 +405,64 @@ static int ensure_stage(pb2_accel* acc, size_t bytes) {
     return PB2_OK;
 }
 
+static int ensure_chunk_streams(pb2_accel* acc) {
+    for (cudaStream_t& st : acc->chunk_streams)
+        if (!st) PB2_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "create chunk stream");
+    for (cudaEvent_t& ev : acc->chunk_events)
+        if (!ev) PB2_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "create chunk event");
+    return PB2_OK;
+}
+
+// Host-array trace: the batch is split into chunks of kHostChunk rays, dealt round-robin to three streams;
+// each chunk's upload, traversal and download are ordered on its stream, so one chunk's copies run on
+// the copy engines while another chunk traverses.  Each stream has its own work counter (accel->work
+// slots 4..6; slots 0..2 belong to the render pipeline).  The caller's stream orders the whole call.
+static constexpr uint32_t kHostChunk = 1u << 19;
+
 static int trace_host(const pb2_accel* cacc, const pb2_ray* rays, uint32_t n, void* out, bool closest,
                       cudaStream_t stream) {
     auto* acc = const_cast<pb2_accel*>(cacc);
+    const size_t osz = closest ? sizeof(pb2_hit) : sizeof(uint32_t);
     const size_t rb = sizeof(pb2_ray) * (size_t)n;
-    const size_t ob = (closest ? sizeof(pb2_hit) : sizeof(uint32_t)) * (size_t)n;
+    const size_t ob = osz * (size_t)n;
     int rc = ensure_stage(acc, rb + ob + 256);
     if (rc) return rc;
     auto* d_rays = static_cast<pb2_ray*>(acc->stage);
-    void* d_out = static_cast<char*>(acc->stage) + ((rb + 255) / 256) * 256;
-    PB2_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, stream), "upload rays");
-    rc = trace_dev(acc, d_rays, n, closest ? static_cast<pb2_hit*>(d_out) : nullptr,
-                   closest ? nullptr : static_cast<uint32_t*>(d_out), closest, stream);
-    if (rc) return rc;
-    PB2_CUDA(cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, stream), "download results");
+    char* d_out = static_cast<char*>(acc->stage) + ((rb + 255) / 256) * 256;
+    if (n <= kHostChunk) {
+        PB2_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, stream), "upload rays");
+        rc = trace_dev(acc, d_rays, n, closest ? reinterpret_cast<pb2_hit*>(d_out) : nullptr,
+                       closest ? nullptr : reinterpret_cast<uint32_t*>(d_out), closest, stream);
+        if (rc) return rc;
+        PB2_CUDA(cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, stream), "download results");
+        PB2_CUDA(cudaStreamSynchronize(stream), "trace sync");
+        return PB2_OK;
+    }
+    if ((rc = ensure_chunk_streams(acc))) return rc;
+    if (acc->counting) PB2_CUDA(cudaMemsetAsync(acc->counters, 0, sizeof(unsigned long long) * 2, stream), "memset");
+    PB2_CUDA(cudaEventRecord(acc->chunk_events[0], stream), "record start");
+    for (cudaStream_t st : acc->chunk_streams) PB2_CUDA(cudaStreamWaitEvent(st, acc->chunk_events[0], 0), "wait start");
+    const uint32_t chunks = (n + kHostChunk - 1) / kHostChunk;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const int k = (int)(c % 3);
+        cudaStream_t st = acc->chunk_streams[k];
+        const size_t lo = (size_t)c * kHostChunk;
+        const uint32_t m = (uint32_t)std::min<size_t>(kHostChunk, n - lo);
+        PB2_CUDA(cudaMemcpyAsync(d_rays + lo, rays + lo, sizeof(pb2_ray) * m, cudaMemcpyHostToDevice, st),
+                 "upload rays");
+        PB2_CUDA(launch_trace_api(acc->view, d_rays + lo, m,
+                                  closest ? reinterpret_cast<pb2_hit*>(d_out) + lo : nullptr,
+                                  closest ? nullptr : reinterpret_cast<uint32_t*>(d_out) + lo, closest, acc->counting,
+                                  acc->work + 4 + k, acc->counters, acc->error_flag, st),
+                 closest ? "trace_closest launch" : "trace_any launch");
+        PB2_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + lo * osz, d_out + lo * osz, osz * m, cudaMemcpyDeviceToHost,
+                                 st),
+                 "download results");
+    }
+    for (int k = 0; k < 3; ++k) {
+        PB2_CUDA(cudaEventRecord(acc->chunk_events[1 + k], acc->chunk_streams[k]), "record chunk");
+        PB2_CUDA(cudaStreamWaitEvent(stream, acc->chunk_events[1 + k], 0), "join chunk");
+    }
     PB2_CUDA(cudaStreamSynchronize(stream), "trace sync");
     return PB2_OK;
 }

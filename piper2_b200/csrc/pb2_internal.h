@@ -51,6 +51,10 @@ struct pb2_accel {
     // staging buffers of the *_host trace calls
     void* stage = nullptr;
     size_t stage_bytes = 0;
+    // streams and events of the pipelined *_host trace calls (upload, trace and download of successive
+    // chunks overlap); created on first use
+    cudaStream_t chunk_streams[3] = { nullptr, nullptr, nullptr };
+    cudaEvent_t chunk_events[4] = { nullptr, nullptr, nullptr, nullptr };
 };
 
 struct pb2_guide {

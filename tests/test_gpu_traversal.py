@@ -72,6 +72,35 @@ def test_full_size_stress_properties():
         assert acc.trace_any(cut).all()
 
 
+def test_host_calls_chunked_equal_device_calls():
+    """The host-array calls pipeline batches above 2^19 rays in chunks over three streams; a 1.3M-ray batch
+    (three chunks, the last one partial) gives the same hits and flags as the device-pointer calls, and the
+    same traversal counters."""
+    import torch
+
+    soup = scenes.triangle_soup(1 << 18, seed=4)
+    n = (1 << 20) + 300_001
+    rays = scenes.soup_rays(n, seed=5, kind="closest")
+    srays = scenes.soup_rays(n, seed=6, kind="any")
+    with _api().Accel(soup) as acc:
+        acc.set_counting(True)
+        h_host = acc.trace_closest(rays)
+        c_host = acc.counters()
+        o_host = acc.trace_any(srays)
+        d_rays = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda()
+        d_hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        acc.trace_closest_dev(d_rays.data_ptr(), n, d_hits.data_ptr())
+        c_dev = acc.counters()
+        d_srays = torch.from_numpy(srays.view(np.float32).reshape(-1, 8)).cuda()
+        d_occ = torch.empty(n, dtype=torch.int32, device="cuda")
+        acc.trace_any_dev(d_srays.data_ptr(), n, d_occ.data_ptr())
+        torch.cuda.synchronize()
+    h_dev = d_hits.cpu().numpy().view(capi.HIT_DTYPE).reshape(-1)
+    assert np.array_equal(h_host.view(np.uint32), h_dev.view(np.uint32))
+    assert np.array_equal(o_host, d_occ.cpu().numpy().view(np.uint32))
+    assert c_host == c_dev and c_host[0] > n
+
+
 def test_edge_cases(oracle):
     # shared edges and vertices (watertightness), degenerate triangles, rays along axes, empty batch
     v = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0.5, 0.5, 0], [2, 2, 2], [2, 2, 2], [3, 3, 3]],
