@@ -417,7 +417,10 @@ static int ensure_chunk_streams(pb2_accel* acc) {
 // each chunk's upload, traversal and download are ordered on its stream, so one chunk's copies run on
 // the copy engines while another chunk traverses.  Each stream has its own work counter (accel->work
 // slots 4..6; slots 0..2 belong to the render pipeline).  The caller's stream orders the whole call.
-static constexpr uint32_t kHostChunk = 1u << 19;
+#ifndef PB2_HOST_CHUNK_LOG2
+#define PB2_HOST_CHUNK_LOG2 19
+#endif
+static constexpr uint32_t kHostChunk = 1u << PB2_HOST_CHUNK_LOG2;
 
 static int trace_host(const pb2_accel* cacc, const pb2_ray* rays, uint32_t n, void* out, bool closest,
                       cudaStream_t stream) {
