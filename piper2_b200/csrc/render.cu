@@ -1847,6 +1847,7 @@ struct pb2_batch {
     pb2_batch_config config{};
     int sms = 0;
     int trace_blocks_max = 0;
+    uint32_t type_mask = 0;  // surface types of all scenes' materials
     // the batch's own non-blocking stream: graphs cannot be captured on the legacy default stream
     cudaStream_t own = nullptr;
     // captured graph of two wavefront iterations (cur = 0 then 1) for `graph_config`
@@ -1891,13 +1892,18 @@ static cudaError_t batch_iteration(pb2_batch* b, uint32_t cur, cudaStream_t stre
     k_batch_regen<<<grid, 256, 0, stream>>>(ctx, ps, cur);
     k_trace_queue<Q_EXTEND><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, b->work, stats);
     k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_MATTE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_PLASTIC><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_GLASS><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_MIRROR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_SUBSTRATE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_CONDUCTOR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
-    k_shade<PB2_SURFACE_BLACKBODY><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    // shading kernels of the surface types some scene of the batch uses
+    const uint32_t tm = b->type_mask;
+    if (tm & (1u << PB2_SURFACE_MATTE)) k_shade<PB2_SURFACE_MATTE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_PLASTIC)) k_shade<PB2_SURFACE_PLASTIC><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_GLASS)) k_shade<PB2_SURFACE_GLASS><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_MIRROR)) k_shade<PB2_SURFACE_MIRROR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_SUBSTRATE))
+        k_shade<PB2_SURFACE_SUBSTRATE><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_CONDUCTOR))
+        k_shade<PB2_SURFACE_CONDUCTOR><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
+    if (tm & (1u << PB2_SURFACE_BLACKBODY))
+        k_shade<PB2_SURFACE_BLACKBODY><<<grid, sb, 0, stream>>>(ctx, ps, gs, cur);
     k_trace_queue<Q_SHADOW><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, b->work + 1, sstats);
     k_trace_queue<Q_MIS><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, b->work + 2, stats);
     k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
@@ -2045,6 +2051,7 @@ int pb2_batch_create(const pb2_scene* scenes, const pb2_render_settings* setting
         const int rc = pb2_pipeline_create(&scenes[i], &settings[i], stream_ptr, &pl);
         if (rc) return cleanup(rc);
         b->pipes.push_back(pl);
+        b->type_mask |= pl->type_mask;
     }
     size_t film = 0;
     unsigned long long path = 0;

@@ -70,3 +70,34 @@ def test_scene_generators_deterministic():
     assert s.triangle_count == 1000
     r = scenes.soup_rays(100, seed=1)
     assert np.allclose(np.linalg.norm(r["dir"], axis=1), 1, atol=1e-6)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every struct the Python binding mirrors has the header's size and field offsets (a C probe compiled
+    with gcc against include/piper2_b200.h prints them)."""
+    import subprocess
+
+    pairs = {"Ray": "pb2_ray", "Hit": "pb2_hit", "Mesh": "pb2_mesh", "Plane": "pb2_plane",
+             "AreaLight": "pb2_area_light", "Material": "pb2_material", "Camera": "pb2_camera", "Scene": "pb2_scene",
+             "RenderSettings": "pb2_render_settings", "Rect": "pb2_rect", "NDCTransform": "pb2_ndc_transform",
+             "AccelInfo": "pb2_accel_info", "LaunchStats": "pb2_launch_stats", "BatchConfig": "pb2_batch_config",
+             "GuideSettings": "pb2_guide_settings"}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "piper2_b200.h"', "int main(void) {"]
+    for py, c in pairs.items():
+        cls = getattr(capi, py)
+        lines.append(f'    printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in cls._fields_:
+            lines.append(f'    printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines.append("    return 0;\n}")
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for py in pairs:
+        cls = getattr(capi, py)
+        assert got[(py, "size")] == C.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert got[(py, name)] == getattr(cls, name).offset, (py, name)
