@@ -36,9 +36,41 @@ __device__ __forceinline__ uint32_t sobol_bits(uint64_t index, uint32_t dim) {
 __device__ __forceinline__ float sobol_sample(uint64_t index, uint32_t dim) {
     return (float)sobol_bits(index, dim) * 0x1p-32f;
 }
+
+// Byte tables of the generator matrices for the render kernels: entry [d][k][b] is the XOR of the columns
+// 8k + j of dimension d over the set bits j of b (the same column index d * 52 + 8k + j that the bitwise
+// loop above reads), so a sample is the XOR of one entry per byte of its index instead of one column per
+// set bit.  XOR is associative, so the value is the same bit for bit.  Filled by k_sobol_byte_tables when
+// a pipeline is created (every GPU that loads the library holds the 7 MiB until exit).
+constexpr uint32_t kSobolIndexBytes = 7;  // indices below 2^56 (a render's indices stay below 2^53)
+static __device__ uint32_t g_sobol_bytes[PB2_SOBOL_DIMS * kSobolIndexBytes * 256];
+
+__global__ void k_sobol_byte_tables() {
+    constexpr uint32_t kColumns = PB2_SOBOL_DIMS * PB2_SOBOL_MATRIX_SIZE;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < PB2_SOBOL_DIMS * kSobolIndexBytes * 256;
+         e += gridDim.x * blockDim.x) {
+        const uint32_t b = e & 255u, k = (e >> 8) % kSobolIndexBytes, d = (e >> 8) / kSobolIndexBytes;
+        uint32_t v = 0;
+        for (uint32_t j = 0; j < 8; ++j) {
+            const uint32_t col = d * PB2_SOBOL_MATRIX_SIZE + 8 * k + j;
+            if (((b >> j) & 1u) && col < kColumns) v ^= pb2_sobol_matrices32[col];
+        }
+        g_sobol_bytes[e] = v;
+    }
+}
+
+__device__ __forceinline__ uint32_t sobol_bits_bytes(uint64_t index, uint32_t dim) {
+    const uint32_t* t = g_sobol_bytes + (size_t)dim * (kSobolIndexBytes * 256);
+    uint32_t v = 0;
+    for (uint32_t k = 0; index && k < kSobolIndexBytes; ++k, index >>= 8, t += 256) v ^= __ldg(t + (index & 0xFFu));
+    return v;
+}
+__device__ __forceinline__ float sobol_sample_fast(uint64_t index, uint32_t dim) {
+    return (float)sobol_bits_bytes(index, dim) * 0x1p-32f;
+}
 // A dimension >= 2 of a launch, Owen-scrambled when the settings ask for it (extension; see pb2_math.h).
 __device__ __forceinline__ float sobol_sample_s(uint64_t index, uint32_t dim, uint32_t scramble, uint32_t seed) {
-    uint32_t v = sobol_bits(index, dim);
+    uint32_t v = sobol_bits_bytes(index, dim);
     if (scramble) v = pb2_owen_scramble(v, pb2_owen_dim_seed(seed, dim));
     return (float)v * 0x1p-32f;
 }
@@ -314,8 +346,8 @@ __device__ __forceinline__ void primary_ray(const LaunchParams& lp, uint32_t sx,
                                             uint64_t& index, float& px, float& py, v3& org, v3& dir) {
     const float res = (float)(1u << lp.log2res);
     index = sobol_interval_to_index(lp.log2res, s, sx, sy);
-    const float offx = fminf(fmaxf(sobol_sample(index, 0) * res - (float)sx, 0.0f), 1.0f);
-    const float offy = fminf(fmaxf(sobol_sample(index, 1) * res - (float)sy, 0.0f), 1.0f);
+    const float offx = fminf(fmaxf(sobol_sample_fast(index, 0) * res - (float)sx, 0.0f), 1.0f);
+    const float offy = fminf(fmaxf(sobol_sample_fast(index, 1) * res - (float)sy, 0.0f), 1.0f);
     px = offx + (float)(lp.full.left + sx);
     py = offy + (float)(lp.full.top + sy);
     const float ndc_x = lp.ndc.ox + lp.ndc.sx * px / (float)lp.width;
@@ -1423,10 +1455,16 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
         (e = cudaMemcpyAsync(pl->materials, mats.data(), sizeof(DevMaterial) * mats.size(), cudaMemcpyHostToDevice, stream)) ||
         (e = cudaMemcpyAsync(pl->lights, lights.data(), sizeof(DevLight) * lights.size(), cudaMemcpyHostToDevice, stream)) ||
         (e = cudaMemcpyAsync(pl->plane_cdf, cdf.data(), sizeof(float) * cdf.size(), cudaMemcpyHostToDevice, stream)) ||
-        (e = cudaMemcpyAsync(pl->plane_pdf, pdf.data(), sizeof(float) * pdf.size(), cudaMemcpyHostToDevice, stream)) ||
-        (e = cudaStreamSynchronize(stream))) {
+        (e = cudaMemcpyAsync(pl->plane_pdf, pdf.data(), sizeof(float) * pdf.size(), cudaMemcpyHostToDevice, stream))) {
         pb2_pipeline_destroy(pl);
         return cuda_fail(e, "pipeline upload");
+    }
+    // the Sobol byte tables of this device (same values on every fill, so a fill may overlap other
+    // pipelines' renders)
+    k_sobol_byte_tables<<<256, 256, 0, stream>>>();
+    if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(stream))) {
+        pb2_pipeline_destroy(pl);
+        return cuda_fail(e, "pipeline set-up");
     }
     int dev = 0;
     cudaGetDevice(&dev);
