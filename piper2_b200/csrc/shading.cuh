@@ -430,13 +430,16 @@ __device__ __forceinline__ void lobe_sample(const Lobe& L, float u1, float u2, v
 
 // Surface init of the Classic module (Classic/Kernel.cpp: matte :249-268, plastic :441-470,
 // glass :613-656, mirror :668-677, substrate :755-778, black body :45-48).
+// kType >= 0 is the material's surface type known at compile time (the per-type shading kernels): the
+// lobe count then folds to a constant and the lobes stay in registers.
+template <int kType = -1>
 __device__ __forceinline__ void bsdf_init(const DevMaterial& m, bool front, Bsdf& b) {
     b.n = 0;
     b.mirror = false;
     b.no_specular = false;
     const spec c0 = mksp(m.c0[0], m.c0[1], m.c0[2]);
     const spec c1 = mksp(m.c1[0], m.c1[1], m.c1[2]);
-    switch (m.type) {
+    switch (kType >= 0 ? (uint32_t)kType : m.type) {
         case PB2_SURFACE_MATTE: {
             Lobe& L = b.l[b.n++];
             L.part = kPartDiffuse | kPartR;
@@ -521,7 +524,9 @@ __device__ __forceinline__ void bsdf_init(const DevMaterial& m, bool front, Bsdf
 
 __device__ __forceinline__ uint32_t bsdf_count(const Bsdf& b, int require) {
     uint32_t c = 0;
-    for (int i = 0; i < b.n; ++i) c += part_match(b.l[i].part, require) ? 1u : 0u;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (i < b.n) c += part_match(b.l[i].part, require) ? 1u : 0u;
     return c;
 }
 
@@ -545,21 +550,25 @@ __device__ __forceinline__ void bsdf_sample(const Bsdf& b, float u1, float u2, v
     if (sel > count - 1) sel = count - 1;
     u1 = u1 * (float)count - (float)sel;
     int chosen = -1;
-    for (int i = 0, k = 0; i < b.n; ++i) {
-        if (!part_match(b.l[i].part, require)) continue;
-        if ((uint32_t)k == sel) { chosen = i; break; }
+#pragma unroll
+    for (int i = 0, k = 0; i < 3; ++i) {
+        if (i >= b.n || chosen >= 0 || !part_match(b.l[i].part, require)) continue;
+        if ((uint32_t)k == sel) chosen = i;
         ++k;
     }
-    lobe_sample(b.l[chosen], u1, u2, wo, out);
+    // the chosen lobe by register selects (a dynamic index would put the lobes in local memory)
+    lobe_sample(chosen == 0 ? b.l[0] : (chosen == 1 ? b.l[1] : b.l[2]), u1, u2, wo, out);
     if (out.pdf <= 0.0f) return;
     if (!(out.part & kPartSpecular)) {
         const int addition = (dot3(wo, ng) * dot3(out.wi, ng)) > 0.0f ? kPartR : kPartT;
-        for (int i = 0; i < b.n; ++i) {
-            if (i == chosen || !part_match(b.l[i].part, require)) continue;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (i >= b.n || i == chosen || !part_match(b.l[i].part, require)) continue;
             if (addition & b.l[i].part) out.f = sp_add(out.f, lobe_eval(b.l[i], wo, out.wi));
         }
-        for (int i = 0; i < b.n; ++i) {
-            if (i == chosen || !part_match(b.l[i].part, require)) continue;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (i >= b.n || i == chosen || !part_match(b.l[i].part, require)) continue;
             out.pdf = out.pdf + lobe_pdf(b.l[i], wo, out.wi);
         }
     }
@@ -570,8 +579,10 @@ __device__ __forceinline__ spec bsdf_eval(const Bsdf& b, v3 wo, v3 wi, v3 ng, in
     if (b.mirror) return sp_zero();
     const int addition = (dot3(wo, ng) * dot3(wi, ng)) > 0.0f ? kPartR : kPartT;
     spec f = sp_zero();
-    for (int i = 0; i < b.n; ++i)
-        if (part_match(b.l[i].part, require) && (addition & b.l[i].part)) f = sp_add(f, lobe_eval(b.l[i], wo, wi));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (i < b.n && part_match(b.l[i].part, require) && (addition & b.l[i].part))
+            f = sp_add(f, lobe_eval(b.l[i], wo, wi));
     return f;
 }
 
@@ -580,8 +591,9 @@ __device__ __forceinline__ float bsdf_pdf(const Bsdf& b, v3 wo, v3 wi, int requi
     const uint32_t count = bsdf_count(b, require);
     if (count == 0) return 0.0f;
     float pdf = 0.0f;
-    for (int i = 0; i < b.n; ++i)
-        if (part_match(b.l[i].part, require)) pdf = pdf + lobe_pdf(b.l[i], wo, wi);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (i < b.n && part_match(b.l[i].part, require)) pdf = pdf + lobe_pdf(b.l[i], wo, wi);
     if (count > 1) pdf = pdf / (float)count;
     return pdf;
 }
