@@ -720,13 +720,10 @@ __device__ __forceinline__ v3 to_local(const Frame& f, v3 v) {
 // a pdf that is not their sampler's density (Classic/Kernel.cpp:405-412), so they keep plain BxDF sampling.
 __host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_MATTE || t == PB2_SURFACE_CONDUCTOR; }
 
-// Resident 128-thread blocks per SM the shading kernels' register budget is sized for.
-#ifndef PB2_SHADE_MIN_BLOCKS
-#define PB2_SHADE_MIN_BLOCKS 4
-#endif
+// (No launch bounds: batched renders launch it with the autotuned block size, up to 512 threads.  A
+// sweep of register budgets for 4-8 resident 128-thread blocks changed render times by under 2 %.)
 template <int kType, class Ctx>
-__global__ void __launch_bounds__(128, PB2_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ Ctx ctx, Paths ps,
-                                                                     GuideState gs, uint32_t cur) {
+__global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
