@@ -462,7 +462,7 @@ def render_bench(args):
     torch.cuda.empty_cache()
     result["batch"] = batch_bench()
     torch.cuda.empty_cache()
-    g = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0,
+    g = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0, repeats=3,
                               truth=lambda img: truth_rel_mse(img, "guiding_room_1280x720"))
     result["guiding"] = g
     result["guiding_mlp"] = mlp_bench()

@@ -41,7 +41,7 @@ def rel_mse(img, ref):
 def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train_steps=4, batch=1 << 16,
              learning_rate=1e-2, selection_prob=0.5, seed=0, tess=15, max_depth=16, chunk=64, train_passes=None,
              weight_quantile=0.99, spatial_cells=0, truth=None, guided_types=0,
-             max_guided_depth=2):
+             max_guided_depth=2, repeats=1):
     import torch
 
     from . import api, scenes
@@ -61,18 +61,24 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train
         film = pl.new_film()
         t_plain, _ = _time(torch, lambda: pl.launch(film, sample_begin=0, sample_count=spp))
         plain = pl.resolve(film).cpu().numpy().astype(np.float64)
-        # guided: fresh network, progressive passes with online training
-        guide = api.Guide(seed=seed + 1)
-        pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20, weight_quantile=weight_quantile,
-                     spatial_cells=spatial_cells, guided_types=guided_types,
-                     max_guided_depth=max_guided_depth)
-        film = pl.new_film()
-        t_guided, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
-                                                                 learning_rate, train_passes))
-        guided = pl.resolve(film).cpu().numpy().astype(np.float64)
-        pl.set_guide(None)
+        # guided: a fresh network per run, progressive passes with online training.  Online training is not
+        # deterministic (records are gathered with atomics), so `repeats` independent runs are made and
+        # their errors and times averaged.
+        runs = []
+        for r in range(max(1, repeats)):
+            guide = api.Guide(seed=seed + 1 + r)
+            pl.set_guide(guide, selection_prob=selection_prob, record_capacity=1 << 20,
+                         weight_quantile=weight_quantile, spatial_cells=spatial_cells, guided_types=guided_types,
+                         max_guided_depth=max_guided_depth)
+            film = pl.new_film()
+            t_g, losses = _time(torch, lambda: pl.render_guided(film, spp, spp_per_pass, train_steps, batch,
+                                                                learning_rate, train_passes))
+            runs.append((t_g, pl.resolve(film).cpu().numpy().astype(np.float64), losses))
+            pl.set_guide(None)
+    t_guided = float(np.mean([r[0] for r in runs]))
+    guided, losses = runs[-1][1], runs[-1][2]
     e_plain = rel_mse(plain, ref) if ref is not None else None
-    e_guided = rel_mse(guided, ref) if ref is not None else None
+    e_guided = float(np.mean([rel_mse(r[1], ref) for r in runs])) if ref is not None else None
     out.update({
         "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
@@ -85,10 +91,14 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train
         "relmse_ratio": e_plain / e_guided if e_guided else None,
         "speedup": (t_plain * e_plain) / (t_guided * e_guided) if e_guided else None,
     })
+    out["guided"]["runs"] = len(runs)
+    out["guided"]["ms_each"] = [round(r[0], 2) for r in runs]
     if truth is not None:
-        f_plain, f_guided = truth(plain), truth(guided)
+        each = [truth(r[1]) for r in runs]
+        f_plain, f_guided = truth(plain), float(np.mean(each))
         out["plain"]["relmse_fp64"] = f_plain
         out["guided"]["relmse_fp64"] = f_guided
+        out["guided"]["relmse_fp64_each"] = each
         out["relmse_ratio_fp64"] = f_plain / f_guided if f_guided > 0 else None
         out["speedup_fp64"] = (t_plain * f_plain) / (t_guided * f_guided) if f_guided > 0 else None
     return out
