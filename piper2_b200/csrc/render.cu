@@ -400,18 +400,29 @@ constexpr int kQSteps = 4;
 
 enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
 
+// The MIS ray of a vertex only matters if its closest hit is a plane of the selected light, or nothing
+// (the environment).  So it is answered with the planes first (all lights' parallelograms, tested in
+// order, as the closest-hit query's plane pass does) and an occlusion query over the triangles:
+//   nearest plane belongs to the selected light at t_L -> any hit on (tmin, next float after t_L): a
+//     triangle at t <= t_L wins the closest-hit query (planes lose ties), otherwise the plane is the hit;
+//   nearest plane belongs to another light -> that plane or a triangle is hit: neither counts, no query;
+//   no plane -> any hit on (tmin, tmax): occluded means a triangle is hit, free means a miss.
+// The record (t, prim) written is what k_finish needs: the plane and its t, PB2_INVALID_PRIM for a miss,
+// or the occluding triangle.  k_finish's result is that of the closest-hit query.
 template <int kKind, class Ctx>
 __global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(const __grid_constant__ Ctx ctx, Paths ps,
                                                            const uint32_t* __restrict__ queue,
                                                            const uint32_t* __restrict__ count_ptr, uint32_t* work,
                                                            unsigned long long* stat) {
-    constexpr bool kClosest = kKind != Q_SHADOW;
+    constexpr bool kClosest = kKind == Q_EXTEND;
     const uint32_t n = *count_ptr;
     __shared__ uint2 stack_smem[kSharedStack * kQThreads];
     Traverser<kClosest, false, kQThreads> tr;
     tr.bind_stack(stack_smem);
     bool active = false;
     uint32_t slot = 0;
+    float mis_t = 0.0f;      // Q_MIS: nearest plane's t and index (kInvalidPrim: none)
+    uint32_t mis_plane = 0;
     BvhView bvh{};
     if constexpr (!Ctx::kBatch) bvh = ctx.bvh(0);
     const unsigned lane = threadIdx.x & 31u;
@@ -442,6 +453,25 @@ __global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(const __grid_cons
                     tr.init(bvh, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w);
                     active = true;
                     ++rays;
+                    if (kKind == Q_MIS) {
+                        mis_t = tr.p.tmax;
+                        mis_plane = kInvalidPrim;
+                        for (uint32_t i = 0; i < bvh.plane_count; ++i) {
+                            float t, u, v;
+                            bool front;
+                            if (plane_test(bvh.planes[i], tr.p, tr.p.tmin, mis_t, t, u, v, front)) {
+                                mis_t = t;
+                                mis_plane = i;
+                            }
+                        }
+                        const uint32_t sel = __float_as_uint(ps.mr_pdf[slot].y);
+                        if (mis_plane != kInvalidPrim && !(sel != 0u && bvh.planes[mis_plane].light == sel - 1u)) {
+                            tr.done = true;  // another light's plane: the ray completes at once with that plane
+                        } else if (mis_plane != kInvalidPrim) {
+                            tr.p.tmax = __uint_as_float(__float_as_uint(mis_t) + 1u);  // the next float after t_L
+                            tr.tbest = tr.p.tmax;
+                        }
+                    }
                 }
             }
             if (__ballot_sync(0xFFFFFFFFu, active) == 0u) break;
@@ -453,13 +483,15 @@ __global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(const __grid_cons
                 if (kClosest) {
                     bool front;
                     tr.finish_planes(bvh, front);
-                    const float4 h = make_float4(tr.tbest, __uint_as_float(tr.best_prim), tr.bu, tr.bv);
-                    if (kKind == Q_EXTEND) {
-                        ps.hit[slot] = h;
-                        ps.hit_slot[slot] = tr.best_slot;
-                    } else {
-                        ps.mhit[slot] = h;
-                    }
+                    ps.hit[slot] = make_float4(tr.tbest, __uint_as_float(tr.best_prim), tr.bu, tr.bv);
+                    ps.hit_slot[slot] = tr.best_slot;
+                } else if (kKind == Q_MIS) {
+                    // the occluding triangle's id, or the nearest plane (kInvalidPrim: none); no marker
+                    // values: every prim written is a real triangle, a plane, or PB2_INVALID_PRIM
+                    const uint32_t prim = tr.best_prim != kInvalidPrim ? tr.best_prim
+                                          : (mis_plane == kInvalidPrim ? kInvalidPrim : (kPlaneFlag | mis_plane));
+                    ps.mhit[slot] = make_float4(tr.best_prim != kInvalidPrim ? tr.tbest : mis_t, __uint_as_float(prim),
+                                                0.0f, 0.0f);
                 } else {
                     ps.occ[slot] = tr.best_prim != kInvalidPrim ? 1u : 0u;
                 }
