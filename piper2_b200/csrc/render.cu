@@ -610,11 +610,26 @@ __global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState
         PB2_CHECK(prim == kInvalidPrim || ((prim & kPlaneFlag) ? (prim & ~kPlaneFlag) < sv.bvh.plane_count
                                                                 : prim < sv.bvh.tri_count),
                   3, K_CLASSIFY, slot, prim);
+        const bool missing = prim == kInvalidPrim;
+        const bool area = !missing && (prim & kPlaneFlag);
+        if (!missing && !area) {
+            // a surface hit (most paths): only its material and the path depth are read here
+            if (ps.depth[slot] >= lp.max_depth) {
+                if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
+                terminate_path(ctx, ps, slot, cur);
+                continue;
+            }
+            PB2_CHECK(sv.prim_material[prim] < sv.material_count, 4, K_CLASSIFY, slot, sv.prim_material[prim]);
+            const uint32_t type = sv.materials[sv.prim_material[prim]].type;
+            PB2_CHECK(type < (uint32_t)kNumSurfaceTypes, 5, K_CLASSIFY, slot, type);
+            ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
+            if (guide_vertex(gs, type, ps.depth[slot])) ps.guide_q[warp_push(&ps.counts[C_GUIDE])] = slot;
+            continue;
+        }
+        // a miss or an area light: emission on specular paths, pass-through, termination
         const float4 o4 = ps.o[slot], d4 = ps.d[slot];
         const float4 pf4 = ps.pf[slot];
         const bool specular = pf4.w != 0.0f;
-        const bool missing = prim == kInvalidPrim;
-        const bool area = !missing && (prim & kPlaneFlag);
         spec sample = mksp(ps.rad[slot].x, ps.rad[slot].y, ps.rad[slot].z);
         const spec pf = mksp(pf4.x, pf4.y, pf4.z);
         const v3 d = mk3(d4.x, d4.y, d4.z);
@@ -644,16 +659,8 @@ __global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState
             ps.ext[cur ^ 1][warp_push(&ps.counts[C_EXT_NEXT])] = slot;
             continue;
         }
-        if (missing || ps.depth[slot] >= lp.max_depth) {
-            if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);
-            terminate_path(ctx, ps, slot, cur);
-            continue;
-        }
-        PB2_CHECK(sv.prim_material[prim] < sv.material_count, 4, K_CLASSIFY, slot, sv.prim_material[prim]);
-        const uint32_t type = sv.materials[sv.prim_material[prim]].type;
-        PB2_CHECK(type < (uint32_t)kNumSurfaceTypes, 5, K_CLASSIFY, slot, type);
-        ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
-        if (guide_vertex(gs, type, ps.depth[slot])) ps.guide_q[warp_push(&ps.counts[C_GUIDE])] = slot;
+        if (gs.enabled) flush_records(gs, slot, ps.rad[slot]);  // a miss ends the path
+        terminate_path(ctx, ps, slot, cur);
     }
 }
 
