@@ -120,7 +120,7 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcOffBar);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 8);
     uint32_t& s_fail = *reinterpret_cast<uint32_t*>(smem + kTcOffBar + 12);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
 
     // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time
     for (int l = 0; l < kLayers; ++l) {

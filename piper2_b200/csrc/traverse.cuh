@@ -260,7 +260,7 @@ struct Traverser {
 
     __device__ __forceinline__ void finish_planes(const BvhView& bvh, bool& plane_front) {
         plane_front = false;
-        if (!kClosest) return;
+        if constexpr (!kClosest) return;
         for (uint32_t i = 0; i < bvh.plane_count; ++i) {
             float t, u, v;
             bool front;
