@@ -219,3 +219,24 @@ def test_cornell_converges_to_fp64_truth():
             means[spp] = float(img.mean())
     assert errs[256] * 8 < errs[16], errs
     assert abs(means[256] / ref.mean() - 1) < 0.01, (means, ref.mean())
+
+
+def test_several_lights_and_environment_bitexact(oracle):
+    """Three area lights (one of two planes) and a non-zero environment: every branch of the MIS query
+    (the selected light's plane, another light's plane, an occluder, an escape to the environment) is
+    taken, and every sample stays bit-exact with the oracle."""
+    from piper2_b200 import scenes as sc
+
+    sd = sc.cornell_box(seed=1, width=48, height=48, spp=4)
+    sd.planes = list(sd.planes) + [sc.plane_make((0.05, 0.999, 0.70), (0.15, 0.0, 0.0), (0.0, 0.0, 0.15)),
+                                   sc.plane_make((0.80, 0.999, 0.05), (0.12, 0.0, 0.0), (0.0, 0.0, 0.12)),
+                                   sc.plane_make((0.80, 0.999, 0.80), (0.10, 0.0, 0.0), (0.0, 0.0, 0.10))]
+    sd.area_lights = list(sd.area_lights) + [((3.0, 5.0, 8.0), 1, 1, (0.0, 0.0, 0.0)),
+                                             ((6.0, 6.0, 2.0), 2, 2, (0.0, 0.0, 0.0))]
+    sd.env_radiance = (0.3, 0.4, 0.5)
+    with _api().Pipeline(sd) as pl:
+        film, samples = pl.render(samples=True)
+    ofilm, osamples = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
+    diff = np.any(samples.view(np.uint32) != osamples.view(np.uint32), axis=-1)
+    assert not diff.any(), f"{diff.sum()} of {diff.size} samples differ"
+    np.testing.assert_allclose(film, ofilm, rtol=1e-5, atol=1e-6)
