@@ -761,7 +761,9 @@ __host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_
 
 // (No launch bounds: batched renders launch it with the autotuned block size, up to 512 threads.  A
 // sweep of register budgets for 4-8 resident 128-thread blocks changed render times by under 2 %.)
-template <int kType, class Ctx>
+// kGuided: the variant launched while a guide is attached (guided sampling and training records compiled in);
+// plain launches use the variant without them, which needs fewer registers.
+template <int kType, class Ctx, bool kGuided = false>
 __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
     const uint32_t n = ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
@@ -854,7 +856,7 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
             }
         }
         // continuation (PathTracing/Kernel.cpp:164-190); guided vertices sample 0.5 BxDF + 0.5 mixture
-        const bool guided = guided_type(kType) && guide_vertex(gs, kType, depth) && bsdf.no_specular;
+        const bool guided = kGuided && guided_type(kType) && guide_vertex(gs, kType, depth) && bsdf.no_specular;
         v3 wi_sh;
         spec fval;
         float pdf;
@@ -1703,7 +1705,8 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
         const uint32_t tm = pl->type_mask;
         if (tm & (1u << PB2_SURFACE_MATTE)) {
-            k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<matte>");
         }
         if (tm & (1u << PB2_SURFACE_PLASTIC)) {
@@ -1723,7 +1726,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             checked("k_shade<substrate>");
         }
         if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
-            k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            if (gs.enabled)
+                k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<conductor>");
         }
         if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
