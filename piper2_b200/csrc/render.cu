@@ -409,8 +409,10 @@ enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
 //   no plane -> any hit on (tmin, tmax): occluded means a triangle is hit, free means a miss.
 // The record (t, prim) written is what k_finish needs: the plane and its t, PB2_INVALID_PRIM for a miss,
 // or the occluding triangle.  k_finish's result is that of the closest-hit query.
+// Resident blocks per SM the register budget is sized for: 10 for closest hit, 9 for the any-hit queries
+// (as the API kernels; at 10 the any-hit queries spilled about 90 bytes).
 template <int kKind, class Ctx>
-__global__ void __launch_bounds__(kQThreads, 10) k_trace_queue(const __grid_constant__ Ctx ctx, Paths ps,
+__global__ void __launch_bounds__(kQThreads, kKind == Q_EXTEND ? 10 : 9) k_trace_queue(const __grid_constant__ Ctx ctx, Paths ps,
                                                            const uint32_t* __restrict__ queue,
                                                            const uint32_t* __restrict__ count_ptr, uint32_t* work,
                                                            unsigned long long* stat) {
@@ -1648,11 +1650,13 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     uint32_t* work = pl->accel->work;
     unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
     unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
-    static int qblocks = 0;
+    static int qblocks = 0, qblocks_any = 0;
     if (!qblocks) {
-        int per = 0;
+        int per = 0, per_any = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_any, k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0);
         qblocks = pl->sms * (per > 0 ? per : 1);
+        qblocks_any = pl->sms * (per_any > 0 ? per_any : 1);
     }
     uint32_t cur = 0;
     const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
@@ -1735,10 +1739,11 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<blackbody>");
         }
-        k_trace_queue<Q_SHADOW><<<qblocks, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1,
-                                                                   sstats);
+        k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
+                                                                       work + 1, sstats);
         checked("k_trace_queue<shadow>");
-        k_trace_queue<Q_MIS><<<qblocks, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats);
+        k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
+                                                                    stats);
         checked("k_trace_queue<mis>");
         k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_finish");
