@@ -136,18 +136,6 @@ def truth_rel_mse(img, name):
     return float(np.mean((val - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def _profile_traffic():
-    """DRAM bytes per closest-hit launch from the committed ncu summary (None if absent)."""
-    path = os.path.join(ROOT, "profiles", "trace_closest_soup1M.md")
-    try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
-                return float(line.split(":")[1].split()[0])
-    except OSError:
-        pass
-    return None
-
-
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
 
@@ -308,7 +296,6 @@ def run_ours(args):
     avg_closest_s = (sum(t_closest) / len(t_closest)) * 1e-3
     achieved = bytes_per_launch / avg_closest_s / 1e9
     peak, peak_kind = _peaks()
-    traffic = _profile_traffic()
     cpu = cpu_baseline(soup, crays, arays, args) if world == 1 else None
     render = render_bench(args) if world == 1 else None
     line = {
@@ -328,7 +315,10 @@ def run_ours(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 2 * N_RAYS * 32,
                 "d2h_bytes_per_step": N_RAYS * 16 + N_RAYS * 4},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "traffic_note": "DRAM bytes need an ncu capture, not taken in this run; see the committed "
+                                     "ncu summary of the closest-hit kernel on this workload",
+                     "peak_source": peak_kind,
                      "kernel": "k_trace_api<closest>",
                      "bytes_model": {"per_ray": BYTES_RAY + BYTES_HIT, "per_node_visit": BYTES_NODE,
                                      "per_triangle_test": BYTES_TRI,
@@ -458,6 +448,7 @@ def render_bench(args):
         for b in range(0, md.settings.samples_per_pixel, 8):
             pl.launch(film, sample_begin=b, sample_count=8)
         mm["relmse_vs_fp64_4096spp"] = truth_rel_mse(pl.resolve(film).cpu().numpy(), "mixed_materials_1920x1080")
+    mm.update(mixed_materials_cpu(md))
     result["mixed_materials"] = mm
     torch.cuda.empty_cache()
     result["batch"] = batch_bench()
@@ -467,6 +458,45 @@ def render_bench(args):
     result["guiding"] = g
     result["guiding_mlp"] = mlp_bench()
     return result
+
+
+def mixed_materials_cpu(md):
+    """CPU baselines of the mixed-materials configuration on a 128 x 64 crop at the frame's 64 spp (524,288
+    samples), on all host threads: the reference's own kernels compiled natively (oracle/_ref; the reference
+    has no conductor, so the GGX conductors become its Plastic with the conductor's F0 as specular colour,
+    no diffuse, and alpha as roughness) and the oracle's port of the same estimator on the exact scene."""
+    import copy
+
+    import oracle_py
+
+    from piper2_b200 import capi, scenes
+
+    crop = capi.Rect(896, 480, 128, 64)
+    n = crop.width * crop.height * md.settings.samples_per_pixel
+    threads = os.cpu_count() or 1
+    out = {}
+    if oracle_py.ref_available():
+        rmd = copy.copy(md)
+        rmd.materials = [scenes.material("Plastic", (0, 0, 0, 1), tuple(m.color1), (m.roughness[0], 0))
+                         if m.type == 6 else m for m in md.materials]
+        rs = oracle_py.RefScene(rmd, use_bvh=True)
+        t0 = time.perf_counter()
+        rs.render(rect=crop, threads=threads, samples=False)
+        dt = time.perf_counter() - t0
+        rs.close()
+        out["cpu_baseline"] = {"value": round(n / dt, 1), "unit": "samples/s", "cores": threads, "kind": "reference",
+                               "sample": "crop x 896-1023, y 480-543 at 64 spp (524,288 samples) through the "
+                                         "reference's own kernels compiled natively, CPU BVH in place of Embree; "
+                                         "GGX conductors as the reference's Plastic (it has no conductor)"}
+    osc = oracle_py.OracleScene(md, use_bvh=True)
+    t0 = time.perf_counter()
+    osc.render(md.settings, rect=crop, threads=threads, samples=False)
+    dt = time.perf_counter() - t0
+    osc.close()
+    out["cpu_baseline_port"] = {"value": round(n / dt, 1), "unit": "samples/s", "cores": threads, "kind": "port",
+                                "sample": "the same crop through the oracle's restatement of the estimator, exact "
+                                          "scene"}
+    return out
 
 
 def cpu_baseline(soup, crays, arays, args, sample=None):

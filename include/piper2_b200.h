@@ -255,9 +255,11 @@ int pb2_accel_get_counters(const pb2_accel* accel, uint64_t* node_visits, uint64
  * holds until exit -- at most 16384 triangles (larger inputs return PB2_ERR_INVALID_ARGUMENT).  Hits
  * equal those of pb2_accel_create + pb2_trace_closest on the same triangles.  The first call on a device
  * looks the array's device address up (cudaGetSymbolAddress) and should come before any stream
- * capture.  The BVH build synchronises `stream`; the trace is queued on it.  All calls share the array
- * and it keeps the last call's contents: calls that overlap on the GPU (other threads or streams) race
- * and must be serialised by the caller. */
+ * capture; the address is kept per device, so the call must not be used across a cudaDeviceReset of a
+ * device it ran on.  The call synchronises `stream` and returns when its hits are written; a ray whose
+ * traversal stack overflowed makes it return PB2_ERR_QUEUE_OVERFLOW.  All calls share the array and it
+ * keeps the last call's contents: calls that overlap on the GPU (other threads or streams) race and
+ * must be serialised by the caller. */
 int pb2_trace_closest_nalloc(const float* triangles_dev, uint32_t tri_count, const pb2_ray* rays_dev, uint32_t n,
                              pb2_hit* hits_dev, void* stream);
 

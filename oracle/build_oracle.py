@@ -5,7 +5,8 @@ Outputs (git-ignored):
   oracle/_build/liboracle.so     the C restatement (pb2_oracle.c)
   oracle/_build/liboracle_fp64.so the same source built with -DOR_FP64: double-precision ground truth
   oracle/_ref/librefcpu.so       the reference's own device code compiled natively with a host shim,
-                                 only when the reference sources are present (see oracle/ref/Makefile)
+                                 only when the reference sources are given (build_ref(reference_dir) or
+                                 the PIPER2_REFERENCE variable; see oracle/ref/Makefile)
 
 Flags: -O2 -ffp-contract=off, no -march=native and no fast-math, so every float operation is the one
 written in the source.
@@ -20,7 +21,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_SRC = os.environ.get("PIPER2_REFERENCE", "/root/reference")
 
 CFLAGS = ["-std=c11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-Wall",
           "-Wno-unused-function"]
@@ -66,17 +66,21 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
-def build_ref(force: bool = False) -> str | None:
-    """Compile the reference's kernels + shim into oracle/_ref/librefcpu.so if the sources exist."""
-    if not os.path.isdir(os.path.join(REFERENCE_SRC, "Src", "BuiltinComponent")):
+def build_ref(reference_dir: str | None = None, force: bool = False) -> str | None:
+    """Compile the reference's kernels + shim into oracle/_ref/librefcpu.so.  `reference_dir` (or the
+    PIPER2_REFERENCE variable) is the root of a Piper2 checkout; without one, or if it holds no
+    Src/BuiltinComponent, nothing is built and None is returned."""
+    src = reference_dir or os.environ.get("PIPER2_REFERENCE")
+    if not src or not os.path.isdir(os.path.join(src, "Src", "BuiltinComponent")):
         return None
     build_oracle()
     os.makedirs(REF_OUT, exist_ok=True)
-    _run(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REFERENCE={REFERENCE_SRC}",
+    _run(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REFERENCE={src}",
           f"OUT={REF_OUT}", f"ORACLE_BUILD={BUILD}"] + (["-B"] if force else []))
     return os.path.join(REF_OUT, "librefcpu.so")
 
 
 if __name__ == "__main__":
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
     print(build_oracle(force="--force" in sys.argv))
-    print(build_ref(force="--force" in sys.argv))
+    print(build_ref(args[0] if args else None, force="--force" in sys.argv))

@@ -25,6 +25,34 @@ int cuda_fail(cudaError_t err, const char* what) {
     return err == cudaErrorMemoryAllocation ? PB2_ERR_OUT_OF_MEMORY : PB2_ERR_CUDA;
 }
 
+int current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+    return dev;
+}
+
+cudaError_t smem_attr_once(const void* kernel, size_t bytes, std::atomic<int> (&done)[kMaxDevices]) {
+    const int dev = current_device();
+    if (dev >= 0 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess && dev >= 0) done[dev].store(1, std::memory_order_release);
+    return e;
+}
+
+int resident_grid_cached(const void* kernel, int threads, size_t smem, std::atomic<int> (&cache)[kMaxDevices]) {
+    const int dev = current_device();
+    if (dev >= 0) {
+        const int v = cache[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
+    int sms = 148, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev >= 0 ? dev : 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+    if (dev >= 0) cache[dev].store(grid, std::memory_order_relaxed);
+    return grid;
+}
+
 }  // namespace pb2
 
 using namespace pb2;

@@ -302,11 +302,9 @@ size_t grad_weights_smem() { return (size_t)kGwRows * (kGwXs + kGwDs) * 2; }
 cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n, float* out, cudaStream_t stream) {
     using namespace guide;
     if (n == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem());
-        attr = true;
-    }
+    static std::atomic<int> attr[kMaxDevices];
+    cudaError_t e = smem_attr_once((const void*)k_forward, forward_smem(), attr);
+    if (e != cudaSuccess) return e;
     const uint32_t tiles = (n + 15) / 16;
     const int grid = (int)std::min<uint32_t>((tiles + kWarps - 1) / kWarps, 148u * 2u);
     k_forward<<<grid, kThreads, forward_smem(), stream>>>(gv, features, n, out);
@@ -321,13 +319,11 @@ size_t guide_workspace_bytes() {
 cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
                            void* workspace, cudaStream_t stream) {
     using namespace guide;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_grad_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_rows_smem());
-        cudaFuncSetAttribute(k_grad_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_weights_smem());
-        attr = true;
-    }
-    cudaError_t e = cudaMemsetAsync(scalars, 0, 2 * sizeof(float), stream);
+    static std::atomic<int> attr_rows[kMaxDevices], attr_weights[kMaxDevices];
+    cudaError_t e = smem_attr_once((const void*)k_grad_rows, grad_rows_smem(), attr_rows);
+    if (e == cudaSuccess) e = smem_attr_once((const void*)k_grad_weights, grad_weights_smem(), attr_weights);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(scalars, 0, 2 * sizeof(float), stream);
     if (e != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
     __nv_bfloat16* sx = static_cast<__nv_bfloat16*>(workspace);

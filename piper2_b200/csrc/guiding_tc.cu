@@ -34,11 +34,9 @@ cudaError_t guide_forward_tc(const GuideView& gv, const float* features, uint32_
                              cudaStream_t stream) {
     using namespace guide;
     if (n == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_tc_smem());
-        attr = true;
-    }
+    static std::atomic<int> attr[kMaxDevices];
+    const cudaError_t e = smem_attr_once((const void*)k_forward_tc, forward_tc_smem(), attr);
+    if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -10,7 +10,13 @@
 // The array is a static __device__ symbol: every GPU that loads this library holds it until the
 // process exits.  Host code cannot take its address directly (the host-side symbol is only a stand-in),
 // so the first call on each device looks the device address up with cudaGetSymbolAddress, with that
-// device current, and caches it per device.
+// device current, and caches it per device.  The cached address belongs to the device's primary
+// context: after cudaDeviceReset the array may live elsewhere, so the call must not be used across a
+// reset of a device it has already run on.
+//
+// A traversal whose 48-entry stack overflows drops nodes; the call then returns
+// PB2_ERR_QUEUE_OVERFLOW instead of hits that could be wrong.  Reading that flag back needs the trace
+// to finish, so the call returns after the work it queued is done.
 #include <mutex>
 
 #include "pb2_internal.h"
@@ -20,7 +26,6 @@ namespace {
 
 constexpr uint32_t kNallocMaxTriangles = 16384;
 constexpr size_t kNallocScratchBytes = 8u << 20;  // 8 MiB
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_nalloc_scratch[kNallocScratchBytes];
 
@@ -104,5 +109,13 @@ extern "C" int pb2_trace_closest_nalloc(const float* triangles_dev, uint32_t tri
     view.root_is_leaf = tri_count <= 1;
     e = launch_trace_api(view, rays_dev, n, hits_dev, nullptr, true, false, work, counters, error_flag, stream);
     if (e != cudaSuccess) return cuda_fail(e, "trace launch (static scratch)");
+    // the stack-overflow flag, into pageable host memory (no allocation), after the trace
+    uint32_t overflow = 0;
+    if ((e = cudaMemcpyAsync(&overflow, error_flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)))
+        return cuda_fail(e, "read the nalloc traversal flag");
+    if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "pb2_trace_closest_nalloc");
+    if (overflow)
+        return fail(PB2_ERR_QUEUE_OVERFLOW, "pb2_trace_closest_nalloc: a ray's traversal stack overflowed (BVH "
+                                            "deeper than 48 entries); its hits are not valid");
     return PB2_OK;
 }

@@ -3,6 +3,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/piper2_b200.h"
@@ -14,6 +15,17 @@ namespace pb2 {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
+
+// Per-device launch set-up.  Function attributes and occupancy belong to a device, so a process that
+// drives several devices (pb2_set_device) keeps one cache entry per device index.
+constexpr int kMaxDevices = 64;
+// The calling thread's current device, or -1 if it cannot be read or is >= kMaxDevices.
+int current_device();
+// Sets a kernel's dynamic shared-memory limit on the current device, once per device.
+cudaError_t smem_attr_once(const void* kernel, size_t bytes, std::atomic<int> (&done)[kMaxDevices]);
+// Resident blocks per SM x SMs of a kernel on the current device (at least the SM count), cached per
+// device in `cache`.
+int resident_grid_cached(const void* kernel, int threads, size_t smem, std::atomic<int> (&cache)[kMaxDevices]);
 
 // The guiding network's inference weights (guiding.cu): the padded bf16 weight image and fp32 biases.
 struct GuideView {

@@ -16,8 +16,9 @@
  *             exact power-of-two scale.
  *   acos    : the binomial (arcsine) series on |x| <= 1/2, and acos(x) = 2 asin(sqrt((1-x)/2)) above.
  *
- * Accuracy is checked against the C library in the CPU tests and against CUDA's own functions in the
- * GPU tests (a few ulp).
+ * Accuracy is checked against the C library in the CPU tests (within 4 ulp).  The device runs these same
+ * definitions, so the GPU parity tests, which compare whole paths bit for bit with the CPU oracle, cover
+ * their device builds.
  */
 #pragma once
 #include <stdint.h>

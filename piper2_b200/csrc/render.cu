@@ -1624,11 +1624,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         gs.accept_prob = expect > pl->g_train_capacity ? (float)(pl->g_train_capacity / expect) : 1.0f;
         gs.salt = ++pl->g_salt;
         for (int k = 0; k < 3; ++k) { gs.bmin[k] = pl->bmin[k]; gs.binv[k] = pl->binv[k]; }
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
-            attr = true;
-        }
+        static std::atomic<int> attr[kMaxDevices];
+        const cudaError_t ea = smem_attr_once((const void*)k_guide_infer, infer_smem(), attr);
+        if (ea != cudaSuccess) return cuda_fail(ea, "k_guide_infer shared-memory limit");
     }
     SceneView sv;
     sv.materials = pl->materials;
@@ -1650,14 +1648,10 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     uint32_t* work = pl->accel->work;
     unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
     unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
-    static int qblocks = 0, qblocks_any = 0;
-    if (!qblocks) {
-        int per = 0, per_any = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_any, k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0);
-        qblocks = pl->sms * (per > 0 ? per : 1);
-        qblocks_any = pl->sms * (per_any > 0 ? per_any : 1);
-    }
+    static std::atomic<int> qcache[kMaxDevices], qcache_any[kMaxDevices];
+    const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
+    const int qblocks_any =
+        resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
     uint32_t cur = 0;
     const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
     // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed

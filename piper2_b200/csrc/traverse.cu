@@ -105,15 +105,6 @@ __global__ void __launch_bounds__(kTraceThreads, kClosest ? kMinBlocks : kMinBlo
     }
 }
 
-static int persistent_blocks(const void* kernel, int threads) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
-    if (per_sm < 1) per_sm = 1;
-    return sms * per_sm;
-}
-
 cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n, pb2_hit* hits, uint32_t* occluded,
                              bool closest, bool count, uint32_t* work, unsigned long long* counters,
                              uint32_t* error_flag, cudaStream_t stream) {
@@ -124,10 +115,9 @@ cudaError_t launch_trace_api(const BvhView& bvh, const pb2_ray* rays, uint32_t n
     const void* kernel;
     if (closest) kernel = count ? (const void*)k_trace_api<true, true> : (const void*)k_trace_api<true, false>;
     else kernel = count ? (const void*)k_trace_api<false, true> : (const void*)k_trace_api<false, false>;
-    static int blocks[4] = { 0, 0, 0, 0 };
+    static std::atomic<int> blocks[4][kMaxDevices];
     const int slot = (closest ? 2 : 0) + (count ? 1 : 0);
-    if (!blocks[slot]) blocks[slot] = persistent_blocks(kernel, kTraceThreads);
-    int grid = blocks[slot];
+    int grid = resident_grid_cached(kernel, kTraceThreads, 0, blocks[slot]);
     const int needed = (int)((n + kTraceThreads - 1) / kTraceThreads);
     if (grid > needed) grid = needed;
     if (closest) {

@@ -3,7 +3,7 @@
 Run where the reference sources are available (they are compiled natively into
 oracle/_ref/librefcpu.so by oracle/build_oracle.py):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py /path/to/Piper2     (or PIPER2_REFERENCE=/path/to/Piper2)
 
 Writes:
   sobol_digest.txt          SHA-256 of the regenerated Sobol tables
@@ -29,8 +29,8 @@ from piper2_b200 import scenes, sobol_tables  # noqa: E402
 
 def main():
     build_oracle.build_oracle()
-    if build_oracle.build_ref() is None:
-        raise SystemExit("reference sources not found")
+    if build_oracle.build_ref(sys.argv[1] if len(sys.argv) > 1 else None) is None:
+        raise SystemExit("reference sources not found: pass the Piper2 checkout or set PIPER2_REFERENCE")
     with open(os.path.join(HERE, "sobol_digest.txt"), "w") as f:
         f.write(sobol_tables.checksum(*sobol_tables.tables()) + "\n")
     sd = scenes.cornell_box(seed=0, width=32, height=32, spp=4)
