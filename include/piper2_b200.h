@@ -278,6 +278,11 @@ int pb2_pipeline_get_rect(const pb2_pipeline* pipeline, pb2_rect* full_rect, pb2
  * per (pixel, sample) the film point and radiance, 5 floats each, in (y, x, sample) order. */
 int pb2_pipeline_launch(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample_begin,
                         uint32_t sample_count, float* rgbw_dev, float* sample_out_dev, void* stream);
+/* Bounds the path slots of a single-scene launch (default 2^22, in [256, 2^30]).  A launch of more paths
+ * (rect pixels x sample_count) runs in waves of `slots` paths, one after another on the launch's stream,
+ * so its path state (about 250 bytes per slot, plus about 400 with a guide attached) stays bounded; the
+ * samples and the film are those of one launch.  Shrinking the bound frees the larger path state. */
+int pb2_pipeline_set_wave_slots(pb2_pipeline* pipeline, uint32_t slots);
 /* Resolve radiance = rgb / w (FixedSampler.cpp:122-131) into rgb_dev (width * height * 3). */
 int pb2_film_resolve(const float* rgbw_dev, uint32_t pixel_count, float* rgb_dev, void* stream);
 int pb2_pipeline_get_stats(const pb2_pipeline* pipeline, pb2_launch_stats* stats, void* stream);
@@ -319,6 +324,13 @@ int pb2_guide_gradient(pb2_guide* guide, const float* records_dev, uint32_t n, f
 /* One Adam step (beta1 0.9, beta2 0.99) on the batch. */
 int pb2_guide_train(pb2_guide* guide, const float* records_dev, uint32_t n, float learning_rate, float* loss_host,
                     void* stream);
+/* Called by every training step (pb2_guide_train, pb2_pipeline_train_guide) between the gradient and the
+ * Adam update, with the step's gradient on the device (grad_dev, `count` = pb2_guide_param_count() floats)
+ * and the stream the step runs on; the hook may rewrite the gradient in place -- e.g. average it over the
+ * ranks of a multi-GPU render with an all-reduce queued on `stream` -- and returns PB2_OK or an error code,
+ * which fails the step.  NULL removes the hook. */
+typedef int (*pb2_gradient_hook)(float* grad_dev, uint32_t count, void* stream, void* user);
+int pb2_guide_set_gradient_hook(pb2_guide* guide, pb2_gradient_hook hook, void* user);
 
 typedef struct pb2_guide_settings {
     float selection_prob;      /* probability of sampling the guide at a guided vertex (0.5) */

@@ -162,6 +162,10 @@ class Pipeline:
         torch.cuda.synchronize()
         return film.cpu().numpy(), (out.cpu().numpy() if out is not None else None)
 
+    def set_wave_slots(self, slots: int):
+        """Bound the path slots in flight; larger launches run in waves of `slots` paths."""
+        capi.check(capi.lib().pb2_pipeline_set_wave_slots(self.h, int(slots)))
+
     def resolve(self, film):
         torch = _torch()
         rgb = torch.empty((self.settings.height, self.settings.width, 3), dtype=torch.float32, device="cuda")
@@ -328,6 +332,27 @@ class Guide:
             self.close()
         except Exception:
             pass
+
+    def set_gradient_hook(self, fn):
+        """Call fn(grad) with each training step's gradient (a float32 CUDA tensor of param_count() values on
+        the library's memory, to be modified in place, e.g. all-reduced over ranks) before the Adam update.
+        fn runs on the training call's thread with torch's current stream; None removes the hook."""
+        if fn is None:
+            capi.check(capi.lib().pb2_guide_set_gradient_hook(self.h, None, None))
+            self._hook = None
+            return
+        torch = _torch()
+
+        def _call(ptr, count, stream, user):
+            try:
+                grad = torch.as_tensor(_DeviceArray(ptr, (count,)), device="cuda")
+                fn(grad)
+                return 0
+            except Exception:  # reported to the library as a failed step
+                return capi.PB2_ERR_INVALID_ARGUMENT
+
+        self._hook = capi.GRADIENT_HOOK(_call)  # kept alive as long as the guide
+        capi.check(capi.lib().pb2_guide_set_gradient_hook(self.h, C.cast(self._hook, C.c_void_p), None))
 
     def get_params(self) -> np.ndarray:
         out = np.empty(self.param_count(), dtype=np.float32)

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libpiper2_b200.so")
 
 PB2_OK = 0
+PB2_ERR_INVALID_ARGUMENT = 1
 PB2_INVALID_PRIM = 0xFFFFFFFF
 PB2_PLANE_FLAG = 0x80000000
 
@@ -167,10 +168,16 @@ SIGNATURES = [
     ("pb2_guide_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_float),
                                       C.c_void_p]),
     ("pb2_guide_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_float), C.c_void_p]),
+    ("pb2_guide_set_gradient_hook", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pb2_pipeline_set_guide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(GuideSettings)]),
+    ("pb2_pipeline_set_wave_slots", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pb2_pipeline_train_guide", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float),
                                             C.c_void_p]),
 ]
+
+
+# int (*)(float* grad_dev, uint32_t count, void* stream, void* user)
+GRADIENT_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p)
 
 
 def lib():

@@ -463,12 +463,26 @@ int pb2_guide_gradient(pb2_guide* g, const float* records, uint32_t n, float* gr
     return PB2_OK;
 }
 
+int pb2_guide_set_gradient_hook(pb2_guide* g, pb2_gradient_hook hook, void* user) {
+    if (!g) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_set_gradient_hook: null guide");
+    g->hook = hook;
+    g->hook_user = hook ? user : nullptr;
+    return PB2_OK;
+}
+
 int pb2_guide_train(pb2_guide* g, const float* records, uint32_t n, float learning_rate, float* loss_host, void* stream) {
     if (!g || (n && !records)) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_train: null argument");
     if (n == 0) return PB2_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, g->workspace, s))) return cuda_fail(e, "guide gradient");
+    if (g->hook) {
+        const int rc = g->hook(g->grad, guide::kParams, stream, g->hook_user);
+        if (rc != PB2_OK) {
+            cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s);  // the next step starts from a zero gradient
+            return fail(rc, "pb2_guide_train: the gradient hook failed");
+        }
+    }
     g->step += 1;
     const float bc1 = 1.0f - std::pow(guide::kBeta1, (float)g->step);
     const float bc2 = 1.0f - std::pow(guide::kBeta2, (float)g->step);

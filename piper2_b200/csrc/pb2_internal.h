@@ -79,5 +79,7 @@ struct pb2_guide {
     float* scalars = nullptr;  // [0] weight sum of the batch, [1] loss
     void* workspace = nullptr; // gradient staging (guide_workspace_bytes)
     uint32_t step = 0;
+    pb2_gradient_hook hook = nullptr;  // between each step's gradient and its Adam update
+    void* hook_user = nullptr;
     pb2::GuideView view() const { return pb2::GuideView{ w16, b32 }; }
 };

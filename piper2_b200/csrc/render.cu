@@ -177,7 +177,8 @@ struct LaunchParams {
     pb2_camera cam;
     uint32_t num_lights;  // area lights
     float env[3];
-    uint32_t path_count;
+    uint32_t path_count;  // paths of this wave (at most the pipeline's slot capacity)
+    uint32_t path_base;   // launch-relative index of the wave's first path
     uint32_t checks;      // PB2_DEBUG_CHECKS: verify indices, record the first violation, skip the path
     uint32_t scramble, scramble_seed;  // Owen scrambling of dimensions >= 2 (extension)
 };
@@ -371,11 +372,12 @@ __global__ void k_camera_rays(LaunchParams lp, uint32_t sample, float4* __restri
     points[i] = make_float2(px, py);
 }
 
+// Starts path lp.path_base + p of the launch in slot p.
 __global__ void k_generate(LaunchParams lp, Paths ps, GuideState gs) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= lp.path_count) return;
     uint32_t sx, sy, s;
-    path_coords(lp, p, sx, sy, s);
+    path_coords(lp, lp.path_base + p, sx, sy, s);
     uint64_t index;
     float px, py;
     v3 o, d;
@@ -549,7 +551,7 @@ __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, 
         if (atomicSub(&ctx.remaining[scene], 1u) == 1u) ctx.done_ns[scene] = globaltimer();
     } else {
         if (ctx.sample_out) {
-            float* o = ctx.sample_out + 5 * (size_t)slot;
+            float* o = ctx.sample_out + 5 * ((size_t)ctx.lp.path_base + slot);
             o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
         }
     }
@@ -1229,6 +1231,10 @@ using namespace pb2;
 
 const char* pb2_sobol_table_sha256() { return PB2_SOBOL_TABLE_SHA256; }
 
+// Path slots of a single-scene wavefront unless set otherwise (pb2_pipeline_set_wave_slots): 4M slots hold
+// about 1 GB of path state (and 1.6 GB more when a guide is attached).
+constexpr uint32_t kDefaultWaveSlots = 1u << 22;
+
 struct pb2_pipeline {
     pb2_accel* accel = nullptr;
     pb2_render_settings settings{};
@@ -1244,7 +1250,8 @@ struct pb2_pipeline {
     uint32_t type_mask = 0;  // surface types of the scene's materials: the shading kernels launched per bounce
     float env[3] = { 0, 0, 0 };
     float gauss_sub = 0.0f;
-    // path state
+    // path state: at most `wave_slots` paths are in flight; a launch with more runs in waves of that many
+    uint32_t wave_slots = kDefaultWaveSlots;
     uint32_t capacity = 0;
     void* state = nullptr;
     Paths ps{};
@@ -1598,14 +1605,16 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     const uint64_t paths = (uint64_t)rect->width * rect->height * sample_count;
     if (paths > 0x7FFFFFFFull) return fail(PB2_ERR_INVALID_ARGUMENT, "launch has more than 2^31 paths");
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    int rc = alloc_paths(pl, (uint32_t)paths);
+    // path slots in flight: the whole launch, or waves of pl->wave_slots paths
+    const uint32_t slots = (uint32_t)std::min<uint64_t>(paths, pl->wave_slots);
+    int rc = alloc_paths(pl, slots);
     if (rc) return rc;
-    const LaunchParams lp = make_params(pl, *rect, sample_begin, sample_count);
+    LaunchParams lp = make_params(pl, *rect, sample_begin, sample_count);
     GuideState gs{};
     if (pl->guide) {
         if (5ull + 9ull * pl->settings.max_depth > PB2_SOBOL_DIMS)
             return fail(PB2_ERR_NOT_SUPPORTED, "guided sampling uses 9 Sobol dimensions per bounce: max_depth too large");
-        if ((rc = alloc_guide_slots(pl, (uint32_t)paths))) return rc;
+        if ((rc = alloc_guide_slots(pl, slots))) return rc;
         gs.enabled = 1;
         gs.sel_prob = pl->guide_settings.selection_prob;
         gs.types = pl->guide_settings.guided_types;
@@ -1639,139 +1648,160 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     Paths ps = pl->ps;
     float4* film = reinterpret_cast<float4*>(rgbw);
     cudaError_t e;
-    if ((e = cudaMemsetAsync(ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream))) return cuda_fail(e, "memset counts");
-    const uint32_t pc = (uint32_t)paths;
-    if ((e = cudaMemcpyAsync(ps.counts + C_EXT_CUR, &pc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream)))
-        return cuda_fail(e, "set count");
-    k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps, gs);
-    const int grid = pl->sms * 8;
-    uint32_t* work = pl->accel->work;
-    unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
-    unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
-    static std::atomic<int> qcache[kMaxDevices], qcache_any[kMaxDevices];
-    const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
-    const int qblocks_any =
-        resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
-    uint32_t cur = 0;
-    const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
-    // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed
-    static const bool debug_sync = [] {
-        const char* v = std::getenv("PB2_DEBUG_SYNC");
-        return v && v[0] == '1';
-    }();
-    const char* failed = nullptr;
-    auto checked = [&](const char* name) {
-        if (!debug_sync || failed) return;
-        cudaError_t err = cudaGetLastError();
-        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-        if (err != cudaSuccess) {
-            failed = name;
-            e = err;
+    // one wave per `slots` paths: each starts its paths in slots 0.., runs its bounces until every path is
+    // splatted, and adds its counters to the pipeline's statistics
+    for (uint64_t base = 0; base < paths; base += slots) {
+        lp.path_base = (uint32_t)base;
+        lp.path_count = (uint32_t)std::min<uint64_t>(slots, paths - base);
+        if ((e = cudaMemsetAsync(ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream))) return cuda_fail(e, "memset counts");
+        const uint32_t pc = lp.path_count;
+        if ((e = cudaMemcpyAsync(ps.counts + C_EXT_CUR, &pc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream)))
+            return cuda_fail(e, "set count");
+        k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps, gs);
+        const int grid = pl->sms * 8;
+        uint32_t* work = pl->accel->work;
+        unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
+        unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
+        static std::atomic<int> qcache[kMaxDevices], qcache_any[kMaxDevices];
+        const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
+        const int qblocks_any =
+            resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
+        uint32_t cur = 0;
+        const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
+        // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed
+        static const bool debug_sync = [] {
+            const char* v = std::getenv("PB2_DEBUG_SYNC");
+            return v && v[0] == '1';
+        }();
+        const char* failed = nullptr;
+        auto checked = [&](const char* name) {
+            if (!debug_sync || failed) return;
+            cudaError_t err = cudaGetLastError();
+            if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+            if (err != cudaSuccess) {
+                failed = name;
+                e = err;
+            }
+        };
+        checked("k_generate");
+        SingleCtx ctx;
+        ctx.lp = lp;
+        ctx.sv = sv;
+        ctx.film = film;
+        ctx.sample_out = sample_out;
+        // The bounce kernels read their queue sizes on the device, so the host checks for completion only
+        // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
+        // the bounces between checks queue up without a host round trip.
+        constexpr int kCheckEvery = 4;
+        uint32_t active = paths > 0 ? 1u : 0u;
+        for (int bounce = 0; !failed; ++bounce) {
+            if (bounce % kCheckEvery == 0) {
+                if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                         stream)) ||
+                    (e = cudaStreamSynchronize(stream)))
+                    return cuda_fail(e, "read queue size");
+                if (active == 0) break;
+            }
+            if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
+            // grid from the last known queue size (an upper bound: queues only shrink); the persistent trace
+            // blocks stop when the queue is drained
+            const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
+            cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
+            k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
+                                                                     stats);
+            checked("k_trace_queue<extend>");
+            k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_classify");
+            if (gs.enabled) k_guide_infer<<<pl->sms * 2, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
+            checked("k_guide_infer");
+            // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
+            const uint32_t tm = pl->type_mask;
+            if (tm & (1u << PB2_SURFACE_MATTE)) {
+                if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<matte>");
+            }
+            if (tm & (1u << PB2_SURFACE_PLASTIC)) {
+                k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<plastic>");
+            }
+            if (tm & (1u << PB2_SURFACE_GLASS)) {
+                k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<glass>");
+            }
+            if (tm & (1u << PB2_SURFACE_MIRROR)) {
+                k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<mirror>");
+            }
+            if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
+                k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<substrate>");
+            }
+            if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
+                if (gs.enabled)
+                    k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<conductor>");
+            }
+            if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
+                k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+                checked("k_shade<blackbody>");
+            }
+            k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
+                                                                           work + 1, sstats);
+            checked("k_trace_queue<shadow>");
+            k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
+                                                                        stats);
+            checked("k_trace_queue<mis>");
+            k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_finish");
+            k_advance<<<1, 1, 0, stream>>>(ps.counts);
+            checked("k_advance");
+            if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
+            cur ^= 1u;
         }
-    };
-    checked("k_generate");
-    SingleCtx ctx;
-    ctx.lp = lp;
-    ctx.sv = sv;
-    ctx.film = film;
-    ctx.sample_out = sample_out;
-    // The bounce kernels read their queue sizes on the device, so the host checks for completion only
-    // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
-    // the bounces between checks queue up without a host round trip.
-    constexpr int kCheckEvery = 4;
-    uint32_t active = paths > 0 ? 1u : 0u;
-    for (int bounce = 0; !failed; ++bounce) {
-        if (bounce % kCheckEvery == 0) {
-            if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                     stream)) ||
-                (e = cudaStreamSynchronize(stream)))
-                return cuda_fail(e, "read queue size");
-            if (active == 0) break;
-        }
-        if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
-        // grid from the last known queue size (an upper bound: queues only shrink); the persistent trace
-        // blocks stop when the queue is drained
-        const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
-        cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
-        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
-                                                                 stats);
-        checked("k_trace_queue<extend>");
-        k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_classify");
-        if (gs.enabled) k_guide_infer<<<pl->sms * 2, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
-        checked("k_guide_infer");
-        // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
-        const uint32_t tm = pl->type_mask;
-        if (tm & (1u << PB2_SURFACE_MATTE)) {
-            if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<matte>");
-        }
-        if (tm & (1u << PB2_SURFACE_PLASTIC)) {
-            k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<plastic>");
-        }
-        if (tm & (1u << PB2_SURFACE_GLASS)) {
-            k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<glass>");
-        }
-        if (tm & (1u << PB2_SURFACE_MIRROR)) {
-            k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<mirror>");
-        }
-        if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
-            k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<substrate>");
-        }
-        if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
-            if (gs.enabled)
-                k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<conductor>");
-        }
-        if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
-            k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<blackbody>");
-        }
-        k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
-                                                                       work + 1, sstats);
-        checked("k_trace_queue<shadow>");
-        k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
-                                                                    stats);
-        checked("k_trace_queue<mis>");
-        k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_finish");
-        k_advance<<<1, 1, 0, stream>>>(ps.counts);
-        checked("k_advance");
-        if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
-        cur ^= 1u;
-    }
-    if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
-    uint32_t counts[C_COUNT];
-    if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
-        (e = cudaStreamSynchronize(stream)))
-        return cuda_fail(e, "read stats");
-    unsigned long long v;
-    std::memcpy(&v, counts + C_STAT_CLOSEST, 8);
-    pl->stats.closest_rays += v;
-    std::memcpy(&v, counts + C_STAT_SHADOW, 8);
-    pl->stats.shadow_rays += v;
-    std::memcpy(&v, counts + C_STAT_VERTICES, 8);
-    pl->stats.path_vertices += v;
-    pl->stats.paths += paths;
-    if (counts[C_CHECK])
-        return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
-                                      std::to_string(counts[C_CHECK + 1]) + " at slot " +
-                                      std::to_string(counts[C_CHECK + 2]) + ", value " +
-                                      std::to_string(counts[C_CHECK + 3]));
-    if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
-    if (counts[C_TC_ERROR]) return fail(PB2_ERR_DEVICE_TIMEOUT, "guide inference: a tensor-core wait timed out");
-    if (gs.enabled) {
-        uint32_t tc[2];
-        if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+        if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
+        uint32_t counts[C_COUNT];
+        if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
             (e = cudaStreamSynchronize(stream)))
-            return cuda_fail(e, "read record count");
-        pl->g_offered = tc[1];
+            return cuda_fail(e, "read stats");
+        unsigned long long v;
+        std::memcpy(&v, counts + C_STAT_CLOSEST, 8);
+        pl->stats.closest_rays += v;
+        std::memcpy(&v, counts + C_STAT_SHADOW, 8);
+        pl->stats.shadow_rays += v;
+        std::memcpy(&v, counts + C_STAT_VERTICES, 8);
+        pl->stats.path_vertices += v;
+        pl->stats.paths += pc;
+        if (counts[C_CHECK])
+            return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
+                                          std::to_string(counts[C_CHECK + 1]) + " at slot " +
+                                          std::to_string(counts[C_CHECK + 2]) + ", value " +
+                                          std::to_string(counts[C_CHECK + 3]));
+        if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+        if (counts[C_TC_ERROR]) return fail(PB2_ERR_DEVICE_TIMEOUT, "guide inference: a tensor-core wait timed out");
+        if (gs.enabled) {
+            uint32_t tc[2];
+            if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+                (e = cudaStreamSynchronize(stream)))
+                return cuda_fail(e, "read record count");
+            pl->g_offered = tc[1];
+        }
+    }
+    return PB2_OK;
+}
+
+int pb2_pipeline_set_wave_slots(pb2_pipeline* pl, uint32_t slots) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_wave_slots: null pipeline");
+    if (slots < 256 || slots > (1u << 30)) return fail(PB2_ERR_INVALID_ARGUMENT, "wave slots must lie in [256, 2^30]");
+    pl->wave_slots = slots;
+    if (pl->capacity > slots) {  // give back path state above the new bound
+        cudaFree(pl->state);
+        pl->state = nullptr;
+        pl->capacity = 0;
+        cudaFree(pl->guide_state);
+        pl->guide_state = nullptr;
+        pl->guide_cap = 0;
     }
     return PB2_OK;
 }

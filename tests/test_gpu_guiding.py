@@ -257,3 +257,55 @@ def test_guide_settings_are_checked():
             pl.set_guide(g, guided_types=1 << 2)
         with pytest.raises(capi.PB2Error):
             pl.train_guide(steps=1)
+
+
+def test_gradient_hook_sees_and_replaces_the_gradient():
+    """The hook receives each step's gradient on the device before Adam and may rewrite it (the multi-GPU
+    render averages it over ranks this way): the first Adam step then moves every parameter by
+    -lr * c / (|c| + eps) for the gradient c the hook left."""
+    api = _api()
+    rng = np.random.default_rng(31)
+    g = api.Guide(seed=5)
+    params = _trained_params(5)
+    g.set_params(params)  # resets the Adam state
+    rec = _records(rng, 4096)
+    expected, _ = g.gradient(rec)
+    seen = []
+    c = np.where(rng.uniform(size=params.size) < 0.5, -1e-3, 2e-3).astype(np.float32)
+
+    def hook(grad):
+        import torch
+
+        seen.append(grad.cpu().numpy().copy())
+        grad.copy_(torch.from_numpy(c).to(grad.device))
+
+    g.set_gradient_hook(hook)
+    lr = 1e-3
+    g.train(rec, learning_rate=lr)
+    assert len(seen) == 1
+    got = seen[0].astype(np.float64)
+    cos = got @ expected / (np.linalg.norm(got) * np.linalg.norm(expected))
+    assert cos > 0.9999, cos
+    upd = g.get_params().astype(np.float64) - params
+    np.testing.assert_allclose(upd, -lr * np.sign(c), rtol=1e-3, atol=1e-6 * np.abs(params).max())
+
+
+def test_gradient_hook_failure_fails_the_step():
+    from piper2_b200 import capi
+
+    api = _api()
+    rng = np.random.default_rng(32)
+    g = api.Guide(seed=6)
+    p0 = g.get_params()
+    rec = _records(rng, 1024)
+
+    def bad(grad):
+        raise RuntimeError("all-reduce failed")
+
+    g.set_gradient_hook(bad)
+    with pytest.raises(capi.PB2Error, match="hook"):
+        g.train(rec, learning_rate=1e-3)
+    assert np.array_equal(g.get_params(), p0)  # no update was applied
+    g.set_gradient_hook(None)
+    g.train(rec, learning_rate=1e-3)
+    assert not np.array_equal(g.get_params(), p0)
