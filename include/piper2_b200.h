@@ -348,6 +348,12 @@ typedef struct pb2_guide_settings {
 
 /* Attaches `guide` (not owned; NULL detaches) to the pipeline: later launches sample and record with it. */
 int pb2_pipeline_set_guide(pb2_pipeline* pipeline, pb2_guide* guide, const pb2_guide_settings* settings);
+/* Verification copy of the in-render inference: while set, every guided launch appends one row of 52
+ * floats per vertex whose mixture it inferred -- the vertex's 9 network inputs (position in the unit scene
+ * box, shading normal, outgoing direction) and the 40 mixture parameters it used (8 lobe weights, 8 unit
+ * means xyz, 8 concentrations), 3 unused -- to rows_dev, at most `capacity` rows; *count_dev (device
+ * memory, cleared by the caller) counts the vertices offered.  rows_dev = NULL stops it. */
+int pb2_pipeline_set_guide_dump(pb2_pipeline* pipeline, float* rows_dev, uint32_t capacity, uint32_t* count_dev);
 /* Runs `steps` Adam steps of `batch` records drawn uniformly from the records of the launches since the
  * last call (weights clamped per pb2_guide_settings.weight_quantile), then clears them.  Writes the last
  * step's loss. */

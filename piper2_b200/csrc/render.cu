@@ -212,7 +212,13 @@ struct GuideState {
     float bmin[3], binv[3];
     uint32_t types;         // bit t set: vertices of surface type t sample the guide
     uint32_t max_depth;     // only vertices at path depth < max_depth sample the guide
+    float* dump;            // optional (pb2_pipeline_set_guide_dump): kGuideDumpFloats per inferred vertex
+    uint32_t* dump_count;
+    uint32_t dump_cap;
 };
+// A dumped row: the vertex's 9 input features (position in the unit box, normal, outgoing direction), then
+// its 40 mixture parameters in the layout of GuideState::mix, 3 floats of padding.
+constexpr uint32_t kGuideDumpFloats = 52;
 
 // Whether a surface vertex of type `type` at path depth `depth` samples the guide (classification and
 // shading must agree: the guide is evaluated exactly for these vertices).
@@ -962,6 +968,9 @@ struct GuideRows {
     GuideState gs;
     __device__ __forceinline__ void features(uint32_t row, float (&f)[9], uint32_t& slot) const {
         slot = ps.guide_q[row];
+        slot_features(slot, f);
+    }
+    __device__ __forceinline__ void slot_features(uint32_t slot, float (&f)[9]) const {
         const float4 h = ps.hit[slot];
         const float4 o4 = ps.o[slot], d4 = ps.d[slot];
         const v3 d = mk3(d4.x, d4.y, d4.z);
@@ -987,6 +996,16 @@ struct GuideRows {
             mp[9 + 3 * k] = m.mu[k][1];
             mp[10 + 3 * k] = m.mu[k][2];
             mp[32 + k] = m.kappa[k];
+        }
+        if (gs.dump) {  // verification copy of the vertex's inputs and mixture
+            const uint32_t i = atomicAdd(gs.dump_count, 1u);
+            if (i < gs.dump_cap) {
+                float f[9];
+                slot_features(slot, f);
+                float* o = gs.dump + (size_t)kGuideDumpFloats * i;
+                for (int k = 0; k < 9; ++k) o[k] = f[k];
+                for (int k = 0; k < 40; ++k) o[9 + k] = mp[k];
+            }
         }
     }
 };
@@ -1264,6 +1283,9 @@ struct pb2_pipeline {
     pb2_guide_settings guide_settings{};
     uint32_t guide_cap = 0;
     void* guide_state = nullptr;
+    float* g_dump = nullptr;  // optional verification rows (pb2_pipeline_set_guide_dump), caller's memory
+    uint32_t* g_dump_count = nullptr;
+    uint32_t g_dump_cap = 0;
     float* g_mix = nullptr;
     float4* g_rec = nullptr;
     uint32_t* g_nrec = nullptr;
@@ -1619,6 +1641,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         gs.sel_prob = pl->guide_settings.selection_prob;
         gs.types = pl->guide_settings.guided_types;
         gs.max_depth = pl->guide_settings.max_guided_depth ? pl->guide_settings.max_guided_depth : 0xFFFFFFFFu;
+        gs.dump = pl->g_dump;
+        gs.dump_count = pl->g_dump_count;
+        gs.dump_cap = pl->g_dump_cap;
         gs.net = pl->guide->view();
         gs.mix = pl->g_mix;
         gs.rec = pl->g_rec;
@@ -1788,6 +1813,16 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             pl->g_offered = tc[1];
         }
     }
+    return PB2_OK;
+}
+
+int pb2_pipeline_set_guide_dump(pb2_pipeline* pl, float* rows_dev, uint32_t capacity, uint32_t* count_dev) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_guide_dump: null pipeline");
+    if (rows_dev && (!count_dev || capacity == 0))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_guide_dump: rows need a capacity and a counter");
+    pl->g_dump = rows_dev;
+    pl->g_dump_count = rows_dev ? count_dev : nullptr;
+    pl->g_dump_cap = rows_dev ? capacity : 0;
     return PB2_OK;
 }
 

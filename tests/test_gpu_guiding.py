@@ -309,3 +309,47 @@ def test_gradient_hook_failure_fails_the_step():
     g.set_gradient_hook(None)
     g.train(rec, learning_rate=1e-3)
     assert not np.array_equal(g.get_params(), p0)
+
+
+def test_in_render_inference_matches_bf16_model():
+    """The per-bounce inference inside the render (k_guide_infer: the tcgen05 tile loop on the guided
+    vertices of the surface queues) against the float64 model with the kernel's bf16 roundings: for every
+    vertex it inferred, the mixture it used (lobe weights, unit means, concentrations) is the model's mixture
+    of the inputs it recorded, and those inputs are a valid hit (position inside the unit box, unit normal
+    facing the outgoing direction)."""
+    import torch
+
+    api = _api()
+    sd = scenes.guiding_room(seed=0, width=64, height=36, spp=4, max_depth=16)
+    params = _trained_params(13)
+    g = api.Guide(seed=13)
+    g.set_params(params)
+    cap = 1 << 14
+    rows = torch.zeros((cap, 52), dtype=torch.float32, device="cuda")
+    count = torch.zeros(4, dtype=torch.int32, device="cuda")
+    from piper2_b200 import capi
+    import ctypes as C
+
+    with api.Pipeline(sd) as pl:
+        pl.set_guide(g, max_guided_depth=0)  # every Matte vertex infers its mixture
+        capi.check(capi.lib().pb2_pipeline_set_guide_dump(pl.h, C.c_void_p(rows.data_ptr()), cap,
+                                                          C.c_void_p(count.data_ptr())))
+        film = pl.new_film()
+        pl.launch(film, sample_begin=0, sample_count=2)
+        torch.cuda.synchronize()
+        capi.check(capi.lib().pb2_pipeline_set_guide_dump(pl.h, None, 0, None))
+    n = min(int(count[0].item()), cap)
+    assert n > 2000, n
+    d = rows[:n].cpu().numpy().astype(np.float64)
+    f = np.zeros((n, 12), dtype=np.float32)
+    f[:, :9] = d[:, :9]
+    assert np.all((f[:, 0:3] > -1e-3) & (f[:, 0:3] < 1 + 1e-3))
+    np.testing.assert_allclose(np.linalg.norm(f[:, 3:6], axis=1), 1.0, atol=1e-4)
+    assert np.all(np.sum(f[:, 3:6] * f[:, 6:9], axis=1) > -1e-4)  # normal on the outgoing side
+    pi, mu, kappa, _, _ = G.mixture(_forward_bf16(params, f))
+    w_gpu, mu_gpu, k_gpu = d[:, 9:17], d[:, 17:41].reshape(n, 8, 3), d[:, 41:49]
+    assert np.linalg.norm(w_gpu - pi) / np.linalg.norm(pi) <= 1e-2
+    assert np.linalg.norm(k_gpu - kappa) / np.linalg.norm(kappa) <= 1e-2
+    heavy = pi > 0.02
+    cos = np.sum(mu_gpu * mu, axis=2)[heavy]
+    assert np.mean(cos) > 0.9999 and np.min(cos) > 0.99, (np.mean(cos), np.min(cos))
