@@ -307,10 +307,10 @@ int pb2_guide_destroy(pb2_guide* guide);
 /* Flat fp32 parameters: per layer W[out][in] then b[out]; setting them resets the Adam state. */
 int pb2_guide_set_params(pb2_guide* guide, const float* params_host, uint32_t count);
 int pb2_guide_get_params(const pb2_guide* guide, float* params_host, uint32_t count);
-/* features_dev: n rows of 12 floats (position in the unit cube xyz, normal xyz, outgoing dir xyz, unused);
- * out_dev: n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused).  Runs on the
- * tcgen05 tensor cores (128 rows per CTA, TMEM accumulators); synchronises `stream` to check that no
- * tensor-core wait timed out (PB2_ERR_DEVICE_TIMEOUT). */
+/* features_dev (16-byte aligned): n rows of 12 floats (position in the unit cube xyz, normal xyz, outgoing dir xyz, unused);
+ * out_dev (16-byte aligned): n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused).
+ * Runs on the tcgen05 tensor cores (four independent 128-row tiles per CTA, TMEM accumulators); synchronises
+ * `stream` to check that no tensor-core wait timed out (PB2_ERR_DEVICE_TIMEOUT). */
 int pb2_guide_forward(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev, void* stream);
 /* The same forward pass on mma.sync tiles (16 rows per warp), asynchronous; the cross-check of the tcgen05
  * path and the form the integrator's per-bounce inference uses. */

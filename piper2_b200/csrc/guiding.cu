@@ -430,6 +430,8 @@ int pb2_guide_get_params(const pb2_guide* g, float* params, uint32_t count) {
 int pb2_guide_forward(const pb2_guide* g, const float* features, uint32_t n, float* out, void* stream) {
     if (!g || (n && (!features || !out))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward: null argument");
     if (n == 0) return PB2_OK;
+    if ((reinterpret_cast<uintptr_t>(features) | reinterpret_cast<uintptr_t>(out)) & 15u)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward: features and outputs must be 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint32_t* flag = reinterpret_cast<uint32_t*>(g->scalars + 3);
     cudaError_t e;

@@ -9,20 +9,28 @@ namespace {
 
 // features: n rows of 12 floats (pos01 xyz, normal xyz, wo xyz, unused); out: n rows of 48 raw outputs
 struct FeatureRows {
+    static constexpr bool kStaged = true;  // a tile's outputs are contiguous: write them with coalesced stores
     const float* feat;
     float* out;
     __device__ __forceinline__ void features(uint32_t row, float (&f)[9], uint32_t& key) const {
-        for (int i = 0; i < 9; ++i) f[i] = feat[12 * (size_t)row + i];
+        const float4* p = reinterpret_cast<const float4*>(feat + 12 * (size_t)row);
+        const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+        f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w;
+        f[4] = b.x; f[5] = b.y; f[6] = b.z; f[7] = b.w;
+        f[8] = c.x;
         key = row;
     }
-    __device__ __forceinline__ void output(uint32_t key, const float (&y)[kOut]) const {
-        float* o = out + (size_t)key * kOut;
-#pragma unroll
-        for (int i = 0; i < kOut; i += 4) *reinterpret_cast<float4*>(o + i) = make_float4(y[i], y[i + 1], y[i + 2], y[i + 3]);
+    __device__ __forceinline__ void store_tile(uint32_t row0, uint32_t count, const float* staged, int t,
+                                               int threads) const {
+        const float4* src = reinterpret_cast<const float4*>(staged);
+        float4* dst = reinterpret_cast<float4*>(out + (size_t)row0 * kOut);
+        const uint32_t n4 = count * (kOut / 4);
+        for (uint32_t i = t; i < n4; i += threads) dst[i] = src[i];
     }
+    __device__ __forceinline__ void output(uint32_t, const float (&)[kOut]) const {}
 };
 
-__global__ void __launch_bounds__(kTcThreads) k_forward_tc(GuideView gv, const float* __restrict__ features, uint32_t n,
+__global__ void __launch_bounds__(kTcThreads, 1) k_forward_tc(GuideView gv, const float* __restrict__ features, uint32_t n,
                                                            float* __restrict__ out, uint32_t* __restrict__ error) {
     extern __shared__ __align__(1024) unsigned char smem[];
     forward_tc_tiles(gv, n, FeatureRows{ features, out }, error, smem);
@@ -41,7 +49,7 @@ cudaError_t guide_forward_tc(const GuideView& gv, const float* features, uint32_
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sms * 2u);
+    const int grid = (int)std::min<uint32_t>((tiles + kTcGroups - 1) / kTcGroups, (uint32_t)sms);
     k_forward_tc<<<grid, kTcThreads, forward_tc_smem(), stream>>>(gv, features, n, out, error);
     return cudaGetLastError();
 }

@@ -1,17 +1,22 @@
 // guiding_tc.cuh -- the guiding network's forward pass on the 5th-generation tensor cores (tcgen05).
 //
-// One CTA of 4 warps evaluates 128 rows at a time.  The encoded inputs and each hidden layer's output are
-// bf16 operands in shared memory in the canonical K-major, no-swizzle UMMA layout (8-row x 16-byte core
-// matrices; within a tile, core matrices adjacent in K are 128 bytes apart (LBO) and 8-row groups are
-// K x 16 bytes apart (SBO)); the weights of all five layers are staged once per CTA in the same layout.
-// For each layer one thread issues K/16 `tcgen05.mma.cta_group::1.kind::f16` (M = 128, N = 64 or 48,
-// BF16 x BF16 -> FP32) into a 64-column TMEM accumulator and commits them to an mbarrier; every warp then
-// reads its 32 rows back with `tcgen05.ld.32x32b`, adds the bias, applies ReLU, and writes the next layer's
-// bf16 operand (or the fp32 outputs after the last layer).  Shared-memory writes that an MMA reads are made
-// visible to the tensor core's async proxy with `fence.proxy.async.shared::cta` before the barrier.
+// A CTA holds the weights of all five layers once in shared memory and runs kTcGroups independent warp
+// groups of 4 warps; each group evaluates its own 128-row tiles, so while one group waits for its MMAs
+// another encodes inputs or drains its accumulator (the tensor pipe is shared by the groups of the SM).
+// The encoded inputs and each hidden layer's output are bf16 operands in shared memory in the canonical
+// K-major, no-swizzle UMMA layout (8-row x 16-byte core matrices; within a tile, core matrices adjacent in
+// K are 128 bytes apart (LBO) and 8-row groups are K x 16 bytes apart (SBO)); the weights use the same
+// layout.  For each layer one thread of the group issues K/16 `tcgen05.mma.cta_group::1.kind::f16`
+// (M = 128, N = 64 or 48, BF16 x BF16 -> FP32) into the group's 64 TMEM columns and commits them to the
+// group's mbarrier; every warp of the group then reads its 32 rows back with `tcgen05.ld.32x32b`, adds the
+// bias, applies ReLU, and writes the next layer's bf16 operand.  A group's two operand buffers alternate
+// between layers (input tile -> H -> A -> H -> A), and after the last layer the input buffer stages the
+// fp32 outputs so that a row-major output is written with coalesced stores.  Shared-memory writes that
+// an MMA reads are made visible to the tensor core's async proxy with `fence.proxy.async.shared::cta`
+// before the group's named barrier.
 //
-// Every wait on the mbarrier is bounded: on time-out the kernel records an error, stops issuing work, gives
-// the tensor core a bounded time to drain, frees its TMEM and returns.
+// Every wait on an mbarrier is bounded: on time-out the group records an error, stops issuing work, gives
+// the tensor core a bounded time to drain, and the CTA frees its TMEM and returns.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -22,24 +27,32 @@ namespace pb2 {
 namespace guide {
 
 constexpr int kTcRows = 128;
-constexpr int kTcThreads = 128;
-constexpr uint32_t kTmemCols = 64;
+constexpr int kTcGroups = 4;                       // independent 128-row tiles in flight per CTA
+constexpr int kTcGroupThreads = 128;
+constexpr int kTcThreads = kTcGroupThreads * kTcGroups;
+constexpr uint32_t kTmemColsPerGroup = 64;
+constexpr uint32_t kTmemCols = kTmemColsPerGroup * kTcGroups;  // 256: a power of two, as tcgen05.alloc needs
 constexpr uint32_t kWaitLimit = 1u << 20;  // mbarrier polls before a wait counts as failed
 
 __host__ __device__ constexpr int tc_w_offset(int l) {  // bytes of layer l's weights in the staged image
     return l == 0 ? 0 : tc_w_offset(l - 1) + layer_out(l - 1) * layer_in(l - 1) * 2;
 }
 constexpr int kTcWBytes = tc_w_offset(kLayers);                        // 43,008
-constexpr int kTcXBytes = kTcRows * kIn * 2;                           // 24,576
+constexpr int kTcABytes = kTcRows * kIn * 2;                           // 24,576: input tile, odd layers' output,
+                                                                       // and the fp32 output staging (128 x 48)
 constexpr int kTcHBytes = kTcRows * kHid * 2;                          // 16,384
+constexpr int kTcGroupBytes = kTcABytes + kTcHBytes;
 constexpr int kTcOffW = 0;
-constexpr int kTcOffX = kTcWBytes;                                     // 1024-aligned below
-constexpr int kTcOffH0 = kTcOffX + kTcXBytes;
-constexpr int kTcOffH1 = kTcOffH0 + kTcHBytes;
-constexpr int kTcOffBias = kTcOffH1 + kTcHBytes;
-constexpr int kTcOffBar = kTcOffBias + kBiasElems * 4;
-constexpr int kTcSmem = kTcOffBar + 16;
-static_assert(kTcOffX % 1024 == 0 && kTcOffH0 % 1024 == 0 && kTcOffH1 % 1024 == 0, "operand alignment");
+constexpr int kTcOffGroups = kTcWBytes;                                // 1024-aligned below
+constexpr int kTcOffBias = kTcOffGroups + kTcGroups * kTcGroupBytes;
+constexpr int kTcOffBar = kTcOffBias + kBiasElems * 4;                 // kTcGroups mbarriers
+constexpr int kTcOffSlot = kTcOffBar + 8 * kTcGroups;                  // TMEM base address
+constexpr int kTcOffFail = kTcOffSlot + 4;                             // kTcGroups failure flags
+constexpr int kTcSmem = kTcOffFail + 4 * kTcGroups;
+static_assert(kTcOffGroups % 1024 == 0 && kTcABytes % 1024 == 0 && kTcGroupBytes % 1024 == 0, "operand alignment");
+static_assert(kTcABytes >= kTcRows * kOut * 4, "output staging fits the input buffer");
+static_assert(kTcOffBar % 8 == 0, "mbarrier alignment");
+static_assert(kTcSmem <= 227 * 1024, "shared memory per CTA");
 
 // Byte offset of element (row, k) of a K-major operand with `kdim` columns in the core-matrix layout.
 __host__ __device__ constexpr uint32_t core_offset(uint32_t row, uint32_t k, uint32_t kdim) {
@@ -106,23 +119,31 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 
+// Barrier of one warp group (named barrier 1 + g; barrier 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(kTcGroupThreads) : "memory");
+}
+
 // The tile loop of the tensor-core forward pass, for a CTA of kTcThreads threads with forward_tc_smem() bytes
-// of dynamic shared memory.  Rows: thread t handles row tile * 128 + t of the n rows; rows.features(row, f,
-// key) fills the 9 input features and a key the thread keeps, rows.output(key, y) receives the 48 raw
-// outputs of a row below n.  error[0] is set when a tensor-core wait timed out.
+// of dynamic shared memory.  Rows: thread t of a group handles row tile * 128 + t of the n rows;
+// rows.features(row, f, key) fills the 9 input features and a key the thread keeps.  Outputs: with
+// Rows::kStaged, rows.store_tile(row0, count, staged, t, threads) writes rows [row0, row0 + count) from the
+// group's staged fp32 outputs (row-major, 48 per row) cooperatively; otherwise rows.output(key, y) receives
+// the 48 raw outputs of a row below n.  error[0] is set when a tensor-core wait timed out.
 template <class Rows>
 __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n, const Rows& rows, uint32_t* error,
                                                  unsigned char* smem) {
-    unsigned char* w_s = smem + kTcOffW;
-    unsigned char* x_s = smem + kTcOffX;
-    unsigned char* h_s[2] = { smem + kTcOffH0, smem + kTcOffH1 };
-    float* b_s = reinterpret_cast<float*>(smem + kTcOffBias);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcOffBar);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 8);
-    uint32_t& s_fail = *reinterpret_cast<uint32_t*>(smem + kTcOffBar + 12);
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = tid / kTcGroupThreads, gt = tid % kTcGroupThreads;  // group and thread within it
+    unsigned char* w_s = smem + kTcOffW;
+    unsigned char* buf[2] = { smem + kTcOffGroups + g * kTcGroupBytes,                // A: input tile
+                              smem + kTcOffGroups + g * kTcGroupBytes + kTcABytes };  // H
+    float* b_s = reinterpret_cast<float*>(smem + kTcOffBias);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcOffBar) + g;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffSlot);
+    volatile uint32_t& s_fail = reinterpret_cast<uint32_t*>(smem + kTcOffFail)[g];
 
-    // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time
+    // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time (all groups)
     for (int l = 0; l < kLayers; ++l) {
         const int in = layer_in(l), outd = layer_out(l), chunks = outd * (in / 8);
         for (int c = tid; c < chunks; c += kTcThreads) {
@@ -132,7 +153,7 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
         }
     }
     for (int i = tid; i < kBiasElems; i += kTcThreads) b_s[i] = gv.b32[i];
-    if (tid == 0) {
+    if (gt == 0) {
         s_fail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -146,14 +167,15 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = *tmem_slot + (uint32_t)g * kTmemColsPerGroup;  // this group's accumulator columns
     const uint32_t bar_addr = smem_u32(bar);
     uint32_t phase = 0;
     bool failed = false;
 
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
-        const uint32_t row = tile * kTcRows + tid;
+    const uint32_t stride = gridDim.x * kTcGroups;
+    for (uint32_t tile = blockIdx.x * kTcGroups + g; tile < tiles && !failed; tile += stride) {
+        const uint32_t row = tile * kTcRows + gt;
         uint32_t key = 0;
         float y[kOut];
         {
@@ -163,35 +185,36 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
             encode_row(f, enc);
 #pragma unroll
             for (int kc = 0; kc < kIn / 8; ++kc)
-                *reinterpret_cast<int4*>(x_s + core_offset(tid, kc * 8, kIn)) = *reinterpret_cast<const int4*>(enc + kc * 8);
+                *reinterpret_cast<int4*>(buf[0] + core_offset(gt, kc * 8, kIn)) = *reinterpret_cast<const int4*>(enc + kc * 8);
         }
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        group_sync(g);
         tc_fence_after();
-        const unsigned char* a_buf = x_s;
         for (int l = 0; l < kLayers; ++l) {
             const uint32_t kdim = layer_in(l), ndim = layer_out(l);
-            if (tid == 0) {
+            const unsigned char* a_buf = buf[l & 1];       // layer l reads A, H, A, H, A
+            unsigned char* o_buf = buf[(l + 1) & 1];       // and writes H, A, H, A
+            if (gt == 0) {
                 const uint32_t a0 = smem_u32(a_buf), b0 = smem_u32(w_s + tc_w_offset(l));
-                for (uint32_t s = 0; s < kdim / 16; ++s)
-                    mma_bf16(tmem, smem_desc(a0 + 256 * s, 128, kdim * 16), smem_desc(b0 + 256 * s, 128, kdim * 16),
-                             instr_desc(ndim), s > 0 ? 1u : 0u);
+                for (uint32_t k = 0; k < kdim / 16; ++k)
+                    mma_bf16(tmem, smem_desc(a0 + 256 * k, 128, kdim * 16), smem_desc(b0 + 256 * k, 128, kdim * 16),
+                             instr_desc(ndim), k > 0 ? 1u : 0u);
                 mma_commit(bar_addr);
             }
             if (!mbar_wait_bounded(bar_addr, phase)) {
-                atomicExch(&s_fail, 1u);
+                s_fail = 1u;
                 atomicExch(error, 1u);
             }
             phase ^= 1u;
             tc_fence_after();
-            __syncthreads();
+            group_sync(g);
             if (s_fail) {
                 failed = true;
                 break;
             }
-            // epilogue: this warp's 32 rows (TMEM lanes 32 warp ..), 16 columns at a time
-            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+            // epilogue: this warp's 32 rows (TMEM lanes 32 (warp % 4) ..), 16 columns at a time
+            const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             for (uint32_t c0 = 0; c0 < ndim; c0 += 16) {
                 float v[16];
                 tmem_ld16(lane_base + c0, v);
@@ -201,31 +224,42 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
                     __align__(16) __nv_bfloat16 hv[16];
 #pragma unroll
                     for (int i = 0; i < 16; ++i) hv[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[i], 0.0f));
-                    unsigned char* dst = h_s[l & 1];
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0 + 8, kHid)) =
+                    *reinterpret_cast<int4*>(o_buf + core_offset(gt, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
+                    *reinterpret_cast<int4*>(o_buf + core_offset(gt, c0 + 8, kHid)) =
                         *reinterpret_cast<const int4*>(hv + 8);
                 } else {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[c0 + i] = v[i] + bias[i];
                 }
             }
-            if (l == kLayers - 1 && row < n) rows.output(key, y);
-            a_buf = h_s[l & 1];
+            if (l == kLayers - 1) {
+                if constexpr (Rows::kStaged) {
+                    // the last MMA has read A: stage the fp32 outputs there, row-major
+                    float* st = reinterpret_cast<float*>(buf[0]);
+#pragma unroll
+                    for (int i = 0; i < kOut; i += 4)
+                        *reinterpret_cast<float4*>(st + gt * kOut + i) = make_float4(y[i], y[i + 1], y[i + 2], y[i + 3]);
+                    group_sync(g);
+                    const uint32_t row0 = tile * kTcRows;
+                    rows.store_tile(row0, min((uint32_t)kTcRows, n - row0), st, gt, kTcGroupThreads);
+                } else if (row < n) {
+                    rows.output(key, y);
+                }
+            }
             fence_async_smem();
             tc_fence_before();
-            __syncthreads();
+            group_sync(g);
             tc_fence_after();
         }
     }
-    if (failed && tid == 0) {
+    if (failed && gt == 0) {
         // give any MMA still in flight a bounded time to finish before its TMEM is freed
         mbar_wait_bounded(bar_addr, phase);
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTmemCols));
 }
 
 

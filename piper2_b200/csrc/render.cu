@@ -963,6 +963,7 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
 // Rows of the guide's forward pass: the vertices in the guided material types' surface queues, in queue
 // order; a row's key is its path slot, whose mixture parameters the output writes.
 struct GuideRows {
+    static constexpr bool kStaged = false;  // outputs go to each vertex's path slot
     SceneView sv;
     Paths ps;
     GuideState gs;
@@ -1011,7 +1012,7 @@ struct GuideRows {
 };
 
 // The guide's mixture for every vertex of the guided material types, on the tcgen05 tensor cores.
-__global__ void __launch_bounds__(guide::kTcThreads) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
+__global__ void __launch_bounds__(guide::kTcThreads, 1) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
     extern __shared__ __align__(1024) unsigned char smem[];
     GuideRows rows{ sv, ps, gs };
     guide::forward_tc_tiles(gs.net, ps.counts[C_GUIDE], rows, ps.counts + C_TC_ERROR, smem);
@@ -1737,7 +1738,7 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             checked("k_trace_queue<extend>");
             k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_classify");
-            if (gs.enabled) k_guide_infer<<<pl->sms * 2, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
+            if (gs.enabled) k_guide_infer<<<pl->sms, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
             checked("k_guide_infer");
             // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
             const uint32_t tm = pl->type_mask;
