@@ -263,6 +263,63 @@ int pb2_accel_get_counters(const pb2_accel* accel, uint64_t* node_visits, uint64
 int pb2_trace_closest_nalloc(const float* triangles_dev, uint32_t tri_count, const pb2_ray* rays_dev, uint32_t n,
                              pb2_hit* hits_dev, void* stream);
 
+/* ---- Piper component payloads -> scene (Tracer::buildPipeline's materialize step) ----------------------
+ * A Piper tracer plugin receives each component's materialized program as a symbol name plus POD payload
+ * bytes (Tracer::buildProgram, MaterializeContext::registerCall / registerResource; Tracer.hpp:86-91,
+ * 121-133).  The builder takes exactly those, byte for byte in the reference's layouts, dispatches on the
+ * symbol, and assembles the pb2_scene and pb2_render_settings of a pipeline.  Supported symbols (the
+ * components of the render path):
+ *   sensor         "rayGen"          PCData (PerspectiveCamera/Shared.hpp:22-29)
+ *   integrator     "trace"           Data (PathTracing/Shared.hpp:22-29)
+ *   render driver  "accumulate"      RDData (FixedSampler/Shared.hpp) -> a call to "box", "triangle" or
+ *                                    "gaussian" (GaussianFilterData)
+ *   sampler        "sobolStart"      no payload (SobolData is made per frame)
+ *   light sampler  "uniformSelect"   no payload
+ *   surface        "blackBodyInit", "matteInit", "plasticInit", "glassInit", "mirrorInit", "substrateInit"
+ *                                    with MatteData / PlasticData / GlassData / MirrorData / SubstrateData
+ *                                    (Surface/Classic/Shared.hpp), their textures calls to
+ *                                    "constantTexture" (ConstantData, ProceduralTexture/Shared.hpp)
+ *   light          "SEInit"          SampledEnvironmentData (BasicLight/Shared.hpp)
+ *                  "diffuseInit"     DiffuseAreaLightData (AreaLight/Shared.hpp) -> a call to "planeSample"
+ *                                    (CDFData, BasicShapes/Shared.hpp) over a resource of PerPlaneData
+ * Any other symbol fails with PB2_ERR_NOT_SUPPORTED naming it, as the reference's pipeline build would
+ * fail on a program it cannot link.  Handles inside payloads (Call<...>, TraversalHandle) are the 64-bit
+ * values this builder returned (pb2_builder_register_call) or was given (pb2_builder_add_node). */
+typedef struct pb2_builder pb2_builder;
+enum pb2_program_kind {
+    PB2_PROGRAM_SENSOR = 0,
+    PB2_PROGRAM_INTEGRATOR = 1,
+    PB2_PROGRAM_RENDER_DRIVER = 2,
+    PB2_PROGRAM_SAMPLER = 3,
+    PB2_PROGRAM_LIGHT_SAMPLER = 4,
+    PB2_PROGRAM_SURFACE = 5,
+    PB2_PROGRAM_LIGHT = 6
+};
+int pb2_builder_create(pb2_builder** out);
+int pb2_builder_destroy(pb2_builder* builder);
+/* MaterializeContext::registerResource: a buffer later payloads name by the returned index. */
+int pb2_builder_register_resource(pb2_builder* builder, const void* data, size_t bytes, uint32_t* index);
+/* MaterializeContext::registerCall: a program and its payload; *handle is the CallHandle value that other
+ * payloads hold in their Call<...> fields. */
+int pb2_builder_register_call(pb2_builder* builder, const char* symbol, const void* payload, size_t bytes,
+                              uint64_t* handle);
+/* A scene node (Tracer::buildNode) by the TraversalHandle value payloads use for it, with its
+ * translation (the only transform the pipeline supports, see pb2_mesh). */
+int pb2_builder_add_node(pb2_builder* builder, uint64_t traversal, const float translation[3]);
+/* A component's materialized program of the given pb2_program_kind: its (first) symbol and payload.
+ * *index (may be NULL) is the material index of a surface, the light index of a light, else 0. */
+int pb2_builder_add_program(pb2_builder* builder, uint32_t kind, const char* symbol, const void* payload,
+                            size_t bytes, uint32_t* index);
+/* A triangle mesh GSM instance (Tracer::buildAcceleration + buildGSMInstance + buildNode); mesh->material is
+ * a surface index from pb2_builder_add_program.  The arrays are copied. */
+int pb2_builder_add_mesh(pb2_builder* builder, const pb2_mesh* mesh);
+/* Pipeline::prepare's inputs: the film, the fit mode and the sampler's samples per pixel.  Fills *scene
+ * and *settings (their arrays belong to the builder and live until it is destroyed); fails if a required
+ * component (sensor, integrator, render driver, sampler, light sampler, the environment as light 0) is
+ * missing. */
+int pb2_builder_build(pb2_builder* builder, uint32_t width, uint32_t height, uint32_t fit_mode,
+                      uint32_t samples_per_pixel, pb2_scene* scene, pb2_render_settings* settings);
+
 /* ---- render pipeline (Tracer::buildPipeline, Pipeline::prepare, TraceLauncher::launch;
  *      Tracer.hpp:100-119, 153-155; Embree.cpp:978-1304) --------------------------------------- */
 typedef struct pb2_pipeline pb2_pipeline;

@@ -103,14 +103,95 @@ class Accel:
         return occ
 
 
+class Builder:
+    """The materialized programs of a Piper scene (symbol names and the reference's POD payloads), turned into
+    the C ABI's scene and settings by the library (pb2_builder_*).  Host-side only: no GPU is needed."""
+
+    KIND = {"sensor": 0, "integrator": 1, "driver": 2, "sampler": 3, "light_sampler": 4, "surface": 5, "light": 6}
+
+    def __init__(self):
+        h = C.c_void_p()
+        capi.check(capi.lib().pb2_builder_create(C.byref(h)))
+        self.h = h
+        self.scene = None
+        self.settings = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().pb2_builder_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _buf(data: bytes):
+        b = C.create_string_buffer(bytes(data), max(1, len(data)))
+        return b, len(data)
+
+    def register_resource(self, data: bytes) -> int:
+        b, n = self._buf(data)
+        idx = C.c_uint32()
+        capi.check(capi.lib().pb2_builder_register_resource(self.h, b, n, C.byref(idx)))
+        return idx.value
+
+    def register_call(self, symbol: str, payload: bytes = b"") -> int:
+        b, n = self._buf(payload)
+        hd = C.c_uint64()
+        capi.check(capi.lib().pb2_builder_register_call(self.h, symbol.encode(), b, n, C.byref(hd)))
+        return hd.value
+
+    def add_node(self, traversal: int, translation):
+        capi.check(capi.lib().pb2_builder_add_node(self.h, int(traversal), capi.f3(translation)))
+
+    def add_program(self, kind, symbol: str, payload: bytes = b"") -> int:
+        b, n = self._buf(payload)
+        idx = C.c_uint32()
+        k = self.KIND[kind] if isinstance(kind, str) else int(kind)
+        capi.check(capi.lib().pb2_builder_add_program(self.h, k, symbol.encode(), b, n, C.byref(idx)))
+        return idx.value
+
+    def add_mesh(self, vertices, indices, material: int, translation=(0.0, 0.0, 0.0)):
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+        m = capi.Mesh()
+        m.vertices, m.indices, m.texcoords = v.ctypes.data, ix.ctypes.data, None
+        m.vert_count, m.tri_count, m.material = v.shape[0], ix.shape[0], int(material)
+        m.translation[:] = [float(x) for x in translation]
+        capi.check(capi.lib().pb2_builder_add_mesh(self.h, C.byref(m)))  # copied by the library
+
+    def build(self, width: int, height: int, fit_mode: int, samples_per_pixel: int):
+        """Fills and returns (capi.Scene, capi.RenderSettings); the scene's arrays live as long as the builder."""
+        sc, st = capi.Scene(), capi.RenderSettings()
+        capi.check(capi.lib().pb2_builder_build(self.h, width, height, fit_mode, samples_per_pixel, C.byref(sc),
+                                                C.byref(st)))
+        self.scene, self.settings = sc, st
+        return sc, st
+
+
 class Pipeline:
     """A render pipeline for one scene and one set of render settings."""
 
     def __init__(self, scene_data, settings=None):
+        """scene_data: a scenes.SceneData, or a Builder that has been built (then `settings` defaults to its
+        built settings)."""
         torch = _torch()
         torch.cuda.init()
-        self.settings = settings if settings is not None else scene_data.settings
-        self._sc, self._keep = scene_data.to_ctypes()
+        if isinstance(scene_data, Builder):
+            self.settings = settings if settings is not None else scene_data.settings
+            self._sc, self._keep = scene_data.scene, scene_data
+        else:
+            self.settings = settings if settings is not None else scene_data.settings
+            self._sc, self._keep = scene_data.to_ctypes()
         h = C.c_void_p()
         capi.check(capi.lib().pb2_pipeline_create(C.byref(self._sc), C.byref(self.settings), _stream(), C.byref(h)))
         self.h = h

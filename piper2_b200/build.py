@@ -20,7 +20,8 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libpiper2_b200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["bvh_build.cu", "traverse.cu", "render.cu", "capi.cu", "nalloc.cu", "guiding.cu", "guiding_tc.cu"]
+SOURCES = ["bvh_build.cu", "traverse.cu", "render.cu", "capi.cu", "nalloc.cu", "guiding.cu", "guiding_tc.cu",
+           "materialize.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
@@ -59,7 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(path), hdr_time):
             cmd = [_nvcc(), *NVCC_FLAGS, "-I", GEN, "-I", CSRC, "-c", path, "-o", obj]

@@ -172,6 +172,16 @@ SIGNATURES = [
     ("pb2_pipeline_set_guide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(GuideSettings)]),
     ("pb2_pipeline_set_wave_slots", C.c_int, [C.c_void_p, C.c_uint32]),
     ("pb2_pipeline_set_guide_dump", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("pb2_builder_create", C.c_int, [C.POINTER(C.c_void_p)]),
+    ("pb2_builder_destroy", C.c_int, [C.c_void_p]),
+    ("pb2_builder_register_resource", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]),
+    ("pb2_builder_register_call", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64)]),
+    ("pb2_builder_add_node", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("pb2_builder_add_program", C.c_int, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_void_p, C.c_size_t,
+                                          C.POINTER(C.c_uint32)]),
+    ("pb2_builder_add_mesh", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pb2_builder_build", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.c_void_p]),
     ("pb2_pipeline_train_guide", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float),
                                             C.c_void_p]),
 ]
