@@ -335,11 +335,12 @@ int pb2_pipeline_get_rect(const pb2_pipeline* pipeline, pb2_rect* full_rect, pb2
  * per (pixel, sample) the film point and radiance, 5 floats each, in (y, x, sample) order. */
 int pb2_pipeline_launch(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample_begin,
                         uint32_t sample_count, float* rgbw_dev, float* sample_out_dev, void* stream);
-/* Bounds the path slots of a single-scene launch (default 2^22, in [256, 2^30]).  A launch of more paths
- * (rect pixels x sample_count) runs in waves of `slots` paths, one after another on the launch's stream,
- * so its path state (about 250 bytes per slot, plus about 400 with a guide attached) stays bounded; the
- * samples and the film are those of one launch.  Shrinking the bound frees the larger path state. */
-int pb2_pipeline_set_wave_slots(pb2_pipeline* pipeline, uint32_t slots);
+/* Bounds the path slots of a single-scene launch (default 2^24, in [256, 2^30]).  A launch keeps at most
+ * `slots` paths (rect pixels x sample_count) in flight: every bounce first refills the slots that finished
+ * paths freed with the launch's next paths, so the wavefront stays full until they run out, and the path
+ * state (about 260 bytes per slot, plus about 400 with a guide attached) stays bounded.  The samples and
+ * the film are those of the same launch without the bound.  Shrinking the bound frees the larger state. */
+int pb2_pipeline_set_path_slots(pb2_pipeline* pipeline, uint32_t slots);
 /* Resolve radiance = rgb / w (FixedSampler.cpp:122-131) into rgb_dev (width * height * 3). */
 int pb2_film_resolve(const float* rgbw_dev, uint32_t pixel_count, float* rgb_dev, void* stream);
 int pb2_pipeline_get_stats(const pb2_pipeline* pipeline, pb2_launch_stats* stats, void* stream);

@@ -243,9 +243,9 @@ class Pipeline:
         torch.cuda.synchronize()
         return film.cpu().numpy(), (out.cpu().numpy() if out is not None else None)
 
-    def set_wave_slots(self, slots: int):
-        """Bound the path slots in flight; larger launches run in waves of `slots` paths."""
-        capi.check(capi.lib().pb2_pipeline_set_wave_slots(self.h, int(slots)))
+    def set_path_slots(self, slots: int):
+        """Bound the path slots in flight; a larger launch refills freed slots with its remaining paths."""
+        capi.check(capi.lib().pb2_pipeline_set_path_slots(self.h, int(slots)))
 
     def resolve(self, film):
         torch = _torch()

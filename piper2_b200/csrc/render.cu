@@ -177,8 +177,8 @@ struct LaunchParams {
     pb2_camera cam;
     uint32_t num_lights;  // area lights
     float env[3];
-    uint32_t path_count;  // paths of this wave (at most the pipeline's slot capacity)
-    uint32_t path_base;   // launch-relative index of the wave's first path
+    uint32_t path_count;  // path slots of a single-scene launch (its capacity)
+    uint32_t refill;      // 1: the launch has more paths than slots, finished paths free their slots
     uint32_t checks;      // PB2_DEBUG_CHECKS: verify indices, record the first violation, skip the path
     uint32_t scramble, scramble_seed;  // Owen scrambling of dimensions >= 2 (extension)
 };
@@ -378,28 +378,6 @@ __global__ void k_camera_rays(LaunchParams lp, uint32_t sample, float4* __restri
     points[i] = make_float2(px, py);
 }
 
-// Starts path lp.path_base + p of the launch in slot p.
-__global__ void k_generate(LaunchParams lp, Paths ps, GuideState gs) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= lp.path_count) return;
-    uint32_t sx, sy, s;
-    path_coords(lp, lp.path_base + p, sx, sy, s);
-    uint64_t index;
-    float px, py;
-    v3 o, d;
-    primary_ray(lp, sx, sy, s, index, px, py, o, d);
-    ps.o[p] = make_float4(o.x, o.y, o.z, 0.0f);
-    ps.d[p] = make_float4(d.x, d.y, d.z, 0.0f);
-    ps.pf[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-    ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ps.sidx[p] = index;
-    ps.dim[p] = 5;
-    ps.depth[p] = 0;
-    ps.point[p] = make_float2(px, py);
-    ps.ext[0][p] = p;
-    if (gs.enabled) gs.nrec[p] = 0;
-}
-
 // ---- traversal over queues -----------------------------------------------------------------------
 
 constexpr int kQThreads = 128;
@@ -556,10 +534,11 @@ __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, 
         ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
         if (atomicSub(&ctx.remaining[scene], 1u) == 1u) ctx.done_ns[scene] = globaltimer();
     } else {
-        if (ctx.sample_out) {
-            float* o = ctx.sample_out + 5 * ((size_t)ctx.lp.path_base + slot);
+        if (ctx.sample_out) {  // at the path's launch-relative index (a slot serves many paths)
+            float* o = ctx.sample_out + 5 * (size_t)ps.scene[slot];
             o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
         }
+        if (ctx.lp.refill) ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
     }
 }
 
@@ -1218,6 +1197,34 @@ __global__ void k_batch_regen(const __grid_constant__ BatchCtx ctx, Paths ps, ui
     }
 }
 
+// Starts the paths claimed for iteration `cur` of a single-scene launch in the slots freed by the previous
+// iteration: path g of the launch (p = ((row * rect.width) + col) * sample_count + k) in slot free_q[cur][i],
+// appended to the current extend queue.  ps.scene[slot] keeps the path's index for its per-sample output.
+__global__ void k_single_regen(LaunchParams lp, Paths ps, GuideState gs, const BatchState* st, uint32_t cur) {
+    const uint32_t m = st->claim_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = ps.free_q[cur][i];
+        const uint32_t g = (uint32_t)(st->claim_begin + i);
+        uint32_t sx, sy, smp;
+        path_coords(lp, g, sx, sy, smp);
+        uint64_t index;
+        float px, py;
+        v3 o, d;
+        primary_ray(lp, sx, sy, smp, index, px, py, o, d);
+        ps.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+        ps.d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        ps.pf[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        ps.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.sidx[slot] = index;
+        ps.dim[slot] = 5;
+        ps.depth[slot] = 0;
+        ps.point[slot] = make_float2(px, py);
+        ps.scene[slot] = g;
+        if (gs.enabled) gs.nrec[slot] = 0;
+        ps.ext[cur][st->claim_base + i] = slot;
+    }
+}
+
 // Per-bounce bookkeeping: next extend queue becomes current; clear per-bounce counters.
 __global__ void k_advance(uint32_t* counts) {
     counts[C_EXT_CUR] = counts[C_EXT_NEXT];
@@ -1251,9 +1258,11 @@ using namespace pb2;
 
 const char* pb2_sobol_table_sha256() { return PB2_SOBOL_TABLE_SHA256; }
 
-// Path slots of a single-scene wavefront unless set otherwise (pb2_pipeline_set_wave_slots): 4M slots hold
-// about 1 GB of path state (and 1.6 GB more when a guide is attached).
-constexpr uint32_t kDefaultWaveSlots = 1u << 22;
+// Path slots of a single-scene wavefront unless set otherwise (pb2_pipeline_set_path_slots): 16M slots hold
+// about 4.4 GB of path state (and 6.7 GB more when a guide is attached).  Refilled slots serve paths in no
+// particular order, which scatters the path state a warp touches, so the bound is set high enough that
+// common launches (a 1920 x 1080 frame at 8 spp is 16.6M paths) start all or nearly all paths at once.
+constexpr uint32_t kDefaultPathSlots = 1u << 24;
 
 struct pb2_pipeline {
     pb2_accel* accel = nullptr;
@@ -1270,8 +1279,9 @@ struct pb2_pipeline {
     uint32_t type_mask = 0;  // surface types of the scene's materials: the shading kernels launched per bounce
     float env[3] = { 0, 0, 0 };
     float gauss_sub = 0.0f;
-    // path state: at most `wave_slots` paths are in flight; a launch with more runs in waves of that many
-    uint32_t wave_slots = kDefaultWaveSlots;
+    // path state: at most `path_slots` paths are in flight; a launch with more refills freed slots
+    uint32_t path_slots = kDefaultPathSlots;
+    BatchState* refill = nullptr;  // claim state of the slot refill (device memory)
     uint32_t capacity = 0;
     void* state = nullptr;
     Paths ps{};
@@ -1373,7 +1383,8 @@ static int alloc_path_state(void** mem, uint32_t* capacity, Paths* ps, uint32_t 
 }
 
 static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
-    return alloc_path_state(&pl->state, &pl->capacity, &pl->ps, cap, false);
+    // with the refill arrays (per-slot path index, freed-slot queues)
+    return alloc_path_state(&pl->state, &pl->capacity, &pl->ps, cap, true);
 }
 
 static float remap_roughness(float roughness) {
@@ -1556,6 +1567,7 @@ int pb2_pipeline_destroy(pb2_pipeline* pl) {
     cudaFree(pl->plane_cdf);
     cudaFree(pl->plane_pdf);
     cudaFree(pl->state);
+    cudaFree(pl->refill);
     cudaFree(pl->guide_state);
     cudaFree(pl->g_train);
     cudaFree(pl->g_batch);
@@ -1628,10 +1640,14 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     const uint64_t paths = (uint64_t)rect->width * rect->height * sample_count;
     if (paths > 0x7FFFFFFFull) return fail(PB2_ERR_INVALID_ARGUMENT, "launch has more than 2^31 paths");
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    // path slots in flight: the whole launch, or waves of pl->wave_slots paths
-    const uint32_t slots = (uint32_t)std::min<uint64_t>(paths, pl->wave_slots);
+    // path slots in flight: the whole launch, or at most pl->path_slots (then refilled as paths finish)
+    const uint32_t slots = (uint32_t)std::min<uint64_t>(paths, pl->path_slots);
     int rc = alloc_paths(pl, slots);
     if (rc) return rc;
+    if (!pl->refill) {
+        const cudaError_t ea = cudaMalloc(&pl->refill, sizeof(BatchState));
+        if (ea != cudaSuccess) return cuda_fail(ea, "cudaMalloc refill state");
+    }
     LaunchParams lp = make_params(pl, *rect, sample_begin, sample_count);
     GuideState gs{};
     if (pl->guide) {
@@ -1674,145 +1690,154 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     Paths ps = pl->ps;
     float4* film = reinterpret_cast<float4*>(rgbw);
     cudaError_t e;
-    // one wave per `slots` paths: each starts its paths in slots 0.., runs its bounces until every path is
-    // splatted, and adds its counters to the pipeline's statistics
-    for (uint64_t base = 0; base < paths; base += slots) {
-        lp.path_base = (uint32_t)base;
-        lp.path_count = (uint32_t)std::min<uint64_t>(slots, paths - base);
-        if ((e = cudaMemsetAsync(ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream))) return cuda_fail(e, "memset counts");
-        const uint32_t pc = lp.path_count;
-        if ((e = cudaMemcpyAsync(ps.counts + C_EXT_CUR, &pc, sizeof(uint32_t), cudaMemcpyHostToDevice, stream)))
-            return cuda_fail(e, "set count");
-        k_generate<<<(pc + 255) / 256, 256, 0, stream>>>(lp, ps, gs);
-        const int grid = pl->sms * 8;
-        uint32_t* work = pl->accel->work;
-        unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
-        unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
-        static std::atomic<int> qcache[kMaxDevices], qcache_any[kMaxDevices];
-        const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
-        const int qblocks_any =
-            resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
-        uint32_t cur = 0;
-        const int max_bounces = 4 * ((int)pl->settings.max_depth + 2) + 64;
-        // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed
-        static const bool debug_sync = [] {
-            const char* v = std::getenv("PB2_DEBUG_SYNC");
-            return v && v[0] == '1';
-        }();
-        const char* failed = nullptr;
-        auto checked = [&](const char* name) {
-            if (!debug_sync || failed) return;
-            cudaError_t err = cudaGetLastError();
-            if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
-            if (err != cudaSuccess) {
-                failed = name;
-                e = err;
-            }
-        };
-        checked("k_generate");
-        SingleCtx ctx;
-        ctx.lp = lp;
-        ctx.sv = sv;
-        ctx.film = film;
-        ctx.sample_out = sample_out;
-        // The bounce kernels read their queue sizes on the device, so the host checks for completion only
-        // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
-        // the bounces between checks queue up without a host round trip.
-        constexpr int kCheckEvery = 4;
-        uint32_t active = paths > 0 ? 1u : 0u;
-        for (int bounce = 0; !failed; ++bounce) {
-            if (bounce % kCheckEvery == 0) {
-                if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                         stream)) ||
-                    (e = cudaStreamSynchronize(stream)))
-                    return cuda_fail(e, "read queue size");
-                if (active == 0) break;
-            }
-            if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
-            // grid from the last known queue size (an upper bound: queues only shrink); the persistent trace
-            // blocks stop when the queue is drained
-            const int qgrid = std::min<int>(qblocks, (int)((active + kQThreads - 1) / kQThreads));
-            cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
-            k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
-                                                                     stats);
-            checked("k_trace_queue<extend>");
-            k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_classify");
-            if (gs.enabled) k_guide_infer<<<pl->sms, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
-            checked("k_guide_infer");
-            // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
-            const uint32_t tm = pl->type_mask;
-            if (tm & (1u << PB2_SURFACE_MATTE)) {
-                if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<matte>");
-            }
-            if (tm & (1u << PB2_SURFACE_PLASTIC)) {
-                k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<plastic>");
-            }
-            if (tm & (1u << PB2_SURFACE_GLASS)) {
-                k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<glass>");
-            }
-            if (tm & (1u << PB2_SURFACE_MIRROR)) {
-                k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<mirror>");
-            }
-            if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
-                k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<substrate>");
-            }
-            if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
-                if (gs.enabled)
-                    k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<conductor>");
-            }
-            if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
-                k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-                checked("k_shade<blackbody>");
-            }
-            k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
-                                                                           work + 1, sstats);
-            checked("k_trace_queue<shadow>");
-            k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
-                                                                        stats);
-            checked("k_trace_queue<mis>");
-            k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_finish");
-            k_advance<<<1, 1, 0, stream>>>(ps.counts);
-            checked("k_advance");
-            if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
-            cur ^= 1u;
+    // every slot starts free; each bounce first refills the slots freed by the previous one from the launch's
+    // remaining paths (k_batch_claim + k_single_regen), so the wavefront stays full until the paths run out
+    lp.path_count = slots;
+    lp.refill = slots < paths ? 1u : 0u;
+    if ((e = cudaMemsetAsync(ps.counts, 0, sizeof(uint32_t) * C_COUNT, stream))) return cuda_fail(e, "memset counts");
+    k_batch_init<<<(slots + 255) / 256, 256, 0, stream>>>(ps, slots, pl->refill, paths);
+    const int grid = pl->sms * 8;
+    uint32_t* work = pl->accel->work;
+    unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
+    unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
+    static std::atomic<int> qcache[kMaxDevices], qcache_any[kMaxDevices];
+    const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
+    const int qblocks_any =
+        resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
+    uint32_t cur = 0;
+    // generous bound: every path needs at most (max depth + light pass-throughs) bounces, and a slot serves
+    // about paths / slots of them one after another
+    const uint64_t max_bounces = (paths / slots + 2) * (4ull * (pl->settings.max_depth + 2) + 64);
+    // PB2_DEBUG_SYNC=1: synchronise after every kernel and name the one that failed
+    static const bool debug_sync = [] {
+        const char* v = std::getenv("PB2_DEBUG_SYNC");
+        return v && v[0] == '1';
+    }();
+    const char* failed = nullptr;
+    auto checked = [&](const char* name) {
+        if (!debug_sync || failed) return;
+        cudaError_t err = cudaGetLastError();
+        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) {
+            failed = name;
+            e = err;
         }
-        if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
-        uint32_t counts[C_COUNT];
-        if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
-            (e = cudaStreamSynchronize(stream)))
-            return cuda_fail(e, "read stats");
-        unsigned long long v;
-        std::memcpy(&v, counts + C_STAT_CLOSEST, 8);
-        pl->stats.closest_rays += v;
-        std::memcpy(&v, counts + C_STAT_SHADOW, 8);
-        pl->stats.shadow_rays += v;
-        std::memcpy(&v, counts + C_STAT_VERTICES, 8);
-        pl->stats.path_vertices += v;
-        pl->stats.paths += pc;
-        if (counts[C_CHECK])
-            return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
-                                          std::to_string(counts[C_CHECK + 1]) + " at slot " +
-                                          std::to_string(counts[C_CHECK + 2]) + ", value " +
-                                          std::to_string(counts[C_CHECK + 3]));
-        if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
-        if (counts[C_TC_ERROR]) return fail(PB2_ERR_DEVICE_TIMEOUT, "guide inference: a tensor-core wait timed out");
-        if (gs.enabled) {
-            uint32_t tc[2];
-            if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+    };
+    checked("k_batch_init");
+    SingleCtx ctx;
+    ctx.lp = lp;
+    ctx.sv = sv;
+    ctx.film = film;
+    ctx.sample_out = sample_out;
+    // The bounce kernels read their queue sizes on the device, so the host checks for completion only
+    // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
+    // the bounces between checks queue up without a host round trip.
+    constexpr int kCheckEvery = 4;
+    bool refilling = true;
+    for (uint64_t bounce = 0; !failed; ++bounce) {
+        if (bounce % kCheckEvery == 0 && bounce > 0) {
+            uint32_t active = 0;
+            unsigned long long next = paths;  // once every path has started, only the queue is read
+            if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     stream)) ||
+                (refilling &&
+                 (e = cudaMemcpyAsync(&next, &pl->refill->next, sizeof(next), cudaMemcpyDeviceToHost, stream))) ||
                 (e = cudaStreamSynchronize(stream)))
-                return cuda_fail(e, "read record count");
-            pl->g_offered = tc[1];
+                return cuda_fail(e, "read queue size");
+            if (active == 0 && next == paths) break;
+            if (next == paths) refilling = false;  // every path has been started
         }
+        if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
+        if (refilling) {
+            k_batch_claim<<<1, 1, 0, stream>>>(ps, pl->refill, cur, work);  // also clears the trace work counters
+            k_single_regen<<<grid, 256, 0, stream>>>(lp, ps, gs, pl->refill, cur);
+            checked("k_single_regen");
+            // all paths fit the slots: the first claim started every one of them
+            if (slots == paths) refilling = false;
+        } else {
+            cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
+        }
+        // the persistent trace blocks stop when the queue is drained
+        const int qgrid = qblocks;
+        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
+                                                                 stats);
+        checked("k_trace_queue<extend>");
+        k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+        checked("k_classify");
+        if (gs.enabled) k_guide_infer<<<pl->sms, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
+        checked("k_guide_infer");
+        // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
+        const uint32_t tm = pl->type_mask;
+        if (tm & (1u << PB2_SURFACE_MATTE)) {
+            if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<matte>");
+        }
+        if (tm & (1u << PB2_SURFACE_PLASTIC)) {
+            k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<plastic>");
+        }
+        if (tm & (1u << PB2_SURFACE_GLASS)) {
+            k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<glass>");
+        }
+        if (tm & (1u << PB2_SURFACE_MIRROR)) {
+            k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<mirror>");
+        }
+        if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
+            k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<substrate>");
+        }
+        if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
+            if (gs.enabled)
+                k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<conductor>");
+        }
+        if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
+            k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            checked("k_shade<blackbody>");
+        }
+        k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
+                                                                       work + 1, sstats);
+        checked("k_trace_queue<shadow>");
+        k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
+                                                                    stats);
+        checked("k_trace_queue<mis>");
+        k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
+        checked("k_finish");
+        k_advance<<<1, 1, 0, stream>>>(ps.counts);
+        checked("k_advance");
+        if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
+        cur ^= 1u;
+    }
+    if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
+    uint32_t counts[C_COUNT];
+    if ((e = cudaMemcpyAsync(counts, ps.counts, sizeof(counts), cudaMemcpyDeviceToHost, stream)) ||
+        (e = cudaStreamSynchronize(stream)))
+        return cuda_fail(e, "read stats");
+    unsigned long long v;
+    std::memcpy(&v, counts + C_STAT_CLOSEST, 8);
+    pl->stats.closest_rays += v;
+    std::memcpy(&v, counts + C_STAT_SHADOW, 8);
+    pl->stats.shadow_rays += v;
+    std::memcpy(&v, counts + C_STAT_VERTICES, 8);
+    pl->stats.path_vertices += v;
+    pl->stats.paths += paths;
+    if (counts[C_CHECK])
+        return fail(PB2_ERR_CUDA, "index check " + std::to_string(counts[C_CHECK]) + " failed in kernel " +
+                                      std::to_string(counts[C_CHECK + 1]) + " at slot " +
+                                      std::to_string(counts[C_CHECK + 2]) + ", value " +
+                                      std::to_string(counts[C_CHECK + 3]));
+    if (counts[C_ERROR]) return fail(PB2_ERR_QUEUE_OVERFLOW, "traversal stack overflow");
+    if (counts[C_TC_ERROR]) return fail(PB2_ERR_DEVICE_TIMEOUT, "guide inference: a tensor-core wait timed out");
+    if (gs.enabled) {
+        uint32_t tc[2];
+        if ((e = cudaMemcpyAsync(tc, pl->g_count, sizeof(tc), cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaStreamSynchronize(stream)))
+            return cuda_fail(e, "read record count");
+        pl->g_offered = tc[1];
     }
     return PB2_OK;
 }
@@ -1827,10 +1852,10 @@ int pb2_pipeline_set_guide_dump(pb2_pipeline* pl, float* rows_dev, uint32_t capa
     return PB2_OK;
 }
 
-int pb2_pipeline_set_wave_slots(pb2_pipeline* pl, uint32_t slots) {
-    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_wave_slots: null pipeline");
-    if (slots < 256 || slots > (1u << 30)) return fail(PB2_ERR_INVALID_ARGUMENT, "wave slots must lie in [256, 2^30]");
-    pl->wave_slots = slots;
+int pb2_pipeline_set_path_slots(pb2_pipeline* pl, uint32_t slots) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_path_slots: null pipeline");
+    if (slots < 256 || slots > (1u << 30)) return fail(PB2_ERR_INVALID_ARGUMENT, "path slots must lie in [256, 2^30]");
+    pl->path_slots = slots;
     if (pl->capacity > slots) {  // give back path state above the new bound
         cudaFree(pl->state);
         pl->state = nullptr;

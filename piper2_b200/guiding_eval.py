@@ -56,10 +56,15 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train
             for s in range(0, ref_spp, chunk):
                 pl.launch(film, sample_begin=spp + s, sample_count=min(chunk, ref_spp - s))
             ref = pl.resolve(film).cpu().numpy().astype(np.float64)
-        # plain: one launch of all samples (its fastest form), after a warm-up launch
+        # plain: its fastest form, one launch of all samples or passes of spp_per_pass samples (timed after a
+        # warm-up launch); both render the same samples
         pl.launch(pl.new_film(), sample_begin=0, sample_count=min(spp, 4))
         film = pl.new_film()
-        t_plain, _ = _time(torch, lambda: pl.launch(film, sample_begin=0, sample_count=spp))
+        t_one, _ = _time(torch, lambda: pl.launch(film, sample_begin=0, sample_count=spp))
+        film_p = pl.new_film()
+        t_passes, _ = _time(torch, lambda: [pl.launch(film_p, sample_begin=b, sample_count=min(spp_per_pass, spp - b))
+                                           for b in range(0, spp, spp_per_pass)])
+        t_plain = min(t_one, t_passes)
         plain = pl.resolve(film).cpu().numpy().astype(np.float64)
         # guided: a fresh network per run, progressive passes with online training.  Online training is not
         # deterministic (records are gathered with atomics), so `repeats` independent runs are made and
@@ -80,7 +85,8 @@ def evaluate(width=1280, height=720, spp=64, ref_spp=1024, spp_per_pass=8, train
     e_plain = rel_mse(plain, ref) if ref is not None else None
     e_guided = float(np.mean([rel_mse(r[1], ref) for r in runs])) if ref is not None else None
     out.update({
-        "plain": {"ms": round(t_plain, 2), "relmse": e_plain, "mean": float(plain.mean())},
+        "plain": {"ms": round(t_plain, 2), "ms_one_launch": round(t_one, 2), "ms_passes": round(t_passes, 2),
+                  "relmse": e_plain, "mean": float(plain.mean())},
         "guided": {"ms": round(t_guided, 2), "relmse": e_guided, "mean": float(guided.mean()),
                    "guided_types": guided_types or "matte", "max_guided_depth": max_guided_depth or None,
                    "passes": spp // spp_per_pass, "train_steps_per_pass": train_steps, "batch": batch,

@@ -243,10 +243,10 @@ def test_several_lights_and_environment_bitexact(oracle):
 
 
 @pytest.mark.parametrize("slots", [256, 1000])
-def test_launch_in_waves_bitexact(oracle, slots):
-    """A launch with more paths than the pipeline's slot bound runs in waves: every sample (written at its
-    launch-relative place) and the film are those of the oracle, for a sub-rect and a sample range that does
-    not start at 0; a guided render in waves works too."""
+def test_launch_with_slot_refill_bitexact(oracle, slots):
+    """A launch with more paths than the pipeline's slot bound refills freed slots with its remaining paths:
+    every sample (written at its launch-relative place) and the film are those of the oracle, for a sub-rect
+    and a sample range that does not start at 0."""
     import torch
 
     from piper2_b200 import capi
@@ -254,7 +254,7 @@ def test_launch_in_waves_bitexact(oracle, slots):
     sd = scenes.cornell_box(seed=2, width=40, height=24, spp=8)
     rect = capi.Rect(4, 2, 30, 20)
     with _api().Pipeline(sd) as pl:
-        pl.set_wave_slots(slots)
+        pl.set_path_slots(slots)
         film = pl.new_film()
         out = torch.zeros((rect.height, rect.width, 5, 5), dtype=torch.float32, device="cuda")
         pl.launch(film, rect, sample_begin=3, sample_count=5, sample_out=out)
@@ -269,10 +269,10 @@ def test_launch_in_waves_bitexact(oracle, slots):
     assert st.paths == rect.width * rect.height * 5
 
 
-def test_wave_slots_rejects_out_of_range():
+def test_path_slots_rejects_out_of_range():
     from piper2_b200 import capi
 
     sd = scenes.cornell_box(seed=0, width=8, height=8)
     with _api().Pipeline(sd) as pl:
-        with pytest.raises(capi.PB2Error, match="wave slots"):
-            pl.set_wave_slots(100)
+        with pytest.raises(capi.PB2Error, match="path slots"):
+            pl.set_path_slots(100)
