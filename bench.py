@@ -360,6 +360,31 @@ def _render_rate(pl, rect, spp, chunk, frames=1):
             "ms_per_frame": round(ms / frames, 3), "rays_per_sample": round(rays / samples, 3)}
 
 
+def render_roofline(pl, rect, spp, chunk, ms_per_frame):
+    """Byte model of the render path for one frame, by the counting build of its traversal queries (a separate
+    untimed render of the same samples): per traced ray its 32-byte ray, the record it writes (closest hit
+    16 B + triangle slot 4 B, MIS record 16 B, occlusion flag 4 B), 80 B per 8-wide node visited and 36 B per
+    triangle tested, plus 48 B of queued path state written and read again per ray, plus 16 B x 4 film splats
+    per sample; over the timed frame, against the measured HBM copy peak."""
+    pl.set_counting(True)
+    film = pl.new_film()
+    for b in range(0, spp, chunk):
+        pl.launch(film, rect, b, min(chunk, spp - b))
+    c = pl.trace_counters()
+    pl.set_counting(False)
+    record = {"extend": 20, "mis": 16, "shadow": 4}
+    traversal = sum(r * (32 + record[k]) + 80 * v + 36 * t for k, (r, v, t) in c.items())
+    rays = sum(r for r, _, _ in c.values())
+    samples = rect.width * rect.height * spp
+    total = traversal + 96 * rays + 64 * samples
+    achieved = total / (ms_per_frame * 1e-3) / 1e9
+    peak, kind = _peaks()
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": kind, "bytes_per_frame": int(total),
+            "per_query": {k: {"rays": r, "node_visits_per_ray": round(v / max(r, 1), 3),
+                              "triangle_tests_per_ray": round(t / max(r, 1), 3)} for k, (r, v, t) in c.items()}}
+
+
 def batch_bench():
     """64 scenes of uneven size (10k-2M triangles, 128-1024 px film side, 4-64 spp) through one batched
     render: autotuned configuration, aggregate samples/s, per-scene completion percentiles; beside it the
@@ -424,6 +449,7 @@ def render_bench(args):
     with api.Pipeline(sd) as pl:
         out = {"workload": "Cornell box 256x256, 16 spp, max depth 8, NEE+MIS (plain BxDF sampling)"}
         out.update(_render_rate(pl, pl.rect, st.samples_per_pixel, st.samples_per_pixel, frames=max(3, args.steps // 2)))
+        out["roofline"] = render_roofline(pl, pl.rect, st.samples_per_pixel, st.samples_per_pixel, out["ms_per_frame"])
         film = pl.new_film()
         pl.launch(film, sample_begin=0, sample_count=st.samples_per_pixel)
         out["relmse_vs_fp64_4096spp"] = truth_rel_mse(pl.resolve(film).cpu().numpy(), "cornell_256x256")
@@ -444,6 +470,7 @@ def render_bench(args):
         mm = {"workload": "mixed materials 1920x1080, 64 spp, max depth 16, 3.1M triangles (terrain + 200 "
                           "icospheres: Lambert / smooth dielectric / GGX conductor), env 0.5 + sun"}
         mm.update(_render_rate(pl, pl.rect, md.settings.samples_per_pixel, 8))
+        mm["roofline"] = render_roofline(pl, pl.rect, md.settings.samples_per_pixel, 8, mm["ms_per_frame"])
         film = pl.new_film()
         for b in range(0, md.settings.samples_per_pixel, 8):
             pl.launch(film, sample_begin=b, sample_count=8)

@@ -335,6 +335,12 @@ int pb2_pipeline_get_rect(const pb2_pipeline* pipeline, pb2_rect* full_rect, pb2
  * per (pixel, sample) the film point and radiance, 5 floats each, in (y, x, sample) order. */
 int pb2_pipeline_launch(pb2_pipeline* pipeline, const pb2_rect* rect, uint32_t sample_begin,
                         uint32_t sample_count, float* rgbw_dev, float* sample_out_dev, void* stream);
+/* Counting build of the render's traversal (for the render path's byte model; slower, off by default):
+ * while on, the closest-hit, MIS and shadow queries of every launch add their rays, node visits and triangle
+ * tests to nine counters (extend rays/visits/tests, MIS ..., shadow ...), cleared when counting is switched
+ * on; pb2_pipeline_get_trace_counters reads them (synchronising `stream`). */
+int pb2_pipeline_set_counting(pb2_pipeline* pipeline, int enable);
+int pb2_pipeline_get_trace_counters(const pb2_pipeline* pipeline, uint64_t* counters9_host, void* stream);
 /* Bounds the path slots of a single-scene launch (default 2^24, in [256, 2^30]).  A launch keeps at most
  * `slots` paths (rect pixels x sample_count) in flight: every bounce first refills the slots that finished
  * paths freed with the launch's next paths, so the wavefront stays full until they run out, and the path

@@ -243,6 +243,16 @@ class Pipeline:
         torch.cuda.synchronize()
         return film.cpu().numpy(), (out.cpu().numpy() if out is not None else None)
 
+    def set_counting(self, enable: bool):
+        """Counting build of the render's traversal queries (rays, node visits, triangle tests per query kind)."""
+        capi.check(capi.lib().pb2_pipeline_set_counting(self.h, 1 if enable else 0))
+
+    def trace_counters(self) -> dict:
+        """Since counting was switched on: {"extend"|"mis"|"shadow": (rays, node visits, triangle tests)}."""
+        c = np.zeros(9, dtype=np.uint64)
+        capi.check(capi.lib().pb2_pipeline_get_trace_counters(self.h, c.ctypes.data_as(C.c_void_p), _stream()))
+        return {k: tuple(int(x) for x in c[3 * i:3 * i + 3]) for i, k in enumerate(("extend", "mis", "shadow"))}
+
     def set_path_slots(self, slots: int):
         """Bound the path slots in flight; a larger launch refills freed slots with its remaining paths."""
         capi.check(capi.lib().pb2_pipeline_set_path_slots(self.h, int(slots)))

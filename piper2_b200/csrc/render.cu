@@ -397,15 +397,19 @@ enum QueueTraceKind : int { Q_EXTEND, Q_MIS, Q_SHADOW };
 // or the occluding triangle.  k_finish's result is that of the closest-hit query.
 // Resident blocks per SM the register budget is sized for: 10 for closest hit, 9 for the any-hit queries
 // (as the API kernels; at 10 the any-hit queries spilled about 90 bytes).
-template <int kKind, class Ctx>
+// kCount: the counting build (pipelines with counting on): adds the rays, node visits and triangle tests of
+// the queue to trace_counters[3 kKind .. 3 kKind + 2] for the byte model of the render roofline.
+template <int kKind, class Ctx, bool kCount = false>
 __global__ void __launch_bounds__(kQThreads, kKind == Q_EXTEND ? 10 : 9) k_trace_queue(const __grid_constant__ Ctx ctx, Paths ps,
                                                            const uint32_t* __restrict__ queue,
                                                            const uint32_t* __restrict__ count_ptr, uint32_t* work,
-                                                           unsigned long long* stat) {
+                                                           unsigned long long* stat,
+                                                           unsigned long long* trace_counters = nullptr) {
     constexpr bool kClosest = kKind == Q_EXTEND;
     const uint32_t n = *count_ptr;
     __shared__ uint2 stack_smem[kSharedStack * kQThreads];
-    Traverser<kClosest, false, kQThreads> tr;
+    Traverser<kClosest, kCount, kQThreads> tr;
+    uint32_t nv = 0, nt = 0;
     tr.bind_stack(stack_smem);
     bool active = false;
     uint32_t slot = 0;
@@ -484,12 +488,27 @@ __global__ void __launch_bounds__(kQThreads, kKind == Q_EXTEND ? 10 : 9) k_trace
                     ps.occ[slot] = tr.best_prim != kInvalidPrim ? 1u : 0u;
                 }
                 if (tr.overflow) atomicOr(&ps.counts[C_ERROR], 1u);
+                if constexpr (kCount) {
+                    nv += tr.node_visits;
+                    nt += tr.tri_tests;
+                }
                 active = false;
             }
         }
     }
     for (int o = 16; o > 0; o >>= 1) rays += __shfl_xor_sync(0xFFFFFFFFu, rays, o);
     if (lane == 0 && rays) atomicAdd(stat, (unsigned long long)rays);
+    if constexpr (kCount) {
+        for (int o = 16; o > 0; o >>= 1) {
+            nv += __shfl_xor_sync(0xFFFFFFFFu, nv, o);
+            nt += __shfl_xor_sync(0xFFFFFFFFu, nt, o);
+        }
+        if (lane == 0) {
+            atomicAdd(trace_counters + 3 * kKind + 0, (unsigned long long)rays);
+            atomicAdd(trace_counters + 3 * kKind + 1, (unsigned long long)nv);
+            atomicAdd(trace_counters + 3 * kKind + 2, (unsigned long long)nt);
+        }
+    }
 }
 
 // ---- film -------------------------------------------------------------------------------------------
@@ -1282,6 +1301,7 @@ struct pb2_pipeline {
     // path state: at most `path_slots` paths are in flight; a launch with more refills freed slots
     uint32_t path_slots = kDefaultPathSlots;
     BatchState* refill = nullptr;  // claim state of the slot refill (device memory)
+    unsigned long long* trace_counters = nullptr;  // counting on (pb2_pipeline_set_counting): 9 counters
     uint32_t capacity = 0;
     void* state = nullptr;
     Paths ps{};
@@ -1568,6 +1588,7 @@ int pb2_pipeline_destroy(pb2_pipeline* pl) {
     cudaFree(pl->plane_pdf);
     cudaFree(pl->state);
     cudaFree(pl->refill);
+    cudaFree(pl->trace_counters);
     cudaFree(pl->guide_state);
     cudaFree(pl->g_train);
     cudaFree(pl->g_batch);
@@ -1759,8 +1780,12 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         }
         // the persistent trace blocks stop when the queue is drained
         const int qgrid = qblocks;
-        k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
-                                                                 stats);
+        if (pl->trace_counters)
+            k_trace_queue<Q_EXTEND, SingleCtx, true><<<qgrid, kQThreads, 0, stream>>>(
+                ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work, stats, pl->trace_counters);
+        else
+            k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
+                                                                     stats);
         checked("k_trace_queue<extend>");
         k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_classify");
@@ -1799,11 +1824,19 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<blackbody>");
         }
-        k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
-                                                                       work + 1, sstats);
+        if (pl->trace_counters)
+            k_trace_queue<Q_SHADOW, SingleCtx, true><<<qblocks_any, kQThreads, 0, stream>>>(
+                ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1, sstats, pl->trace_counters);
+        else
+            k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
+                                                                           work + 1, sstats);
         checked("k_trace_queue<shadow>");
-        k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
-                                                                    stats);
+        if (pl->trace_counters)
+            k_trace_queue<Q_MIS, SingleCtx, true><<<qblocks_any, kQThreads, 0, stream>>>(
+                ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats, pl->trace_counters);
+        else
+            k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
+                                                                        stats);
         checked("k_trace_queue<mis>");
         k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_finish");
@@ -1849,6 +1882,32 @@ int pb2_pipeline_set_guide_dump(pb2_pipeline* pl, float* rows_dev, uint32_t capa
     pl->g_dump = rows_dev;
     pl->g_dump_count = rows_dev ? count_dev : nullptr;
     pl->g_dump_cap = rows_dev ? capacity : 0;
+    return PB2_OK;
+}
+
+int pb2_pipeline_set_counting(pb2_pipeline* pl, int enable) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_counting: null pipeline");
+    cudaError_t e;
+    if (!enable) {
+        if ((e = cudaDeviceSynchronize())) return cuda_fail(e, "pb2_pipeline_set_counting");
+        cudaFree(pl->trace_counters);
+        pl->trace_counters = nullptr;
+        return PB2_OK;
+    }
+    if (!pl->trace_counters && (e = cudaMalloc(&pl->trace_counters, 9 * sizeof(unsigned long long))))
+        return cuda_fail(e, "cudaMalloc trace counters");
+    if ((e = cudaMemset(pl->trace_counters, 0, 9 * sizeof(unsigned long long)))) return cuda_fail(e, "clear counters");
+    return PB2_OK;
+}
+
+int pb2_pipeline_get_trace_counters(const pb2_pipeline* pl, uint64_t* counters, void* stream) {
+    if (!pl || !counters) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_get_trace_counters: null argument");
+    if (!pl->trace_counters) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_get_trace_counters: counting is off");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(counters, pl->trace_counters, 9 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaStreamSynchronize(s)))
+        return cuda_fail(e, "read trace counters");
     return PB2_OK;
 }
 

@@ -373,3 +373,19 @@ def test_guided_render_with_slot_refill_is_unbiased():
         m1, s1 = _mean_and_se(pl)
     se = np.sqrt(s0 ** 2 + s1 ** 2)
     assert np.all(np.abs(m1 - m0) <= 4 * se + 1e-6), (m0, m1, se)
+
+
+def test_trained_guide_lowers_error_at_equal_samples():
+    """What the online-trained network gains over plain BxDF sampling, on the hard-indirect room at its
+    configuration (1280 x 720, 256 spp, depth 16; light behind a wall with a 5 cm door gap): at the same sample
+    count, the mean relMSE of three independently trained guided renders against the double-precision
+    4096-spp truth (tests/golden/truth_guiding_room_1280x720.npz) is below the plain render's.  (Measured
+    ratios on a B200 are 1.09-1.23; one run alone scatters by about 15 %, hence three.)"""
+    import bench
+    from piper2_b200 import guiding_eval
+
+    r = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0, repeats=3,
+                              truth=lambda img: bench.truth_rel_mse(img, "guiding_room_1280x720"))
+    plain, guided = r["plain"]["relmse_fp64"], r["guided"]["relmse_fp64"]
+    assert guided < 0.98 * plain, (plain, r["guided"]["relmse_fp64_each"])
+    assert r["guided"]["last_loss"] < r["guided"]["first_loss"]

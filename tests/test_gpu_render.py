@@ -276,3 +276,22 @@ def test_path_slots_rejects_out_of_range():
     with _api().Pipeline(sd) as pl:
         with pytest.raises(capi.PB2Error, match="path slots"):
             pl.set_path_slots(100)
+
+
+def test_counting_build_counts_and_keeps_results(oracle):
+    """The counting build of the render's traversal queries gives the same samples, and counts the rays the
+    launch statistics count (closest: extend + MIS; shadow)."""
+    sd = scenes.cornell_box(seed=3, width=32, height=32, spp=4)
+    with _api().Pipeline(sd) as pl:
+        _, s0 = pl.render(samples=True)
+        st0 = pl.stats()
+        pl.set_counting(True)
+        _, s1 = pl.render(samples=True)
+        c = pl.trace_counters()
+        st1 = pl.stats()
+        pl.set_counting(False)
+    assert np.array_equal(s0.view(np.uint32), s1.view(np.uint32))
+    assert c["extend"][0] + c["mis"][0] == st1.closest_rays - st0.closest_rays
+    assert c["shadow"][0] == st1.shadow_rays - st0.shadow_rays
+    for k, (rays, visits, tests) in c.items():
+        assert rays > 0 and visits >= rays * 0.5 and tests > 0, (k, rays, visits, tests)
