@@ -295,3 +295,24 @@ def test_counting_build_counts_and_keeps_results(oracle):
     assert c["shadow"][0] == st1.shadow_rays - st0.shadow_rays
     for k, (rays, visits, tests) in c.items():
         assert rays > 0 and visits >= rays * 0.5 and tests > 0, (k, rays, visits, tests)
+
+
+def test_two_devices_in_one_process(oracle):
+    """Kernel attributes and launch grids are cached per device: a process that switches devices with
+    pb2_set_device renders on both, each bit-exact with the oracle (needs two GPUs; skipped otherwise)."""
+    import torch
+
+    from piper2_b200 import capi
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU")
+    sd = scenes.cornell_box(seed=1, width=24, height=24, spp=2)
+    _, osamples = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
+    for dev in (0, 1, 0):
+        torch.cuda.set_device(dev)
+        capi.check(capi.lib().pb2_set_device(dev))
+        with _api().Pipeline(sd) as pl:
+            _, samples = pl.render(samples=True)
+        assert np.array_equal(samples.view(np.uint32), osamples.view(np.uint32)), dev
+    torch.cuda.set_device(0)
+    capi.check(capi.lib().pb2_set_device(0))
