@@ -114,9 +114,11 @@ def mlp_bench():
         res[name] = {"ms": round(ms, 4), "tflops": round(tf, 2), "frac": round(tf / peak, 4)}
     res["peak_tflops"] = peak
     res["peak_source"] = kind
-    res["note"] = ("forward_tcgen05: tcgen05.mma kind::f16 M=128 per CTA, TMEM accumulators (one stream "
-                   "synchronisation per call included); forward_mma_sync and training: mma.sync m16n8k16 bf16 "
-                   "tiles; the network is 64 wide")
+    res["note"] = ("forward_tcgen05: tcgen05.mma kind::f16, four 128-row warp groups per CTA, TMEM accumulators "
+                   "(one stream synchronisation per call included); training: one fused tcgen05 kernel per batch "
+                   "(forward, loss gradient, backward-data and the weight gradients accumulated in TMEM) plus the "
+                   "reduction over CTAs and Adam; forward_mma_sync: the mma.sync m16n8k16 cross-check; the "
+                   "network is 64 wide")
     return res
 
 

@@ -385,7 +385,13 @@ int pb2_guide_forward_mma(const pb2_guide* guide, const float* features_dev, uin
  * floats, may be NULL) and the loss; parameters unchanged. */
 int pb2_guide_gradient(pb2_guide* guide, const float* records_dev, uint32_t n, float* grad_host, float* loss_host,
                        void* stream);
-/* One Adam step (beta1 0.9, beta2 0.99) on the batch. */
+/* The same gradient on mma.sync tiles (16 records per warp, staged layer inputs and deltas, batch-K weight
+ * GEMMs); the cross-check of the tcgen05 training kernel that pb2_guide_gradient and pb2_guide_train use. */
+int pb2_guide_gradient_mma(pb2_guide* guide, const float* records_dev, uint32_t n, float* grad_host, float* loss_host,
+                           void* stream);
+/* One Adam step (beta1 0.9, beta2 0.99) on the batch.  The gradient runs on the tcgen05 tensor cores; a
+ * tensor-core wait that timed out is reported (PB2_ERR_DEVICE_TIMEOUT) by the next call that synchronises
+ * (pb2_guide_gradient, pb2_guide_train with loss_host, pb2_pipeline_train_guide). */
 int pb2_guide_train(pb2_guide* guide, const float* records_dev, uint32_t n, float learning_rate, float* loss_host,
                     void* stream);
 /* Called by every training step (pb2_guide_train, pb2_pipeline_train_guide) between the gradient and the

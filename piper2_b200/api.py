@@ -465,14 +465,16 @@ class Guide:
         torch.cuda.synchronize()
         return out.cpu().numpy()
 
-    def gradient(self, records: np.ndarray):
-        """records (n, 16) -> (gradient over the flat parameters, loss)."""
+    def gradient(self, records: np.ndarray, tiles: str = "tcgen05"):
+        """records (n, 16) -> (gradient over the flat parameters, loss); tiles = "tcgen05" (default, the
+        training kernel) or "mma" (the mma.sync cross-check)."""
         torch = _torch()
         r = torch.from_numpy(np.ascontiguousarray(records, dtype=np.float32)).cuda()
         g = np.empty(self.param_count(), dtype=np.float32)
         loss = C.c_float(0.0)
-        capi.check(capi.lib().pb2_guide_gradient(self.h, C.c_void_p(r.data_ptr()), r.shape[0],
-                                                 g.ctypes.data_as(C.c_void_p), C.byref(loss), _stream()))
+        fn = capi.lib().pb2_guide_gradient if tiles == "tcgen05" else capi.lib().pb2_guide_gradient_mma
+        capi.check(fn(self.h, C.c_void_p(r.data_ptr()), r.shape[0], g.ctypes.data_as(C.c_void_p), C.byref(loss),
+                      _stream()))
         return g, loss.value
 
     def train(self, records, learning_rate=5e-3) -> float:

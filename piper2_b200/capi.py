@@ -168,6 +168,8 @@ SIGNATURES = [
     ("pb2_guide_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_float),
                                       C.c_void_p]),
     ("pb2_guide_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_float), C.c_void_p]),
+    ("pb2_guide_gradient_mma", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_float),
+                                          C.c_void_p]),
     ("pb2_guide_set_gradient_hook", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pb2_pipeline_set_guide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(GuideSettings)]),
     ("pb2_pipeline_set_path_slots", C.c_int, [C.c_void_p, C.c_uint32]),

@@ -316,8 +316,8 @@ size_t guide_workspace_bytes() {
     return (size_t)kChunkRows * (kStageX + kStageD) * 2 + (size_t)kGwMaxBlocks * kParams * 4;
 }
 
-cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
-                           void* workspace, cudaStream_t stream) {
+cudaError_t guide_gradient_mma(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
+                               void* workspace, cudaStream_t stream) {
     using namespace guide;
     static std::atomic<int> attr_rows[kMaxDevices], attr_weights[kMaxDevices];
     cudaError_t e = smem_attr_once((const void*)k_grad_rows, grad_rows_smem(), attr_rows);
@@ -353,6 +353,22 @@ using namespace pb2;
 extern "C" {
 
 uint32_t pb2_guide_param_count(void) { return (uint32_t)guide::kParams; }
+
+}  // extern "C"
+
+namespace {
+// scalars[2] of a guide: set (as uint32 1) by a training step whose tensor-core wait timed out; sticky until
+// read by a call that synchronises.
+uint32_t* train_error(pb2_guide* g) { return reinterpret_cast<uint32_t*>(g->scalars + 2); }
+bool train_failed(pb2_guide* g, float flag_bits) {
+    uint32_t v;
+    std::memcpy(&v, &flag_bits, 4);
+    if (v) cudaMemset(g->scalars + 2, 0, 4);
+    return v != 0;
+}
+}  // namespace
+
+extern "C" {
 
 int pb2_guide_create(uint32_t seed, pb2_guide** out) {
     if (!out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_create: null argument");
@@ -454,7 +470,27 @@ int pb2_guide_gradient(pb2_guide* g, const float* records, uint32_t n, float* gr
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if ((e = cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s))) return cuda_fail(e, "memset grad");
-    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, g->workspace, s))) return cuda_fail(e, "guide gradient");
+    if ((e = guide_gradient_tc(g->view(), records, n, g->grad, g->scalars, g->workspace, train_error(g), s)))
+        return cuda_fail(e, "guide gradient");
+    float sc[3] = { 0, 0, 0 };
+    if ((e = cudaMemcpyAsync(sc, g->scalars, 12, cudaMemcpyDeviceToHost, s))) return cuda_fail(e, "read loss");
+    if (grad_host && (e = cudaMemcpyAsync(grad_host, g->grad, guide::kParams * 4, cudaMemcpyDeviceToHost, s)))
+        return cuda_fail(e, "read grad");
+    if ((e = cudaStreamSynchronize(s))) return cuda_fail(e, "sync");
+    if ((e = cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s))) return cuda_fail(e, "memset grad");
+    if (loss_host) *loss_host = sc[1];
+    if (train_failed(g, sc[2])) return fail(PB2_ERR_DEVICE_TIMEOUT, "pb2_guide_gradient: a tensor-core wait timed out");
+    return PB2_OK;
+}
+
+int pb2_guide_gradient_mma(pb2_guide* g, const float* records, uint32_t n, float* grad_host, float* loss_host,
+                           void* stream) {
+    if (!g || (n && !records)) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_gradient_mma: null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s))) return cuda_fail(e, "memset grad");
+    if ((e = guide_gradient_mma(g->view(), records, n, g->grad, g->scalars, g->workspace, s)))
+        return cuda_fail(e, "guide gradient");
     float sc[2] = { 0, 0 };
     if ((e = cudaMemcpyAsync(sc, g->scalars, 8, cudaMemcpyDeviceToHost, s))) return cuda_fail(e, "read loss");
     if (grad_host && (e = cudaMemcpyAsync(grad_host, g->grad, guide::kParams * 4, cudaMemcpyDeviceToHost, s)))
@@ -477,7 +513,8 @@ int pb2_guide_train(pb2_guide* g, const float* records, uint32_t n, float learni
     if (n == 0) return PB2_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
-    if ((e = guide_gradient(g->view(), records, n, g->grad, g->scalars, g->workspace, s))) return cuda_fail(e, "guide gradient");
+    if ((e = guide_gradient_tc(g->view(), records, n, g->grad, g->scalars, g->workspace, train_error(g), s)))
+        return cuda_fail(e, "guide gradient");
     if (g->hook) {
         const int rc = g->hook(g->grad, guide::kParams, stream, g->hook_user);
         if (rc != PB2_OK) {
@@ -492,10 +529,11 @@ int pb2_guide_train(pb2_guide* g, const float* records, uint32_t n, float learni
                                                                g->w16, g->b32);
     if ((e = cudaGetLastError())) return cuda_fail(e, "k_adam");
     if (loss_host) {
-        float sc[2];
-        if ((e = cudaMemcpyAsync(sc, g->scalars, 8, cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
+        float sc[3];
+        if ((e = cudaMemcpyAsync(sc, g->scalars, 12, cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
             return cuda_fail(e, "read loss");
         *loss_host = sc[1];
+        if (train_failed(g, sc[2])) return fail(PB2_ERR_DEVICE_TIMEOUT, "pb2_guide_train: a tensor-core wait timed out");
     }
     return PB2_OK;
 }

@@ -34,8 +34,12 @@ struct GuideView {
 };
 cudaError_t guide_forward(const GuideView& gv, const float* features, uint32_t n, float* out, cudaStream_t stream);
 // Batch loss gradient (added to grad) and loss; `workspace` holds guide_workspace_bytes() of staging.
-cudaError_t guide_gradient(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
-                           void* workspace, cudaStream_t stream);
+cudaError_t guide_gradient_mma(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
+                               void* workspace, cudaStream_t stream);
+// The same gradient on the tcgen05 tensor cores (guiding_train_tc.cu): one fused kernel per batch, each CTA's
+// partial gradient in `workspace`, then a reduction; error[0] is set if a tensor-core wait timed out.
+cudaError_t guide_gradient_tc(const GuideView& gv, const float* records, uint32_t n, float* grad, float* scalars,
+                              void* workspace, uint32_t* error, cudaStream_t stream);
 size_t guide_workspace_bytes();
 // The same forward pass on the tcgen05 tensor cores (guiding_tc.cu); error[0] is set if a tensor-core
 // wait timed out.

@@ -389,3 +389,24 @@ def test_trained_guide_lowers_error_at_equal_samples():
     plain, guided = r["plain"]["relmse_fp64"], r["guided"]["relmse_fp64"]
     assert guided < 0.98 * plain, (plain, r["guided"]["relmse_fp64_each"])
     assert r["guided"]["last_loss"] < r["guided"]["first_loss"]
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 4096, 70001])
+def test_gradient_tcgen05_matches_mma_tiles(n):
+    """The training kernel on the tcgen05 tensor cores against the mma.sync form of the same gradient (the
+    same bf16 roundings; accumulation order differs): parameters and loss agree, for tiles with padded
+    records and for several tiles per CTA."""
+    api = _api()
+    rng = np.random.default_rng(200 + n)
+    g = api.Guide(seed=7)
+    g.set_params(_trained_params(7))
+    rec = _records(rng, n)
+    g_tc, l_tc = g.gradient(rec, tiles="tcgen05")
+    g_mma, l_mma = g.gradient(rec, tiles="mma")
+    cos = float(g_tc.astype(np.float64) @ g_mma / (np.linalg.norm(g_tc) * np.linalg.norm(g_mma)))
+    rel = float(np.linalg.norm(g_tc - g_mma) / np.linalg.norm(g_mma))
+    assert cos > 0.99999 and rel < 2e-3, (cos, rel)
+    assert abs(l_tc - l_mma) <= 1e-4 * max(1.0, abs(l_mma))
+    # a second call gives the same gradient (no state kept in shared or tensor memory)
+    g_tc2, _ = g.gradient(rec, tiles="tcgen05")
+    assert np.allclose(g_tc2, g_tc, rtol=1e-5, atol=1e-7 * np.abs(g_tc).max())
