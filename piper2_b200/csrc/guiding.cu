@@ -357,14 +357,17 @@ uint32_t pb2_guide_param_count(void) { return (uint32_t)guide::kParams; }
 }  // extern "C"
 
 namespace {
-// scalars[2] of a guide: set (as uint32 1) by a training step whose tensor-core wait timed out; sticky until
-// read by a call that synchronises.
-uint32_t* train_error(pb2_guide* g) { return reinterpret_cast<uint32_t*>(g->scalars + 2); }
-bool train_failed(pb2_guide* g, float flag_bits) {
-    uint32_t v;
-    std::memcpy(&v, &flag_bits, 4);
-    if (v) cudaMemset(g->scalars + 2, 0, 4);
-    return v != 0;
+// scalars[4..7] of a guide: set by a training step whose tensor-core wait timed out (flag, stage, tile,
+// block); sticky until read by a call that synchronises, which reports and clears them.
+uint32_t* train_error(pb2_guide* g) { return reinterpret_cast<uint32_t*>(g->scalars + 4); }
+bool train_failed(pb2_guide* g) {
+    uint32_t v[4] = { 0, 0, 0, 0 };
+    cudaMemcpy(v, g->scalars + 4, sizeof(v), cudaMemcpyDeviceToHost);
+    if (!v[0]) return false;
+    cudaMemset(g->scalars + 4, 0, sizeof(v));
+    set_error("a tensor-core wait of the guide's training timed out (stage " + std::to_string(v[1]) + ", tile " +
+              std::to_string(v[2]) + ", block " + std::to_string(v[3]) + ")");
+    return true;
 }
 }  // namespace
 
@@ -378,8 +381,13 @@ int pb2_guide_create(uint32_t seed, pb2_guide** out) {
     cudaError_t e;
     if ((e = cudaMalloc(&g->params, P * 4)) || (e = cudaMalloc(&g->m, P * 4)) || (e = cudaMalloc(&g->v, P * 4)) ||
         (e = cudaMalloc(&g->grad, P * 4)) || (e = cudaMalloc(&g->w16, guide::kW16Elems * 2)) ||
-        (e = cudaMalloc(&g->b32, guide::kBiasElems * 4)) || (e = cudaMalloc(&g->scalars, 16)) ||
+        (e = cudaMalloc(&g->b32, guide::kBiasElems * 4)) || (e = cudaMalloc(&g->scalars, 64)) ||
         (e = cudaMalloc(&g->workspace, guide_workspace_bytes()))) {
+        pb2_guide_destroy(g);
+        return cuda_fail(e, "pb2_guide_create");
+    }
+    // loss scalars and the training's time-out record start cleared (device memory comes uninitialised)
+    if ((e = cudaMemset(g->scalars, 0, 64))) {
         pb2_guide_destroy(g);
         return cuda_fail(e, "pb2_guide_create");
     }
@@ -479,7 +487,7 @@ int pb2_guide_gradient(pb2_guide* g, const float* records, uint32_t n, float* gr
     if ((e = cudaStreamSynchronize(s))) return cuda_fail(e, "sync");
     if ((e = cudaMemsetAsync(g->grad, 0, guide::kParams * 4, s))) return cuda_fail(e, "memset grad");
     if (loss_host) *loss_host = sc[1];
-    if (train_failed(g, sc[2])) return fail(PB2_ERR_DEVICE_TIMEOUT, "pb2_guide_gradient: a tensor-core wait timed out");
+    if (train_failed(g)) return PB2_ERR_DEVICE_TIMEOUT;
     return PB2_OK;
 }
 
@@ -533,7 +541,7 @@ int pb2_guide_train(pb2_guide* g, const float* records, uint32_t n, float learni
         if ((e = cudaMemcpyAsync(sc, g->scalars, 12, cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
             return cuda_fail(e, "read loss");
         *loss_host = sc[1];
-        if (train_failed(g, sc[2])) return fail(PB2_ERR_DEVICE_TIMEOUT, "pb2_guide_train: a tensor-core wait timed out");
+        if (train_failed(g)) return PB2_ERR_DEVICE_TIMEOUT;
     }
     return PB2_OK;
 }

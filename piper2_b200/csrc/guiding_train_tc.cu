@@ -51,6 +51,24 @@ constexpr uint32_t kTrTmemCols = 512;
 constexpr uint32_t kAccCol = 0;                        // forward / backward-data accumulator (64 columns)
 __host__ __device__ constexpr uint32_t dw_col(int l) { return 64u + 64u * (uint32_t)l; }  // dW_l^T: out_l columns
 
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the mbarrier phase for at most kTrWaitNs of device time (not a poll count, so that a busy GPU does
+// not shorten it); false on time-out.
+constexpr unsigned long long kTrWaitNs = 200ull * 1000 * 1000;  // 200 ms
+__device__ __forceinline__ bool mbar_wait_timed(uint32_t bar, uint32_t parity) {
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (now_ns() - t0 > kTrWaitNs) return false;
+    }
+}
+
 // kind::f16 instruction descriptor with operand majorness: a_mn / b_mn = 1 reads that operand MN-major.
 __device__ __forceinline__ uint32_t instr_desc_major(uint32_t n, uint32_t a_mn, uint32_t b_mn) {
     return instr_desc(n) | (a_mn << 15) | (b_mn << 16);
@@ -115,14 +133,21 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     const float gscale = -(wsum > 0.f ? 1.f / wsum : 1.f / (float)(n ? n : 1));
     float loss_acc = 0.f;
 
-    // commits the MMAs thread 0 issued and waits for them (all threads); false if the wait timed out
+    // commits the MMAs thread 0 issued and waits for them (all threads); false if the wait timed out.  On
+    // time-out error[0] = 1 and, from the first CTA to fail, error[1..3] = the wait's stage (1 + layer for the
+    // forward, 16 + layer for the backward), the tile and the block.
+    uint32_t stage = 0, cur_tile = 0;
     auto commit_wait = [&]() -> bool {
         if (tid == 0) mma_commit(bar_addr);
-        bool ok = mbar_wait_bounded(bar_addr, phase);
+        bool ok = mbar_wait_timed(bar_addr, phase);
         phase ^= 1u;
         if (!ok) {
             s_fail = 1u;
-            atomicExch(error, 1u);
+            if (atomicExch(error, 1u) == 0u) {
+                error[1] = stage;
+                error[2] = cur_tile;
+                error[3] = blockIdx.x;
+            }
         }
         tc_fence_after();
         __syncthreads();
@@ -139,6 +164,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     bool first = true;
     for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
         const uint32_t row = tile * kTcRows + tid;
+        cur_tile = tile;
         float r[16];
         if (row < n) {
             const float4* p = reinterpret_cast<const float4*>(rec + 16 * (size_t)row);
@@ -165,6 +191,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
         float y[kOut];
         for (int l = 0; l < kLayers && !failed; ++l) {
             const uint32_t kdim = layer_in(l), ndim = layer_out(l);
+            stage = 1u + (uint32_t)l;
             if (tid == 0) {
                 const uint32_t a0 = smem_u32(act(smem, l)), b0 = smem_u32(w_s + tc_w_offset(l));
                 for (uint32_t s = 0; s < kdim / 16; ++s)
@@ -223,6 +250,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
             // dZ_l: dY for the output layer, else written over a_{l+1}
             const unsigned char* dz = l == kLayers - 1 ? smem + kTrOffDY : act(smem, l + 1);
             const uint32_t dz_dim = l == kLayers - 1 ? (uint32_t)kOut : (uint32_t)kActDim;
+            stage = 16u + (uint32_t)l;
             if (tid == 0) {
                 // dW_l^T (M = 128 feature rows, N = out_l) += a_l^T . dZ_l over this tile's 128 records (K)
                 const uint32_t a0 = smem_u32(act(smem, l)), z0 = smem_u32(dz);
@@ -267,7 +295,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
         }
         first = false;
     }
-    if (failed && tid == 0) mbar_wait_bounded(bar_addr, phase);  // let MMAs in flight finish before freeing
+    if (failed && tid == 0) mbar_wait_timed(bar_addr, phase);  // let MMAs in flight finish before freeing
     for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xFFFFFFFFu, loss_acc, o);
     if (lane == 0 && loss_acc != 0.f) atomicAdd(loss, loss_acc);
     tc_fence_before();
