@@ -21,6 +21,7 @@
 // Waits on the mbarrier are bounded: on time-out the CTA records an error, stops, gives the tensor core a
 // bounded time to drain, frees its TMEM and returns.
 #include <algorithm>
+#include <cstdlib>
 
 #include "guiding_tc.cuh"
 #include "pb2_internal.h"
@@ -82,7 +83,7 @@ __host__ __device__ constexpr uint32_t act_dim(int l) { return l == 0 ? (uint32_
 __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const float* __restrict__ rec, uint32_t n,
                                                           const float* __restrict__ scalars,
                                                           float* __restrict__ partial, float* __restrict__ loss,
-                                                          uint32_t* __restrict__ error) {
+                                                          uint32_t* __restrict__ error, uint32_t skip_commit) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     unsigned char* w_s = smem + kTrOffW;
@@ -137,8 +138,10 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     // time-out error[0] = 1 and, from the first CTA to fail, error[1..3] = the wait's stage (1 + layer for the
     // forward, 16 + layer for the backward), the tile and the block.
     uint32_t stage = 0, cur_tile = 0;
+    bool first = true;  // this CTA's first tile: the weight-gradient accumulators start from zero
     auto commit_wait = [&]() -> bool {
-        if (tid == 0) mma_commit(bar_addr);
+        // skip_commit (failure-detection tests only): the first tile's wait at that stage gets no arrival
+        if (tid == 0 && !(first && stage == skip_commit)) mma_commit(bar_addr);
         bool ok = mbar_wait_timed(bar_addr, phase);
         phase ^= 1u;
         if (!ok) {
@@ -161,7 +164,6 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     };
 
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    bool first = true;
     for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
         const uint32_t row = tile * kTcRows + tid;
         cur_tile = tile;
@@ -389,7 +391,11 @@ cudaError_t guide_gradient_tc(const GuideView& gv, const float* records, uint32_
     float* wpart = partial + (size_t)grid * kParams;  // kWsBlocks floats after the CTAs' partial gradients
     k_weight_sum_part<<<kWsBlocks, kWsThreads, 0, stream>>>(records, n, wpart);
     k_weight_sum_final<<<1, 32, 0, stream>>>(wpart, scalars);
-    k_grad_tc<<<grid, kTrThreads, kTrSmem, stream>>>(gv, records, n, scalars, partial, scalars + 1, error);
+    // PB2_TEST_TRAIN_TIMEOUT=<stage> (failure-detection tests): the first tile's MMAs of that stage are committed
+    // to nothing, so its bounded wait runs out and the step reports the time-out; read on every call
+    const char* inject = std::getenv("PB2_TEST_TRAIN_TIMEOUT");
+    const uint32_t skip = inject ? (uint32_t)std::strtoul(inject, nullptr, 10) : 0u;
+    k_grad_tc<<<grid, kTrThreads, kTrSmem, stream>>>(gv, records, n, scalars, partial, scalars + 1, error, skip);
     k_grad_reduce_all<<<(kParams + 255) / 256, 256, 0, stream>>>(partial, grid, grad);
     return cudaGetLastError();
 }

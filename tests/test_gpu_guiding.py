@@ -410,3 +410,24 @@ def test_gradient_tcgen05_matches_mma_tiles(n):
     # a second call gives the same gradient (no state kept in shared or tensor memory)
     g_tc2, _ = g.gradient(rec, tiles="tcgen05")
     assert np.allclose(g_tc2, g_tc, rtol=1e-5, atol=1e-7 * np.abs(g_tc).max())
+
+
+def test_training_wait_timeout_is_reported(monkeypatch):
+    """Failure detection without a GPU fault: with PB2_TEST_TRAIN_TIMEOUT the training kernel commits one
+    stage's tensor-core work to nothing, so that stage's bounded wait runs out (a flag nothing sets); the
+    kernel frees its tensor memory and returns, the step reports PB2_ERR_DEVICE_TIMEOUT with the stage, and
+    the next step on the same guide and context succeeds."""
+    from piper2_b200 import capi
+
+    api = _api()
+    rng = np.random.default_rng(41)
+    g = api.Guide(seed=8)
+    rec = _records(rng, 4096)
+    monkeypatch.setenv("PB2_TEST_TRAIN_TIMEOUT", "17")  # the backward stage of layer 1
+    with pytest.raises(capi.PB2Error, match="timed out.*stage 17"):
+        g.train(rec, learning_rate=1e-3)
+    monkeypatch.delenv("PB2_TEST_TRAIN_TIMEOUT")
+    loss = g.train(rec, learning_rate=1e-3)
+    assert np.isfinite(loss) and loss != 0.0
+    grad, _ = g.gradient(rec)
+    assert np.all(np.isfinite(grad)) and np.abs(grad).max() > 0
