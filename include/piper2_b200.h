@@ -53,9 +53,12 @@ typedef struct pb2_hit {
 
 /* One triangle mesh placed in the scene.  Mirrors TriangleIndexedGeometryDesc
  * (Src/Interface/BuiltinComponent/Tracer.hpp:51-63) plus the GSM instance (geometry + surface,
- * Tracer.hpp:146-147) and its node transform (Tracer.hpp:148).  Transforms are translation-only:
- * the reference inverts instance transforms with calcInverse (Src/Kernel/Transform.hpp:344-362),
- * which is wrong for any rotation or scale, so scenes bake those into the vertices. */
+ * Tracer.hpp:146-147) and its node transform (Tracer.hpp:148).  A vertex lands in world space as
+ * transform * vertex + translation.  `transform` NULL is the reference's translation-only instance.  A
+ * non-NULL transform (rotation, scale, skew: pb2_srt_matrix) is a divergence: the reference inverts instance
+ * transforms with calcInverse (Src/Kernel/Transform.hpp:344-362), which is wrong for any rotation or scale;
+ * here the instance is flattened into world space when the acceleration structure is built, so its hits,
+ * normals and shading are those of the transformed geometry. */
 typedef struct pb2_mesh {
     const float* vertices;    /* vert_count * 3 floats */
     const uint32_t* indices;  /* tri_count * 3 */
@@ -64,7 +67,19 @@ typedef struct pb2_mesh {
     uint32_t tri_count;
     uint32_t material;        /* index into pb2_scene.materials */
     float translation[3];
+    const float* transform;   /* NULL, or a row-major 3x4 local-to-world matrix [L | t] (12 floats) */
 } pb2_mesh;
+
+/* TransformSRT (Src/Kernel/Transform.hpp:390-393), the reference's instance transform: Embree's
+ * RTCQuaternionDecomposition, local-to-world = T * R * S (S = scale with skew and shift, R = the rotation of
+ * the quaternion, T = translation). */
+typedef struct pb2_srt {
+    float scale[3];       /* scaleX, scaleY, scaleZ */
+    float skew[3];        /* skewXY, skewXZ, skewYZ */
+    float shift[3];       /* shiftX, shiftY, shiftZ */
+    float quat[4];        /* quatW, quatX, quatY, quatZ (normalised on use) */
+    float translation[3]; /* transX, transY, transZ */
+} pb2_srt; /* 64 bytes */
 
 /* Parallelogram primitive of the BasicShapes "Plane" geometry: PerPlaneData
  * (Src/BuiltinComponent/Geometry/BasicShapes/Shared.hpp:22-28), byte-compatible (64 bytes).
@@ -181,6 +196,12 @@ int pb2_set_device(int device);
 /* ---- component helpers (host) -------------------------------------------------------------- */
 /* Plane primitive from Origin/U/V (BasicShapes.cpp:70-89). */
 int pb2_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out);
+/* The row-major 3x4 local-to-world matrix of an SRT transform; PB2_ERR_INVALID_ARGUMENT for a zero or non-finite
+ * quaternion or a non-finite entry. */
+int pb2_srt_matrix(const pb2_srt* srt, float matrix[12]);
+/* A plane mapped by a 3x4 local-to-world matrix: origin as a point, u and v as vectors, then pb2_plane_make (the
+ * normal of the mapped parallelogram is the correctly transformed normal). */
+int pb2_plane_transform(const pb2_plane* in, const float matrix[12], pb2_plane* out);
 /* Camera from the PerspectiveCamera config keys in their config units (mm, FStop)
  * (PerspectiveCamera.cpp:39-44). */
 int pb2_camera_from_config(const float position[3], const float look_at[3], const float up[3],
@@ -304,8 +325,13 @@ int pb2_builder_register_resource(pb2_builder* builder, const void* data, size_t
 int pb2_builder_register_call(pb2_builder* builder, const char* symbol, const void* payload, size_t bytes,
                               uint64_t* handle);
 /* A scene node (Tracer::buildNode) by the TraversalHandle value payloads use for it, with its
- * translation (the only transform the pipeline supports, see pb2_mesh). */
+ * translation. */
 int pb2_builder_add_node(pb2_builder* builder, uint64_t traversal, const float translation[3]);
+/* A scene node with a full local-to-world transform (row-major 3x4, e.g. from pb2_srt_matrix).  A light on it has
+ * its planes mapped into world space (pb2_plane_transform) unless the linear part is the identity, in which case
+ * it is the translation-only node of pb2_builder_add_node; a camera on it stands at the transform's origin, as the
+ * reference's rayGen reads only the origin of its node (PerspectiveCamera/Kernel.cpp:25-28). */
+int pb2_builder_add_node_transform(pb2_builder* builder, uint64_t traversal, const float matrix[12]);
 /* A component's materialized program of the given pb2_program_kind: its (first) symbol and payload.
  * *index (may be NULL) is the material index of a surface, the light index of a light, else 0. */
 int pb2_builder_add_program(pb2_builder* builder, uint32_t kind, const char* symbol, const void* payload,

@@ -710,7 +710,7 @@ or_scene* or_scene_create(const pb2_scene* d, int use_bvh) {
         for (uint32_t i = 0; i < mesh->tri_count; ++i, ++k) {
             for (int j = 0; j < 3; ++j) {
                 const uint32_t vi = mesh->indices[3 * i + j];
-                for (int a = 0; a < 3; ++a) s->tri[9 * k + 3 * j + a] = mesh->vertices[3 * vi + a] + mesh->translation[a];
+                pb2_mesh_vertex(mesh->transform, mesh->translation, mesh->vertices + 3 * vi, s->tri + 9 * k + 3 * j);
             }
             s->tri_mat[k] = mesh->material;
         }

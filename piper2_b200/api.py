@@ -153,6 +153,11 @@ class Builder:
     def add_node(self, traversal: int, translation):
         capi.check(capi.lib().pb2_builder_add_node(self.h, int(traversal), capi.f3(translation)))
 
+    def add_node_transform(self, traversal: int, matrix):
+        """A node with a full row-major 3x4 local-to-world transform (scenes.srt_matrix)."""
+        m = np.ascontiguousarray(matrix, dtype=np.float32).reshape(12)
+        capi.check(capi.lib().pb2_builder_add_node_transform(self.h, int(traversal), m.ctypes.data))
+
     def add_program(self, kind, symbol: str, payload: bytes = b"") -> int:
         b, n = self._buf(payload)
         idx = C.c_uint32()
@@ -160,13 +165,22 @@ class Builder:
         capi.check(capi.lib().pb2_builder_add_program(self.h, k, symbol.encode(), b, n, C.byref(idx)))
         return idx.value
 
-    def add_mesh(self, vertices, indices, material: int, translation=(0.0, 0.0, 0.0)):
+    def add_mesh(self, vertices, indices, material: int, translation=(0.0, 0.0, 0.0), transform=None,
+                 texcoords=None):
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         ix = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
         m = capi.Mesh()
         m.vertices, m.indices, m.texcoords = v.ctypes.data, ix.ctypes.data, None
         m.vert_count, m.tri_count, m.material = v.shape[0], ix.shape[0], int(material)
         m.translation[:] = [float(x) for x in translation]
+        if transform is not None:
+            tr = np.ascontiguousarray(transform, dtype=np.float32).reshape(12)
+            m.transform = tr.ctypes.data
+        if texcoords is not None:
+            tc = np.ascontiguousarray(texcoords, dtype=np.float32).reshape(-1, 2)
+            if tc.shape[0] != v.shape[0]:
+                raise ValueError("texcoords must hold one (u, v) per vertex")
+            m.texcoords = tc.ctypes.data
         capi.check(capi.lib().pb2_builder_add_mesh(self.h, C.byref(m)))  # copied by the library
 
     def build(self, width: int, height: int, fit_mode: int, samples_per_pixel: int):

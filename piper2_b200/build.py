@@ -1,9 +1,10 @@
 """Builds the CUDA library piper2_b200/_lib/libpiper2_b200.so for sm_100a.
 
 Every translation unit is compiled with
-    -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -fmad=false
+    -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -fmad=false -Xcompiler -ffp-contract=off
 -fmad=false keeps every float operation a single IEEE operation in source order (fused multiply-adds
-are written out where wanted), which is what makes device paths bit-identical to the CPU oracle.
+are written out where wanted), and -ffp-contract=off does the same for host code (the flattening of instance
+transforms), which is what makes device paths bit-identical to the CPU oracle.
 The generated Sobol tables (piper2_b200/sobol_tables.py) are written to piper2_b200/_build/gen/.
 """
 from __future__ import annotations
@@ -23,7 +24,7 @@ ROOT = os.path.dirname(HERE)
 SOURCES = ["bvh_build.cu", "traverse.cu", "render.cu", "capi.cu", "nalloc.cu", "guiding.cu", "guiding_tc.cu",
            "guiding_train_tc.cu", "materialize.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
-              "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 
 
 def _nvcc():

@@ -39,6 +39,12 @@ assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
 class Mesh(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("indices", C.c_void_p), ("texcoords", C.c_void_p),
                 ("vert_count", C.c_uint32), ("tri_count", C.c_uint32), ("material", C.c_uint32),
+                ("translation", C.c_float * 3), ("transform", C.c_void_p)]
+
+
+class SRT(C.Structure):
+    """pb2_srt: the reference's TransformSRT (Src/Kernel/Transform.hpp:390-393)."""
+    _fields_ = [("scale", C.c_float * 3), ("skew", C.c_float * 3), ("shift", C.c_float * 3), ("quat", C.c_float * 4),
                 ("translation", C.c_float * 3)]
 
 
@@ -120,6 +126,8 @@ SIGNATURES = [
     ("pb2_abi_version", C.c_int, []),
     ("pb2_set_device", C.c_int, [C.c_int]),
     ("pb2_plane_make", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(Plane)]),
+    ("pb2_srt_matrix", C.c_int, [C.POINTER(SRT), C.POINTER(C.c_float)]),
+    ("pb2_plane_transform", C.c_int, [C.POINTER(Plane), C.POINTER(C.c_float), C.POINTER(Plane)]),
     ("pb2_camera_from_config", C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                           C.POINTER(C.c_float), C.c_float, C.c_float, C.POINTER(Camera)]),
     ("pb2_calc_render_rect", C.c_int, [C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.POINTER(NDCTransform),
@@ -181,6 +189,7 @@ SIGNATURES = [
     ("pb2_builder_register_resource", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]),
     ("pb2_builder_register_call", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64)]),
     ("pb2_builder_add_node", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("pb2_builder_add_node_transform", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
     ("pb2_builder_add_program", C.c_int, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_void_p, C.c_size_t,
                                           C.POINTER(C.c_uint32)]),
     ("pb2_builder_add_mesh", C.c_int, [C.c_void_p, C.c_void_p]),

@@ -99,6 +99,26 @@ int pb2_plane_make(const float origin[3], const float u[3], const float v[3], pb
     return PB2_OK;
 }
 
+int pb2_srt_matrix(const pb2_srt* srt, float matrix[12]) {
+    if (!srt || !matrix) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_srt_matrix: null argument");
+    const float* f = reinterpret_cast<const float*>(srt);
+    for (int i = 0; i < 16; ++i)
+        if (!std::isfinite(f[i])) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_srt_matrix: non-finite entry");
+    if (f[9] == 0.0f && f[10] == 0.0f && f[11] == 0.0f && f[12] == 0.0f)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_srt_matrix: zero quaternion");
+    pb2_srt_matrix_hd(f, matrix);
+    return PB2_OK;
+}
+
+int pb2_plane_transform(const pb2_plane* in, const float matrix[12], pb2_plane* out) {
+    if (!in || !matrix || !out) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_plane_transform: null argument");
+    float o[3], u[3], v[3];
+    pb2_xform_point(matrix, in->origin, o);
+    pb2_xform_vector(matrix, in->u, u);
+    pb2_xform_vector(matrix, in->v, v);
+    return pb2_plane_make(o, u, v, out);
+}
+
 /* PerspectiveCamera config -> payload (Src/BuiltinComponent/Sensor/PerspectiveCamera/PerspectiveCamera.cpp:39-44) */
 int pb2_camera_from_config(const float position[3], const float look_at[3], const float up[3],
                            const float sensor_size_mm[2], float focal_length_mm, float fstop, pb2_camera* out) {
@@ -166,6 +186,10 @@ int pb2_accel_create(const pb2_scene* scene, void* stream_ptr, pb2_accel** out) 
         for (uint64_t i = 0; i < 3ull * mesh.tri_count; ++i)
             if (mesh.indices[i] >= mesh.vert_count)
                 return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: vertex index out of range");
+        if (mesh.transform)
+            for (int i = 0; i < 12; ++i)
+                if (!std::isfinite(mesh.transform[i]))
+                    return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_accel_create: non-finite mesh transform");
         n64 += mesh.tri_count;
     }
     if (n64 >= 0x80000000ull) return fail(PB2_ERR_NOT_SUPPORTED, "pb2_accel_create: more than 2^31 triangles");
@@ -184,7 +208,7 @@ int pb2_accel_create(const pb2_scene* scene, void* stream_ptr, pb2_accel** out) 
             float v[9];
             for (int j = 0; j < 3; ++j) {
                 const uint32_t vi = mesh.indices[3 * i + j];
-                for (int a = 0; a < 3; ++a) v[3 * j + a] = mesh.vertices[3 * vi + a] + mesh.translation[a];
+                pb2_mesh_vertex(mesh.transform, mesh.translation, mesh.vertices + 3 * vi, v + 3 * j);
             }
             uint32_t id = k;
             float w;

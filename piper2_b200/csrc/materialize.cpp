@@ -104,7 +104,11 @@ struct pb2_builder {
     };
     std::vector<std::vector<unsigned char>> resources;
     std::vector<Call> calls;  // CallHandle value = index + 1
-    std::unordered_map<uint64_t, std::array<float, 3>> nodes;
+    struct Node {
+        float m[12];    // row-major 3x4 local-to-world
+        bool linear;    // the linear part is not the identity (a rotation, scale or skew)
+    };
+    std::unordered_map<uint64_t, Node> nodes;
     bool sensor = false, integrator = false, driver = false, sampler = false, light_sampler = false, env = false;
     pb2::payload::PCData camera{};
     uint32_t max_depth = 0, min_rr_depth = 0, filter = PB2_FILTER_BOX;
@@ -114,7 +118,7 @@ struct pb2_builder {
     std::vector<pb2_plane> planes;
     std::vector<pb2_area_light> area_lights;
     struct Mesh {
-        std::vector<float> vertices, texcoords;
+        std::vector<float> vertices, texcoords, transform;
         std::vector<uint32_t> indices;
         pb2_mesh desc;
     };
@@ -201,11 +205,17 @@ int surface(pb2_builder* b, const std::string& sym, const void* p, size_t n, pb2
     return PB2_OK;
 }
 
-int node_translation(const pb2_builder* b, uint64_t traversal, float (&t)[3]) {
+const pb2_builder::Node* find_node(const pb2_builder* b, uint64_t traversal) {
     auto it = b->nodes.find(traversal);
-    if (it == b->nodes.end())
-        return fail(PB2_ERR_INVALID_ARGUMENT, "traversal handle " + std::to_string(traversal) + " names no node");
-    for (int k = 0; k < 3; ++k) t[k] = it->second[k];
+    return it == b->nodes.end() ? nullptr : &it->second;
+}
+
+// The node's origin: its translation, or for a full transform the image of the local origin (the reference's
+// rayGen reads only this, Sensor/PerspectiveCamera/Kernel.cpp:25-28).
+int node_translation(const pb2_builder* b, uint64_t traversal, float (&t)[3]) {
+    const pb2_builder::Node* nd = find_node(b, traversal);
+    if (!nd) return fail(PB2_ERR_INVALID_ARGUMENT, "traversal handle " + std::to_string(traversal) + " names no node");
+    for (int k = 0; k < 3; ++k) t[k] = nd->m[4 * k + 3];
     return PB2_OK;
 }
 
@@ -241,6 +251,8 @@ int light(pb2_builder* b, const std::string& sym, const void* p, size_t n, uint3
             return fail(PB2_ERR_INVALID_ARGUMENT, "planeSample: the primitive resource is not size x PerPlaneData");
         pb2_area_light al{};
         if ((rc = node_translation(b, cdf.traversal, al.translation))) return rc;
+        const pb2_builder::Node* nd = find_node(b, cdf.traversal);
+        if (nd->linear) al.translation[0] = al.translation[1] = al.translation[2] = 0.0f;  // planes mapped below
         al.radiance[0] = d.radiance.x;
         al.radiance[1] = d.radiance.y;
         al.radiance[2] = d.radiance.z;
@@ -249,6 +261,10 @@ int light(pb2_builder* b, const std::string& sym, const void* p, size_t n, uint3
         for (uint32_t i = 0; i < cdf.size; ++i) {
             pb2_plane pl;
             std::memcpy(&pl, res.data() + i * sizeof(pb2_plane), sizeof(pl));
+            if (nd->linear) {
+                pb2_plane local = pl;
+                if ((rc = pb2_plane_transform(&local, nd->m, &pl))) return rc;
+            }
             b->planes.push_back(pl);
         }
         b->area_lights.push_back(al);
@@ -293,7 +309,22 @@ int pb2_builder_register_call(pb2_builder* b, const char* symbol, const void* pa
 
 int pb2_builder_add_node(pb2_builder* b, uint64_t traversal, const float translation[3]) {
     if (!b || !translation) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_builder_add_node: null argument");
-    b->nodes[traversal] = { translation[0], translation[1], translation[2] };
+    pb2_builder::Node nd{ { 1, 0, 0, translation[0], 0, 1, 0, translation[1], 0, 0, 1, translation[2] }, false };
+    b->nodes[traversal] = nd;
+    return PB2_OK;
+}
+
+int pb2_builder_add_node_transform(pb2_builder* b, uint64_t traversal, const float matrix[12]) {
+    if (!b || !matrix) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_builder_add_node_transform: null argument");
+    pb2_builder::Node nd{};
+    for (int i = 0; i < 12; ++i) {
+        if (!std::isfinite(matrix[i]))
+            return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_builder_add_node_transform: non-finite entry");
+        nd.m[i] = matrix[i];
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) nd.linear |= matrix[4 * r + c] != (r == c ? 1.0f : 0.0f);
+    b->nodes[traversal] = nd;
     return PB2_OK;
 }
 
@@ -369,6 +400,7 @@ int pb2_builder_add_mesh(pb2_builder* b, const pb2_mesh* mesh) {
     m.vertices.assign(mesh->vertices, mesh->vertices + 3 * (size_t)mesh->vert_count);
     m.indices.assign(mesh->indices, mesh->indices + 3 * (size_t)mesh->tri_count);
     if (mesh->texcoords) m.texcoords.assign(mesh->texcoords, mesh->texcoords + 2 * (size_t)mesh->vert_count);
+    if (mesh->transform) m.transform.assign(mesh->transform, mesh->transform + 12);
     m.desc = *mesh;
     b->meshes.push_back(std::move(m));
     return PB2_OK;
@@ -390,6 +422,7 @@ int pb2_builder_build(pb2_builder* b, uint32_t width, uint32_t height, uint32_t 
         d.vertices = m.vertices.data();
         d.indices = m.indices.data();
         d.texcoords = m.texcoords.empty() ? nullptr : m.texcoords.data();
+        d.transform = m.transform.empty() ? nullptr : m.transform.data();
         b->mesh_descs.push_back(d);
     }
     std::memset(scene, 0, sizeof(*scene));

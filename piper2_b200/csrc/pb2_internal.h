@@ -8,6 +8,7 @@
 
 #include "../../include/piper2_b200.h"
 #include "pb2_bvh.h"
+#include "pb2_math.h"
 
 namespace pb2 {
 

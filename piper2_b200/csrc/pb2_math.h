@@ -188,3 +188,58 @@ PB2_HD uint32_t pb2_owen_scramble(uint32_t v, uint32_t seed) {
     return pb2_reverse_bits(x);
 }
 
+
+/* ---- instance transforms -------------------------------------------------------------------------------
+ * An instance's local-to-world transform in the reference's TransformSRT layout (Src/Kernel/Transform.hpp:390-393):
+ * 16 floats -- scale x y z, skew xy xz yz, shift x y z, quaternion w x y z, translation x y z.  The reference hands
+ * it to Embree 3 unchanged as an RTCQuaternionDecomposition (Src/BuiltinComponent/Tracer/Embree/Embree.cpp:699-703),
+ * whose published meaning is local-to-world = T * R * S with
+ *     S = [ sx kxy kxz hx ]      R = rotation of the unit quaternion (w, x, y, z)     T = translation
+ *         [  0  sy kyz hy ]
+ *         [  0   0  sz hz ]
+ * pb2_srt_matrix_hd writes the row-major 3x4 matrix [L | t], L = R * S(3x3), t = R * h + translation, normalising the
+ * quaternion first (the caller rejects a zero quaternion).  Points map as ((m0 x + m1 y) + m2 z) + m3 per row, every
+ * operation a single IEEE operation, so the host flattening and a device evaluation agree bit for bit. */
+PB2_HD void pb2_srt_matrix_hd(const float* srt, float* m) {
+    const float sx = srt[0], sy = srt[1], sz = srt[2], kxy = srt[3], kxz = srt[4], kyz = srt[5];
+    const float hx = srt[6], hy = srt[7], hz = srt[8];
+    const float n2 = ((srt[9] * srt[9] + srt[10] * srt[10]) + srt[11] * srt[11]) + srt[12] * srt[12];
+    const float inv = 1.0f / sqrtf(n2);
+    const float w = srt[9] * inv, x = srt[10] * inv, y = srt[11] * inv, z = srt[12] * inv;
+    float r[9];
+    r[0] = 1.0f - 2.0f * (y * y + z * z);
+    r[1] = 2.0f * (x * y - w * z);
+    r[2] = 2.0f * (x * z + w * y);
+    r[3] = 2.0f * (x * y + w * z);
+    r[4] = 1.0f - 2.0f * (x * x + z * z);
+    r[5] = 2.0f * (y * z - w * x);
+    r[6] = 2.0f * (x * z - w * y);
+    r[7] = 2.0f * (y * z + w * x);
+    r[8] = 1.0f - 2.0f * (x * x + y * y);
+    for (int i = 0; i < 3; ++i) {
+        const float a = r[3 * i], b = r[3 * i + 1], c = r[3 * i + 2];
+        m[4 * i + 0] = a * sx;
+        m[4 * i + 1] = a * kxy + b * sy;
+        m[4 * i + 2] = (a * kxz + b * kyz) + c * sz;
+        m[4 * i + 3] = ((a * hx + b * hy) + c * hz) + srt[13 + i];
+    }
+}
+
+PB2_HD void pb2_xform_point(const float* m, const float* p, float* out) {
+    for (int i = 0; i < 3; ++i) out[i] = ((m[4 * i] * p[0] + m[4 * i + 1] * p[1]) + m[4 * i + 2] * p[2]) + m[4 * i + 3];
+}
+
+PB2_HD void pb2_xform_vector(const float* m, const float* v, float* out) {
+    for (int i = 0; i < 3; ++i) out[i] = (m[4 * i] * v[0] + m[4 * i + 1] * v[1]) + m[4 * i + 2] * v[2];
+}
+
+/* A mesh vertex in world space: the instance matrix (if any), then the node translation. */
+PB2_HD void pb2_mesh_vertex(const float* matrix, const float* translation, const float* p, float* out) {
+    if (matrix) {
+        float q[3];
+        pb2_xform_point(matrix, p, q);
+        for (int i = 0; i < 3; ++i) out[i] = q[i] + translation[i];
+    } else {
+        for (int i = 0; i < 3; ++i) out[i] = p[i] + translation[i];
+    }
+}

@@ -1472,12 +1472,14 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
         float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
         for (uint32_t m = 0; m < scene->mesh_count; ++m) {
             const pb2_mesh& me = scene->meshes[m];
-            for (uint32_t v = 0; v < me.vert_count; ++v)
+            for (uint32_t v = 0; v < me.vert_count; ++v) {
+                float x[3];
+                pb2_mesh_vertex(me.transform, me.translation, me.vertices + 3 * v, x);
                 for (int k = 0; k < 3; ++k) {
-                    const float x = me.vertices[3 * v + k] + me.translation[k];
-                    lo[k] = std::fmin(lo[k], x);
-                    hi[k] = std::fmax(hi[k], x);
+                    lo[k] = std::fmin(lo[k], x[k]);
+                    hi[k] = std::fmax(hi[k], x[k]);
                 }
+            }
         }
         for (uint32_t i = 0; i < scene->plane_count; ++i) {
             const pb2_plane& pp = scene->planes[i];

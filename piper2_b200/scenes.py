@@ -10,9 +10,11 @@ so the same seed gives the same float32 arrays on every machine.
   uniform in [0,1]^3 and lognormal edge lengths (median 0.01, sigma 0.5); 4M closest-hit rays from
   the bounding sphere towards uniform interior points, 4M any-hit rays of length U[0.1, 1].
 
-Rotations are baked into vertex positions and instance transforms are translation-only, because the
-reference inverts instance transforms with a routine that is only correct for translations
-(Src/Kernel/Transform.hpp:344-362).
+The benchmark scenes bake rotations into vertex positions and use translation-only instances, the only
+instance transforms the reference renders correctly (it inverts them with a routine that is only correct for
+translations, Src/Kernel/Transform.hpp:344-362).  A mesh may instead carry a full SRT instance transform
+(:func:`srt_matrix`, ``MeshData.transform``), which the library flattens into world space when it builds the
+acceleration structure -- a divergence from the reference for rotated or scaled instances.
 """
 from __future__ import annotations
 
@@ -53,6 +55,45 @@ def plane_make(origin, u, v) -> capi.Plane:
     return p
 
 
+def euler_quaternion(pitch: float, yaw: float, roll: float) -> tuple:
+    """The quaternion (w, x, y, z) of the reference's three-angle "Rotation" (Src/PiperRenderer.cpp:113-124), in
+    float32 arithmetic."""
+    hp, hy, hr = f32(0.5) * f32(pitch), f32(0.5) * f32(yaw), f32(0.5) * f32(roll)
+    cp, sp = f32(np.cos(hp)), f32(np.sin(hp))
+    cy, sy = f32(np.cos(hy)), f32(np.sin(hy))
+    cr, sr = f32(np.cos(hr)), f32(np.sin(hr))
+    return (float(cr * cp * cy + sr * sp * sy), float(cr * sp * cy + sr * cp * sy),
+            float(cr * cp * sy - sr * sp * cy), float(sr * cp * cy - cr * sp * sy))
+
+
+def srt(translation=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0), quat=(1.0, 0.0, 0.0, 0.0), skew=(0.0, 0.0, 0.0),
+        shift=(0.0, 0.0, 0.0)) -> capi.SRT:
+    t = capi.SRT()
+    sc = [scale] * 3 if np.isscalar(scale) else list(scale)
+    t.scale[:] = [float(x) for x in sc]
+    t.skew[:] = [float(x) for x in skew]
+    t.shift[:] = [float(x) for x in shift]
+    t.quat[:] = [float(x) for x in quat]
+    t.translation[:] = [float(x) for x in translation]
+    return t
+
+
+def srt_matrix(transform: capi.SRT | None = None, **kw) -> np.ndarray:
+    """The (12,) float32 row-major 3x4 local-to-world matrix of an SRT transform (pb2_srt_matrix); keyword
+    arguments build the SRT as :func:`srt` does."""
+    t = transform if transform is not None else srt(**kw)
+    m = np.zeros(12, np.float32)
+    capi.check(capi.lib().pb2_srt_matrix(C.byref(t), m.ctypes.data_as(C.POINTER(C.c_float))))
+    return m
+
+
+def plane_transform(plane: capi.Plane, matrix) -> capi.Plane:
+    m = np.ascontiguousarray(matrix, dtype=np.float32).reshape(12)
+    out = capi.Plane()
+    capi.check(capi.lib().pb2_plane_transform(C.byref(plane), m.ctypes.data_as(C.POINTER(C.c_float)), C.byref(out)))
+    return out
+
+
 def camera_from_config(position, look_at, up, sensor_size_mm, focal_length_mm, fstop) -> capi.Camera:
     """PerspectiveCamera config keys -> camera payload (PerspectiveCamera.cpp:39-44): sizes in mm
     times 1e-3f, up normalised, aperture radius = focal / (2 FStop)."""
@@ -75,6 +116,7 @@ class MeshData:
     indices: np.ndarray   # (T, 3) uint32
     material: int
     translation: tuple = (0.0, 0.0, 0.0)
+    transform: np.ndarray | None = None  # (12,) float32 row-major 3x4 local-to-world, or None
 
 
 @dataclass
@@ -106,6 +148,12 @@ class SceneData:
             meshes[i].tri_count = ix.shape[0]
             meshes[i].material = m.material
             meshes[i].translation[:] = [float(x) for x in m.translation]
+            if m.transform is not None:
+                t = np.ascontiguousarray(m.transform, dtype=np.float32).reshape(12)
+                keep.append(t)
+                meshes[i].transform = t.ctypes.data
+            else:
+                meshes[i].transform = None
         planes = (capi.Plane * max(1, len(self.planes)))(*self.planes)
         lights = (capi.AreaLight * max(1, len(self.area_lights)))()
         for i, (rad, first, count, tr) in enumerate(self.area_lights):
@@ -208,6 +256,45 @@ def cornell_box(seed: int = 0, width: int = 256, height: int = 256, spp: int = 1
     cam = camera_from_config((0.5, 0.5, -1.4), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), (sensor_mm, sensor_mm), focal_mm,
                              1e30)
     sd.settings = render_settings(width, height, spp, max_depth, min_rr_depth, cam)
+    return sd
+
+
+def _unit_cube():
+    """The cube [-0.5, 0.5] x [0, 1] x [-0.5, 0.5] (12 triangles, outward winding as :func:`_box`)."""
+    return _box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 0.0)
+
+
+def instanced_room(seed: int = 0, width: int = 64, height: int = 64, spp: int = 8, max_depth: int = 8,
+                   min_rr_depth: int = 3, light_tilt: float = 0.35) -> SceneData:
+    """The Cornell room with its boxes as instances of one unit cube under full SRT transforms (scale, a
+    rotation about a tilted axis, skew, translation) and the ceiling light tilted by `light_tilt` radians about
+    the x axis through its centre: geometry the reference can only render correctly with rotations baked into the
+    vertices.  Materials: white Matte walls, a Plastic box and a rough Glass box."""
+    rng = np.random.default_rng(seed)
+    sd = cornell_box(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, min_rr_depth=min_rr_depth)
+    sd.name = f"instanced_room(seed={seed})"
+    sd.meshes = sd.meshes[:5]
+    sd.materials.append(material("Plastic", (0.4, 0.3, 0.6), (0.5, 0.5, 0.5), (0.25, 0.0)))
+    sd.materials.append(material("Glass", (1, 1, 1), (1, 1, 1), (0.15, 0.15)))
+    v, ix = _unit_cube()
+    v = v.astype(np.float32)
+    for k, (center, size) in enumerate((((0.68, 0.0, 0.35), (0.28, 0.28, 0.28)),
+                                        ((0.33, 0.02, 0.65), (0.26, 0.5, 0.22)))):
+        axis = rng.normal(size=3) * (0.3, 1.0, 0.3)
+        axis /= np.linalg.norm(axis)
+        ang = rng.uniform(-0.6, 0.6)
+        q = (math.cos(ang / 2), *(math.sin(ang / 2) * axis))
+        skew = (rng.uniform(-0.1, 0.1), 0.0, rng.uniform(-0.1, 0.1))
+        m = srt_matrix(translation=center, scale=size, quat=q, skew=skew)
+        sd.meshes.append(MeshData(v, ix, 3 + k, transform=m))
+    c = np.array([0.5, 0.95, 0.5], np.float32)
+    light = plane_make((0.375, 0.95, 0.375), (0.25, 0.0, 0.0), (0.0, 0.0, 0.25))
+    # rotate about the x axis through the light's centre: T(c) R T(-c)
+    qa = (math.cos(light_tilt / 2), math.sin(light_tilt / 2), 0.0, 0.0)
+    r = srt_matrix(quat=qa).reshape(3, 4)
+    t = c - r[:, :3] @ c
+    m = np.concatenate([r[:, :3], t[:, None].astype(np.float32)], axis=1).astype(np.float32)
+    sd.planes = [plane_transform(light, m)]
     return sd
 
 
