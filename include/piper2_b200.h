@@ -119,7 +119,29 @@ typedef struct pb2_material {
     float color0[4];
     float color1[4];
     float roughness[2];
-} pb2_material; /* 44 bytes */
+    /* Per parameter (color0, color1, roughness[0], roughness[1]): 0 takes the constant above (ConstantTexture),
+     * k > 0 samples pb2_scene.textures[k - 1] at the hit's texture coordinate instead.  A color takes a 4-channel
+     * texture, a roughness a 1-channel one (the reference's loadTexture(desc, 4 / 1), Surface/Classic/Classic.cpp). */
+    uint32_t texture[4];
+} pb2_material; /* 60 bytes */
+
+/* Textures a material parameter can sample.  The texture coordinate of a triangle hit is the barycentric blend of
+ * its mesh's texcoords (calcTriangleMeshSurface, Src/BuiltinComponent/Tracer/Embree/Kernel.cpp:170-192), (0, 0)
+ * for a mesh without them. */
+enum pb2_texture_kind {
+    PB2_TEXTURE_CHECKERBOARD = 1, /* CheckBoard (Texture/ProceduralTexture/Kernel.cpp:27-38): `scale`, `black`, `white` */
+    PB2_TEXTURE_IMAGE = 2         /* SampledTexture (Texture/SampledTexture/Kernel.cpp:59-83): bilinear over 8-bit texels */
+};
+enum pb2_texture_wrap { PB2_WRAP_REPEAT = 0, PB2_WRAP_MIRROR = 1 };
+typedef struct pb2_texture {
+    uint32_t kind;
+    uint32_t channel;        /* 1, 2 or 4 */
+    uint32_t wrap;           /* image: pb2_texture_wrap */
+    uint32_t width, height;  /* image: texels, rows of width * channel bytes, top row first */
+    const uint8_t* texels;   /* image: host memory, copied to the device when the pipeline is created */
+    float scale;             /* checkerboard */
+    float black[4], white[4];
+} pb2_texture;
 
 /* Perspective camera (Src/BuiltinComponent/Sensor/PerspectiveCamera/Shared.hpp:22-29, config parse
  * PerspectiveCamera.cpp:35-46).  `position` is the camera node's translation (the reference reads it
@@ -144,6 +166,8 @@ typedef struct pb2_scene {
     const pb2_material* materials;
     uint32_t material_count;
     float env_radiance[3]; /* the single "SampledEnvironment" light, lights[0] (Embree.cpp:1174-1188) */
+    const pb2_texture* textures;
+    uint32_t texture_count;
 } pb2_scene;
 
 /* ---- render settings (component configs) -------------------------------------------------- */

@@ -28,11 +28,12 @@ _ref = None
 
 
 def _load(path):
-    if not os.path.exists(path):
-        sys.path.insert(0, HERE)
-        from build_oracle import build_oracle as _b
+    # (re)build when missing or older than its sources (a no-op otherwise): the library reads the C ABI's structs,
+    # so a stale build would misread them
+    sys.path.insert(0, HERE)
+    from build_oracle import build_oracle as _b
 
-        _b()
+    _b()
     return C.CDLL(path)
 
 
@@ -50,6 +51,11 @@ def oracle():
         h.or_sobol_digest.restype = C.c_char_p
         h.or_remap_roughness.restype = C.c_float
         h.or_remap_roughness.argtypes = [C.c_float]
+        h.or_logf.restype = C.c_float
+        h.or_logf.argtypes = [C.c_float]
+        h.or_remap_roughness_point.restype = C.c_float
+        h.or_remap_roughness_point.argtypes = [C.c_float]
+        h.or_texture_sample.argtypes = [C.POINTER(capi.Texture), C.c_float, C.c_float, C.POINTER(C.c_float)]
         h.or_camera_ray.argtypes = [C.POINTER(capi.Camera), C.c_float, C.c_float, C.c_float, C.c_float,
                                     C.POINTER(capi.Ray)]
         h.or_scene_create.restype = C.c_void_p
@@ -104,6 +110,10 @@ def ref_available() -> bool:
 def ref():
     global _ref
     if _ref is None:
+        sys.path.insert(0, HERE)
+        from build_oracle import build_ref as _br
+
+        _br()  # rebuilds a stale library when the reference sources are at hand (PIPER2_REFERENCE), else no-op
         if not os.path.exists(REF_SO):
             raise FileNotFoundError(f"{REF_SO} not built (needs the reference sources)")
         h = C.CDLL(REF_SO)

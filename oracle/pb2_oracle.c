@@ -143,6 +143,8 @@ static real remap_roughness(real roughness) {
     return R_FMAX(1e-3f, 1.62142f + (0.819955f + (0.1734f + (0.0171201f + 0.000640711f * x) * x) * x) * x);
 }
 float or_remap_roughness(float roughness) { return (float)remap_roughness(roughness); }
+float or_logf(float x) { return pb2_logf(x); }
+float or_remap_roughness_point(float roughness) { return pb2_remap_roughness(roughness); }
 
 /* Plane construction (Src/BuiltinComponent/Geometry/BasicShapes/BasicShapes.cpp:70-89) */
 void or_plane_make(const float origin[3], const float u[3], const float v[3], pb2_plane* out) {
@@ -261,6 +263,9 @@ struct or_scene {
     uint32_t nmat;
     pb2_material* mats;
     real* alpha;        /* remapped roughness x, y per material */
+    uint32_t ntex;
+    pb2_texture* tex;   /* texels copied */
+    float* tri_uv;      /* 6 floats per triangle: the texcoords of its vertices in index order, or NULL */
     spec env;
     /* BVH */
     or_node* nodes;
@@ -764,6 +769,35 @@ or_scene* or_scene_create(const pb2_scene* d, int use_bvh) {
             s->alpha[2 * m + 1] = remap_roughness(mt->roughness[1]);
         }
     }
+    s->ntex = d->texture_count;
+    s->tex = (pb2_texture*)calloc(d->texture_count ? d->texture_count : 1, sizeof(pb2_texture));
+    for (uint32_t i = 0; i < d->texture_count; ++i) {
+        s->tex[i] = d->textures[i];
+        if (d->textures[i].kind == PB2_TEXTURE_IMAGE) {
+            const size_t n = (size_t)d->textures[i].width * d->textures[i].height * d->textures[i].channel;
+            uint8_t* copy = (uint8_t*)malloc(n ? n : 1);
+            memcpy(copy, d->textures[i].texels, n);
+            s->tex[i].texels = copy;
+        }
+    }
+    s->tri_uv = NULL;
+    int textured = 0;
+    for (uint32_t m = 0; m < d->material_count; ++m)
+        for (int k = 0; k < 4; ++k) textured |= d->materials[m].texture[k] != 0;
+    if (textured) {
+        s->tri_uv = (float*)calloc(6 * (nt ? nt : 1), sizeof(float));
+        uint64_t q = 0;
+        for (uint32_t m = 0; m < d->mesh_count; ++m) {
+            const pb2_mesh* mesh = &d->meshes[m];
+            for (uint32_t i = 0; i < mesh->tri_count; ++i, ++q)
+                if (mesh->texcoords)
+                    for (int j = 0; j < 3; ++j) {
+                        const uint32_t vi = mesh->indices[3 * i + j];
+                        s->tri_uv[6 * q + 2 * j] = mesh->texcoords[2 * vi];
+                        s->tri_uv[6 * q + 2 * j + 1] = mesh->texcoords[2 * vi + 1];
+                    }
+        }
+    }
     s->env = mksp(d->env_radiance[0], d->env_radiance[1], d->env_radiance[2]);
     if (use_bvh && s->ntri > 0) build_bvh(s);
     return s;
@@ -773,6 +807,9 @@ void or_scene_destroy(or_scene* s) {
     if (!s) return;
     free(s->tri); free(s->tri_mat); free(s->planes); free(s->plane_light); free(s->plane_cdf);
     free(s->plane_pdf); free(s->lights); free(s->mats); free(s->alpha); free(s->nodes); free(s->order);
+    for (uint32_t i = 0; i < s->ntex; ++i)
+        if (s->tex[i].kind == PB2_TEXTURE_IMAGE) free((void*)s->tex[i].texels);
+    free(s->tex); free(s->tri_uv);
     free(s);
 }
 
@@ -788,6 +825,7 @@ typedef struct surf_info {
     int front;
     uint32_t material;
     uint32_t light; /* area light index */
+    float tu, tv;   /* texture coordinate (triangles of a textured scene) */
 } surf_info;
 
 /* piperEmbreeTrace (Src/BuiltinComponent/Tracer/Embree/Embree.cpp:267-355) with
@@ -831,6 +869,14 @@ static void trace_surface(const or_scene* s, v3 o, v3 d, real tmin, real tmax, s
     else
         si->T = cross3(si->N, e2);
     si->B = cross3(si->N, si->T);
+    /* calcTriangleMeshSurface's texCoord (Tracer/Embree/Kernel.cpp:181-190): tc[i1] u + tc[i2] v + tc[i0] w */
+    si->tu = si->tv = 0.0f;
+    if (s->tri_uv) {
+        const float* q = s->tri_uv + 6 * (size_t)h.prim;
+        const real w = (1.0f - h.u) - h.v;
+        si->tu = (float)((q[2] * h.u + q[4] * h.v) + q[0] * w);
+        si->tv = (float)((q[3] * h.u + q[5] * h.v) + q[1] * w);
+    }
 }
 
 static int occluded(const or_scene* s, v3 o, v3 d, real tmin, real tmax, uint64_t* nrays) {
@@ -1226,11 +1272,42 @@ static void lobe_sample(const lobe* L, real u1, real u2, v3 wo, bsdf_sample* res
 
 /* Surface init (matteInit :249-268, plasticInit :441-470, glassInit :613-656, mirrorInit :668-677,
  * substrateInit :755-778, blackBodyInit :45-48).  Lobe order = the KERNEL_FUNCTION_GROUP order. */
-static void bsdf_init(const or_scene* s, uint32_t mat, int front, bsdf* b) {
-    const pb2_material* m = &s->mats[mat];
+/* The material's textured parameters at (tu, tv) (CheckBoard, ProceduralTexture/Kernel.cpp:27-38; SampledTexture,
+ * SampledTexture/Kernel.cpp:59-83); a textured roughness is remapped per point with pb2_logf. */
+static void texture_value(const pb2_texture* t, float tu, float tv, float* out) {
+    if (t->kind == PB2_TEXTURE_IMAGE) {
+        pb2_tex_sample(t->texels, t->width, t->height, t->channel, t->wrap, tu, tv, out);
+    } else {
+        const float* arr = pb2_checker_white(tu, tv, t->scale) ? t->white : t->black;
+        for (uint32_t i = 0; i < t->channel; ++i) out[i] = arr[i];
+    }
+}
+
+void or_texture_sample(const pb2_texture* t, float tu, float tv, float* out) { texture_value(t, tu, tv, out); }
+
+static void bsdf_init(const or_scene* s, uint32_t mat, int front, float tu, float tv, bsdf* b) {
+    pb2_material mm = s->mats[mat];
+    const pb2_material* m = &mm;
+    real ax = s->alpha[2 * mat], ay = s->alpha[2 * mat + 1];
+    for (int k = 0; k < 4; ++k) {
+        if (!mm.texture[k]) continue;
+        float v[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+        texture_value(&s->tex[mm.texture[k] - 1], tu, tv, v);
+        if (k == 0) { mm.color0[0] = v[0]; mm.color0[1] = v[1]; mm.color0[2] = v[2]; }
+        if (k == 1) { mm.color1[0] = v[0]; mm.color1[1] = v[1]; mm.color1[2] = v[2]; }
+        if (k == 2) {
+            mm.roughness[0] = v[0];
+            if (mm.type == PB2_SURFACE_CONDUCTOR) ax = ay = v[0];
+            else if (mm.type == PB2_SURFACE_PLASTIC) ax = ay = pb2_remap_roughness(v[0]);
+            else ax = pb2_remap_roughness(v[0]);
+        }
+        if (k == 3) {
+            mm.roughness[1] = v[0];
+            if (mm.type != PB2_SURFACE_CONDUCTOR && mm.type != PB2_SURFACE_PLASTIC) ay = pb2_remap_roughness(v[0]);
+        }
+    }
     const spec c0 = mksp(m->color0[0], m->color0[1], m->color0[2]);
     const spec c1 = mksp(m->color1[0], m->color1[1], m->color1[2]);
-    const real ax = s->alpha[2 * mat], ay = s->alpha[2 * mat + 1];
     memset(b, 0, sizeof(*b));
     switch (m->type) {
         case PB2_SURFACE_MATTE: {
@@ -1594,7 +1671,7 @@ static spec trace_path(path_ctx* c, const pb2_render_settings* st, v3 o, v3 d, u
         const v3 wo = to_shading(&si, neg3(d));
         const v3 ng_sh = to_shading(&si, si.Ng);
         bsdf b;
-        bsdf_init(s, si.material, si.front, &b);
+        bsdf_init(s, si.material, si.front, si.tu, si.tv, &b);
         const v3 hit = add3(o, mul3s(d, si.t));
         if (b.no_specular) sample = sp_add(sample, sp_mul(pf, mis(c, hit, &b, wo, &si, ng_sh)));
         bsdf_sample ss;
@@ -1655,7 +1732,7 @@ static void splat(const pb2_render_settings* st, float* rgbw, float px, float py
 void or_bsdf_sample(const or_scene* s, uint32_t mat, int front, const float wo_in[3], uint32_t n, const float* u,
                     float* wi, float* f, float* pdf) {
     bsdf b;
-    bsdf_init(s, mat, front, &b);
+    bsdf_init(s, mat, front, 0.0f, 0.0f, &b);
     const v3 wo = mk3(wo_in[0], wo_in[1], wo_in[2]);
     const v3 ng = mk3(0.0f, 0.0f, 1.0f);
     for (uint32_t i = 0; i < n; ++i) {
@@ -1672,7 +1749,7 @@ void or_bsdf_sample(const or_scene* s, uint32_t mat, int front, const float wo_i
 void or_bsdf_eval(const or_scene* s, uint32_t mat, int front, const float wo_in[3], uint32_t n, const float* wi,
                   float* f, float* pdf) {
     bsdf b;
-    bsdf_init(s, mat, front, &b);
+    bsdf_init(s, mat, front, 0.0f, 0.0f, &b);
     const v3 wo = mk3(wo_in[0], wo_in[1], wo_in[2]);
     const v3 ng = mk3(0.0f, 0.0f, 1.0f);
     for (uint32_t i = 0; i < n; ++i) {

@@ -32,6 +32,11 @@ void or_sobol_start(uint32_t resolution, uint32_t log2_resolution, uint32_t px, 
 const char* or_sobol_digest(void);
 
 float or_remap_roughness(float roughness);
+/* pb2_logf and the per-point roughness remap of a textured roughness (checks of the shared math) */
+float or_logf(float x);
+float or_remap_roughness_point(float roughness);
+/* A texture's value at (tu, tv): CheckBoard or the bilinear SampledTexture, out[0..channel). */
+void or_texture_sample(const pb2_texture* t, float tu, float tv, float* out);
 void or_camera_ray(const pb2_camera* cam, float ndc_x, float ndc_y, float u1, float u2, pb2_ray* ray);
 
 /* Scene: flattens meshes (translation baked in) and builds a BVH if use_bvh != 0. */

@@ -68,6 +68,8 @@ void planeSurface(RestrictedContext, const void*, const void*, SurfaceIntersecti
 void planeSample(RestrictedContext, const void*, const Point<Distance, FOR::World>&, float, float, Point<Distance, FOR::World>&,
                  Normal<float, FOR::World>&, Dimensionless<float>&);
 void constantTexture(RestrictedContext, const void*, const Vector2<float>&, Dimensionless<float>*);
+void checkBoard(RestrictedContext, const void*, const Vector2<float>&, Dimensionless<float>*);
+void sampleTexture(RestrictedContext, const void*, const Vector2<float>&, Dimensionless<float>*);
 void calcTriangleMeshSurface(RestrictedContext, const void*, const void*, SurfaceIntersectionInfo&);
 void piperMain(TaskContext ctx);
 #define SURFACE_DECL(P)                                                                                          \
@@ -208,6 +210,34 @@ struct RefScene {
         for (uint32_t i = 0; i < channel; ++i) d.value[i].val = v[i];
         return call(&constantTexture, payload(d));
     }
+    /* The payload of the SampledTexture kernel (its Data, Texture/SampledTexture/Shared.hpp:22-30; a struct of the
+     * same name in the PathTracing header keeps it from being included beside the others). */
+    struct SampledTextureData {
+        TextureWrap wrap;
+        uint32_t width, height, stride, channel, texel;
+        StatisticsHandle profileSample;
+    };
+    /* A material parameter: its constant, or the scene texture it names (CheckBoard / SampledTexture). */
+    CallHandle texture(const pb2_scene* d, uint32_t index, const float* v, uint32_t channel) {
+        if (!index) return constant(v, channel);
+        const pb2_texture& t = d->textures[index - 1];
+        if (t.kind == PB2_TEXTURE_CHECKERBOARD) {
+            CheckBoardData c{};
+            c.scale = t.scale;
+            c.channel = t.channel;
+            for (uint32_t i = 0; i < 4; ++i) { c.black[i].val = t.black[i]; c.white[i].val = t.white[i]; }
+            return call(&checkBoard, payload(c));
+        }
+        SampledTextureData sd{};
+        sd.wrap = t.wrap ? TextureWrap::Mirror : TextureWrap::Repeat;
+        sd.width = t.width;
+        sd.height = t.height;
+        sd.stride = t.width * t.channel;
+        sd.channel = t.channel;
+        sd.texel = resource(const_cast<uint8_t*>(t.texels));
+        sd.profileSample = nullptr;
+        return call(&sampleTexture, payload(sd));
+    }
     ~RefScene() {
         if (oracle) or_scene_destroy(oracle);
         for (auto* n : nodes) delete n;
@@ -311,30 +341,34 @@ extern "C" void* ref_scene_create(const pb2_scene* d, const pb2_render_settings*
         SurfaceCalls& c = surf[m];
         switch (mt.type) {
             case PB2_SURFACE_MATTE: {
-                const MatteData* p = S->payload(MatteData{ { S->constant(mt.color0, 4) }, { S->constant(mt.roughness, 1) } });
+                const MatteData* p = S->payload(MatteData{ { S->texture(d, mt.texture[0], mt.color0, 4) },
+                                                           { S->texture(d, mt.texture[2], mt.roughness, 1) } });
                 c = { S->call(&matteInit, p), S->call(&matteSample, p), S->call(&matteEvaluate, p), S->call(&mattePdf, p) };
             } break;
             case PB2_SURFACE_PLASTIC: {
-                const PlasticData* p = S->payload(PlasticData{ { S->constant(mt.color0, 4) }, { S->constant(mt.color1, 4) },
-                                                              { S->constant(mt.roughness, 1) } });
+                const PlasticData* p = S->payload(PlasticData{ { S->texture(d, mt.texture[0], mt.color0, 4) },
+                                                              { S->texture(d, mt.texture[1], mt.color1, 4) },
+                                                              { S->texture(d, mt.texture[2], mt.roughness, 1) } });
                 c = { S->call(&plasticInit, p), S->call(&plasticSample, p), S->call(&plasticEvaluate, p),
                       S->call(&plasticPdf, p) };
             } break;
             case PB2_SURFACE_GLASS: {
-                const GlassData* p = S->payload(GlassData{ { S->constant(mt.color0, 4) }, { S->constant(mt.color1, 4) },
-                                                          { S->constant(&mt.roughness[0], 1) },
-                                                          { S->constant(&mt.roughness[1], 1) } });
+                const GlassData* p = S->payload(GlassData{ { S->texture(d, mt.texture[0], mt.color0, 4) },
+                                                          { S->texture(d, mt.texture[1], mt.color1, 4) },
+                                                          { S->texture(d, mt.texture[2], &mt.roughness[0], 1) },
+                                                          { S->texture(d, mt.texture[3], &mt.roughness[1], 1) } });
                 c = { S->call(&glassInit, p), S->call(&glassSample, p), S->call(&glassEvaluate, p), S->call(&glassPdf, p) };
             } break;
             case PB2_SURFACE_MIRROR: {
-                const MirrorData* p = S->payload(MirrorData{ { S->constant(mt.color0, 4) } });
+                const MirrorData* p = S->payload(MirrorData{ { S->texture(d, mt.texture[0], mt.color0, 4) } });
                 c = { S->call(&mirrorInit, p), S->call(&mirrorSample, p), S->call(&blackBodyEvaluate, p),
                       S->call(&blackBodyPdf, p) };
             } break;
             case PB2_SURFACE_SUBSTRATE: {
-                const SubstrateData* p = S->payload(SubstrateData{ { S->constant(mt.color0, 4) }, { S->constant(mt.color1, 4) },
-                                                                  { S->constant(&mt.roughness[0], 1) },
-                                                                  { S->constant(&mt.roughness[1], 1) } });
+                const SubstrateData* p = S->payload(SubstrateData{ { S->texture(d, mt.texture[0], mt.color0, 4) },
+                                                                  { S->texture(d, mt.texture[1], mt.color1, 4) },
+                                                                  { S->texture(d, mt.texture[2], &mt.roughness[0], 1) },
+                                                                  { S->texture(d, mt.texture[3], &mt.roughness[1], 1) } });
                 c = { S->call(&substrateInit, p), S->call(&substrateSample, p), S->call(&substrateEvaluate, p),
                       S->call(&substratePdf, p) };
             } break;

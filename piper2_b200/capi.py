@@ -60,7 +60,17 @@ class AreaLight(C.Structure):
 
 class Material(C.Structure):
     _fields_ = [("type", C.c_uint32), ("color0", C.c_float * 4), ("color1", C.c_float * 4),
-                ("roughness", C.c_float * 2)]
+                ("roughness", C.c_float * 2), ("texture", C.c_uint32 * 4)]
+
+
+class Texture(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("channel", C.c_uint32), ("wrap", C.c_uint32), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("texels", C.c_void_p), ("scale", C.c_float), ("black", C.c_float * 4),
+                ("white", C.c_float * 4)]
+
+
+TEXTURE_CHECKERBOARD, TEXTURE_IMAGE = 1, 2
+WRAP = {"Repeat": 0, "Mirror": 1}
 
 
 class Camera(C.Structure):
@@ -72,7 +82,7 @@ class Scene(C.Structure):
     _fields_ = [("meshes", C.POINTER(Mesh)), ("mesh_count", C.c_uint32), ("planes", C.POINTER(Plane)),
                 ("plane_count", C.c_uint32), ("area_lights", C.POINTER(AreaLight)), ("area_light_count", C.c_uint32),
                 ("materials", C.POINTER(Material)), ("material_count", C.c_uint32),
-                ("env_radiance", C.c_float * 3)]
+                ("env_radiance", C.c_float * 3), ("textures", C.POINTER(Texture)), ("texture_count", C.c_uint32)]
 
 
 class RenderSettings(C.Structure):
@@ -100,7 +110,7 @@ class LaunchStats(C.Structure):
                 ("path_vertices", C.c_uint64), ("depth_histogram", C.c_uint32 * 32)]
 
 
-assert C.sizeof(Plane) == 64 and C.sizeof(Material) == 44
+assert C.sizeof(Plane) == 64 and C.sizeof(Material) == 60
 
 
 class PB2Error(RuntimeError):

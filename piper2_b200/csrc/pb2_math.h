@@ -243,3 +243,95 @@ PB2_HD void pb2_mesh_vertex(const float* matrix, const float* translation, const
         for (int i = 0; i < 3; ++i) out[i] = p[i] + translation[i];
     }
 }
+
+/* ---- natural logarithm ------------------------------------------------------------------------------------
+ * For finite x > 0: x = m 2^e with m in [sqrt(1/2), sqrt(2)), log(m) = 2 atanh(s), s = (m - 1) / (m + 1)
+ * (|s| <= 0.1716), atanh(s) = s + s^3/3 + s^5/5 + ... to s^15 (truncation < 1e-13 relative), then
+ * e ln2 with ln2 in two parts (the constants of pb2_expf).  Used where a logarithm is evaluated per shading point (the roughness remap of a
+ * textured material) so that the device and the oracle agree bit for bit. */
+PB2_HD float pb2_logf(float x) {
+    union { float f; uint32_t u; } b;
+    b.f = x;
+    int e = 0;
+    if (b.u < 0x00800000u) { /* subnormal (x > 0 assumed): scale into the normal range */
+        b.f = x * 8388608.0f;
+        e = -23;
+    }
+    e += (int)(b.u >> 23) - 127;
+    b.u = (b.u & 0x007FFFFFu) | 0x3F800000u; /* m in [1, 2) */
+    float m = b.f;
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = 0.0666666667f;               /* 1/15 */
+    p = PB2_FMA(p, s2, 0.0769230769f);     /* 1/13 */
+    p = PB2_FMA(p, s2, 0.0909090909f);     /* 1/11 */
+    p = PB2_FMA(p, s2, 0.111111111f);      /* 1/9 */
+    p = PB2_FMA(p, s2, 0.142857143f);      /* 1/7 */
+    p = PB2_FMA(p, s2, 0.2f);              /* 1/5 */
+    p = PB2_FMA(p, s2, 0.333333333f);      /* 1/3 */
+    const float lm = 2.0f * PB2_FMA(s * s2, p, s);
+    const float fe = (float)e;
+    return PB2_FMA(fe, PB2_LN2_HI, PB2_FMA(fe, PB2_LN2_LO, lm));
+}
+
+/* MicrofacetDistribution::remapRoughness (Src/BuiltinComponent/Surface/Classic/Kernel.cpp:378-381) with pb2_logf:
+ * the per-point form for textured roughness (a constant roughness is remapped once on the host with the C
+ * library's log, as the reference does). */
+PB2_HD float pb2_remap_roughness(float roughness) {
+    const float x = pb2_logf(fmaxf(1e-3f, roughness));
+    return fmaxf(1e-3f, 1.62142f + (0.819955f + (0.1734f + (0.0171201f + 0.000640711f * x) * x) * x) * x);
+}
+
+/* ---- textures ---------------------------------------------------------------------------------------------
+ * CheckBoard (Src/BuiltinComponent/Texture/ProceduralTexture/Kernel.cpp:27-38) and the bilinear SampledTexture
+ * (Texture/SampledTexture/Kernel.cpp:22-83), including its wrap arithmetic: IEEE remainder, "Mirror" folding into
+ * [0, size/2] (fabs of the remainder), the last texel repeated at the edge of a mirrored axis, 8-bit texels scaled
+ * by 0.003921568f.  remainderf is exact on both sides. */
+PB2_HD float pb2_checker_mod(float x, float scale) {
+    const float r = remainderf(x * scale, 2.0f);
+    return r < 0.0f ? r + 2.0f : r;
+}
+
+PB2_HD int pb2_checker_white(float u, float v, float scale) {
+    return (pb2_checker_mod(u, scale) > 1.0f) == (pb2_checker_mod(v, scale) > 1.0f);
+}
+
+PB2_HD uint32_t pb2_tex_locate(float p, uint32_t size, uint32_t mirror) {
+    const float mod = (float)size;
+    float s = remainderf(p, mod);
+    if (mirror) s = fabsf(s);
+    else if (s < 0.0f) s = s + mod;
+    if (!(s >= 0.0f)) s = 0.0f; /* a NaN coordinate */
+    const uint32_t i = s < 4294967040.0f ? (uint32_t)s : 0xFFFFFFFFu;
+    return i < size - 1u ? i : size - 1u;
+}
+
+PB2_HD uint32_t pb2_tex_next(uint32_t p, uint32_t size, uint32_t mirror) {
+    const uint32_t s = p + 1u;
+    return s == size ? (mirror ? p : 0u) : s;
+}
+
+PB2_HD float pb2_tex_left_weight(float u) { return (0.5f + floorf(u + 0.5f)) - u; }
+
+/* Bilinear lookup of `channel` 8-bit channels at texture coordinate (tu, tv); out[0..channel). */
+PB2_HD void pb2_tex_sample(const uint8_t* texels, uint32_t width, uint32_t height, uint32_t channel, uint32_t mirror,
+                           float tu, float tv, float* out) {
+    const uint32_t stride = width * channel;
+    const float u = tu * (float)width, v = tv * (float)height;
+    const uint32_t plu = pb2_tex_locate(u - 0.5f, width, mirror), pru = pb2_tex_next(plu, width, mirror);
+    const uint32_t plv = pb2_tex_locate(v - 0.5f, height, mirror), prv = pb2_tex_next(plv, height, mirror);
+    const float lwx = pb2_tex_left_weight(u), lwy = pb2_tex_left_weight(v);
+    const float rwx = 1.0f - lwx, rwy = 1.0f - lwy;
+    const uint32_t cu[4] = { plu, pru, plu, pru }, cv[4] = { plv, plv, prv, prv };
+    const float w[4] = { lwx * lwy, rwx * lwy, lwx * rwy, rwx * rwy };
+    for (uint32_t i = 0; i < channel; ++i) out[i] = 0.0f;
+    for (int c = 0; c < 4; ++c) {
+        const uint32_t idx = cv[c] * stride + cu[c] * channel;
+        for (uint32_t i = 0; i < channel; ++i) out[i] = out[i] + w[c] * (float)texels[idx + i];
+    }
+    for (uint32_t i = 0; i < channel; ++i) out[i] = out[i] * 0.003921568f;
+}

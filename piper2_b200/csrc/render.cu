@@ -185,6 +185,8 @@ struct LaunchParams {
 
 struct SceneView {
     const DevMaterial* materials;
+    const DevTexture* textures;
+    const float2* tri_uv;  // texture coordinates of each primitive's three vertices (index order), if textured
     const uint32_t* prim_material;
     const DevLight* lights;
     const float* plane_cdf;
@@ -809,7 +811,19 @@ __global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs
         const v3 wo = to_shading(fr, neg3(d));
         const v3 ng_sh = to_shading(fr, fr.Ng);
         Bsdf bsdf;
-        bsdf_init<kType>(sv.materials[sv.prim_material[prim]], front, bsdf);
+        DevMaterial mat = sv.materials[sv.prim_material[prim]];
+        if (mat.tex[0] | mat.tex[1] | mat.tex[2] | mat.tex[3]) {
+            // calcTriangleMeshSurface's texCoord (Tracer/Embree/Kernel.cpp:181-190): tc[i1] u + tc[i2] v + tc[i0] w
+            float tu = 0.0f, tv = 0.0f;
+            if (sv.tri_uv) {
+                const float2* q = sv.tri_uv + 3 * (size_t)prim;
+                const float bw = (1.0f - h.z) - h.w;
+                tu = (q[1].x * h.z + q[2].x * h.w) + q[0].x * bw;
+                tv = (q[1].y * h.z + q[2].y * h.w) + q[0].y * bw;
+            }
+            apply_textures(mat, sv.textures, tu, tv);
+        }
+        bsdf_init<kType>(mat, front, bsdf);
         const v3 hit = add3(o, mul3s(d, h.x));
         uint32_t flags = 0;
         if (bsdf.no_specular) {
@@ -1290,6 +1304,9 @@ struct pb2_pipeline {
     pb2_ndc_transform ndc{};
     uint32_t log2res = 0;
     DevMaterial* materials = nullptr;
+    DevTexture* textures = nullptr;
+    uint8_t* texels = nullptr;
+    float2* tri_uv = nullptr;
     DevLight* lights = nullptr;
     float* plane_cdf = nullptr;
     float* plane_pdf = nullptr;
@@ -1407,9 +1424,101 @@ static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
     return alloc_path_state(&pl->state, &pl->capacity, &pl->ps, cap, true);
 }
 
+// The scene's textures and the materials' references to them: kinds, channels (a color takes 4, a roughness 1, as
+// the reference's loadTexture(desc, 4 / 1) demands, Surface/Classic/Classic.cpp), image sizes and texels.
+static int check_textures(const pb2_scene* scene) {
+    if (scene->texture_count && !scene->textures) return fail(PB2_ERR_INVALID_ARGUMENT, "textures: null array");
+    for (uint32_t i = 0; i < scene->texture_count; ++i) {
+        const pb2_texture& t = scene->textures[i];
+        const std::string name = "texture " + std::to_string(i);
+        if (t.channel != 1 && t.channel != 2 && t.channel != 4)
+            return fail(PB2_ERR_INVALID_ARGUMENT, name + ": channel must be 1, 2 or 4");
+        if (t.kind == PB2_TEXTURE_IMAGE) {
+            if (!t.width || !t.height || !t.texels || t.wrap > PB2_WRAP_MIRROR)
+                return fail(PB2_ERR_INVALID_ARGUMENT, name + ": an image needs a size, texels and a wrap mode");
+            if ((uint64_t)t.width * t.height * t.channel > 0xFFFFFFFFull)
+                return fail(PB2_ERR_NOT_SUPPORTED, name + ": more than 2^32 bytes of texels");
+        } else if (t.kind != PB2_TEXTURE_CHECKERBOARD) {
+            return fail(PB2_ERR_INVALID_ARGUMENT, name + ": unknown kind");
+        }
+    }
+    static const char* params[4] = { "color0", "color1", "roughness[0]", "roughness[1]" };
+    for (uint32_t m = 0; m < scene->material_count; ++m)
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t ti = scene->materials[m].texture[k];
+            if (!ti) continue;
+            const std::string where = "material " + std::to_string(m) + " " + params[k];
+            if (ti > scene->texture_count) return fail(PB2_ERR_INVALID_ARGUMENT, where + ": texture index out of range");
+            const uint32_t want = k < 2 ? 4u : 1u;
+            if (scene->textures[ti - 1].channel != want)
+                return fail(PB2_ERR_INVALID_ARGUMENT, where + ": mismatched channel, expect " + std::to_string(want) +
+                                                          ", but get " + std::to_string(scene->textures[ti - 1].channel));
+        }
+    return PB2_OK;
+}
+
 static float remap_roughness(float roughness) {
     const float x = std::log(std::fmax(1e-3f, roughness));
     return std::fmax(1e-3f, 1.62142f + (0.819955f + (0.1734f + (0.0171201f + 0.000640711f * x) * x) * x) * x);
+}
+
+// Textures (texels pooled in one device buffer) and, when a material samples one, each triangle's three texture
+// coordinates in index order ((0, 0) for a mesh without texcoords).  The upload is stream-ordered; the caller
+// synchronises before the host vectors go out of scope.
+static int upload_textures(pb2_pipeline* pl, const pb2_scene* scene, cudaStream_t stream) {
+    bool textured = false;
+    for (uint32_t m = 0; m < scene->material_count; ++m)
+        for (int k = 0; k < 4; ++k) textured |= scene->materials[m].texture[k] != 0;
+    if (!textured) return PB2_OK;
+    size_t bytes = 0;
+    std::vector<size_t> offset(scene->texture_count, 0);
+    for (uint32_t i = 0; i < scene->texture_count; ++i) {
+        const pb2_texture& t = scene->textures[i];
+        if (t.kind != PB2_TEXTURE_IMAGE) continue;
+        offset[i] = bytes;
+        bytes += ((size_t)t.width * t.height * t.channel + 15) & ~(size_t)15;
+    }
+    cudaError_t e;
+    if (bytes && (e = cudaMalloc(&pl->texels, bytes))) return cuda_fail(e, "texel upload");
+    std::vector<DevTexture> dev(scene->texture_count ? scene->texture_count : 1);
+    for (uint32_t i = 0; i < scene->texture_count; ++i) {
+        const pb2_texture& t = scene->textures[i];
+        DevTexture& d = dev[i];
+        std::memset(&d, 0, sizeof(d));
+        d.kind = t.kind;
+        d.channel = t.channel;
+        d.wrap = t.wrap;
+        d.width = t.width;
+        d.height = t.height;
+        d.scale = t.scale;
+        for (int k = 0; k < 4; ++k) { d.black[k] = t.black[k]; d.white[k] = t.white[k]; }
+        if (t.kind == PB2_TEXTURE_IMAGE) {
+            d.texels = pl->texels + offset[i];
+            if ((e = cudaMemcpyAsync(pl->texels + offset[i], t.texels, (size_t)t.width * t.height * t.channel,
+                                     cudaMemcpyHostToDevice, stream)))
+                return cuda_fail(e, "texel upload");
+        }
+    }
+    uint64_t ntri = 0;
+    for (uint32_t m = 0; m < scene->mesh_count; ++m) ntri += scene->meshes[m].tri_count;
+    std::vector<float2> uv(3 * (ntri ? ntri : 1), make_float2(0.0f, 0.0f));
+    size_t k = 0;
+    for (uint32_t m = 0; m < scene->mesh_count; ++m) {
+        const pb2_mesh& me = scene->meshes[m];
+        for (uint32_t i = 0; i < me.tri_count; ++i, k += 3)
+            if (me.texcoords)
+                for (int j = 0; j < 3; ++j) {
+                    const uint32_t vi = me.indices[3 * i + j];
+                    uv[k + j] = make_float2(me.texcoords[2 * vi], me.texcoords[2 * vi + 1]);
+                }
+    }
+    if ((e = cudaMalloc(&pl->textures, sizeof(DevTexture) * dev.size())) ||
+        (e = cudaMalloc(&pl->tri_uv, sizeof(float2) * uv.size())) ||
+        (e = cudaMemcpyAsync(pl->textures, dev.data(), sizeof(DevTexture) * dev.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaMemcpyAsync(pl->tri_uv, uv.data(), sizeof(float2) * uv.size(), cudaMemcpyHostToDevice, stream)) ||
+        (e = cudaStreamSynchronize(stream)))
+        return cuda_fail(e, "texture upload");
+    return PB2_OK;
 }
 
 extern "C" {
@@ -1447,6 +1556,7 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
     if (st->filter > PB2_FILTER_GAUSSIAN) return fail(PB2_ERR_INVALID_ARGUMENT, "unknown filter");
     for (uint32_t m = 0; m < scene->material_count; ++m)
         if (scene->materials[m].type > PB2_SURFACE_CONDUCTOR) return fail(PB2_ERR_INVALID_ARGUMENT, "unknown surface type");
+    if (int rc = check_textures(scene)) return rc;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     auto* pl = new pb2_pipeline();
     int rc = pb2_accel_create(scene, stream_ptr, &pl->accel);
@@ -1509,6 +1619,7 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
         d.valid1 = s.color1[0] > 0.0f || s.color1[1] > 0.0f || s.color1[2] > 0.0f;
         d.roughness0 = s.roughness[0];
         d.roughness1 = s.roughness[1];
+        for (int k = 0; k < 4; ++k) d.tex[k] = s.texture[k];
         if (s.type == PB2_SURFACE_CONDUCTOR) {
             d.ax = d.ay = s.roughness[0];
         } else if (s.type == PB2_SURFACE_PLASTIC) {
@@ -1556,6 +1667,10 @@ int pb2_pipeline_create(const pb2_scene* scene, const pb2_render_settings* st, v
     if (scene->material_count == 0) pl->type_mask = (1u << kNumSurfaceTypes) - 1u;
     for (int k = 0; k < 3; ++k) pl->env[k] = scene->env_radiance[k];
     cudaError_t e;
+    if (int rt = upload_textures(pl, scene, stream)) {
+        pb2_pipeline_destroy(pl);
+        return rt;
+    }
     if ((e = cudaMalloc(&pl->materials, sizeof(DevMaterial) * mats.size())) ||
         (e = cudaMalloc(&pl->lights, sizeof(DevLight) * lights.size())) ||
         (e = cudaMalloc(&pl->plane_cdf, sizeof(float) * cdf.size())) ||
@@ -1585,6 +1700,9 @@ int pb2_pipeline_destroy(pb2_pipeline* pl) {
     if (!pl) return PB2_OK;
     pb2_accel_destroy(pl->accel);
     cudaFree(pl->materials);
+    cudaFree(pl->textures);
+    cudaFree(pl->texels);
+    cudaFree(pl->tri_uv);
     cudaFree(pl->lights);
     cudaFree(pl->plane_cdf);
     cudaFree(pl->plane_pdf);
@@ -1704,6 +1822,8 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     }
     SceneView sv;
     sv.materials = pl->materials;
+    sv.textures = pl->textures;
+    sv.tri_uv = pl->tri_uv;
     sv.prim_material = pl->accel->prim_material;
     sv.lights = pl->lights;
     sv.plane_cdf = pl->plane_cdf;
@@ -2295,6 +2415,8 @@ int pb2_batch_create(const pb2_scene* scenes, const pb2_render_settings* setting
         BatchScene sc{};
         sc.lp = make_params(pl, pl->full, 0, pl->settings.samples_per_pixel);
         sc.sv.materials = pl->materials;
+        sc.sv.textures = pl->textures;
+        sc.sv.tri_uv = pl->tri_uv;
         sc.sv.prim_material = pl->accel->prim_material;
         sc.sv.lights = pl->lights;
         sc.sv.plane_cdf = pl->plane_cdf;

@@ -61,7 +61,62 @@ struct DevMaterial {
     float on_a, on_b;  // Oren-Nayar A, B (Classic/Kernel.cpp:103-109)
     uint32_t valid0, valid1;
     float roughness0, roughness1;
+    uint32_t tex[4];  // color0, color1, roughness0, roughness1: 0 constant, k > 0 samples DevTexture k - 1
 };
+
+// A texture on the device: pb2_texture with the texels moved to device memory.
+struct DevTexture {
+    uint32_t kind, channel, wrap, width, height;
+    const uint8_t* texels;
+    float scale;
+    float black[4], white[4];
+};
+
+__device__ __forceinline__ void texture_sample(const DevTexture& t, float tu, float tv, float* out) {
+    if (t.kind == PB2_TEXTURE_IMAGE) {
+        pb2_tex_sample(t.texels, t.width, t.height, t.channel, t.wrap, tu, tv, out);
+    } else {
+        const float* arr = pb2_checker_white(tu, tv, t.scale) ? t.white : t.black;
+        for (uint32_t i = 0; i < t.channel; ++i) out[i] = arr[i];
+    }
+}
+
+// The material's textured parameters at texture coordinate (tu, tv), then what the surface init derives from them
+// per point (Classic/Kernel.cpp: the remapped roughness of plastic :459-462, glass :636-639 and substrate :770-772,
+// Oren-Nayar's A and B :103-109); parameters without a texture keep the values set up once on the host.
+__device__ __forceinline__ void apply_textures(DevMaterial& m, const DevTexture* tex, float tu, float tv) {
+    float v[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+    if (m.tex[0]) {
+        texture_sample(tex[m.tex[0] - 1], tu, tv, v);
+        m.c0[0] = v[0]; m.c0[1] = v[1]; m.c0[2] = v[2];
+        m.valid0 = v[0] > 0.0f || v[1] > 0.0f || v[2] > 0.0f;
+    }
+    if (m.tex[1]) {
+        texture_sample(tex[m.tex[1] - 1], tu, tv, v);
+        m.c1[0] = v[0]; m.c1[1] = v[1]; m.c1[2] = v[2];
+        m.valid1 = v[0] > 0.0f || v[1] > 0.0f || v[2] > 0.0f;
+    }
+    if (m.tex[2]) {
+        texture_sample(tex[m.tex[2] - 1], tu, tv, v);
+        m.roughness0 = v[0];
+        if (m.type == PB2_SURFACE_CONDUCTOR) {
+            m.ax = m.ay = v[0];
+        } else if (m.type == PB2_SURFACE_PLASTIC) {
+            m.ax = m.ay = pb2_remap_roughness(v[0]);
+        } else {
+            m.ax = pb2_remap_roughness(v[0]);
+        }
+        const float sigma = v[0] * 3.14159265358979323846f;
+        const float sigma2 = sigma * sigma;
+        m.on_a = 1.0f - (sigma2 / (2.0f * (sigma2 + 0.33f)));
+        m.on_b = 0.45f * sigma2 / (sigma2 + 0.09f);
+    }
+    if (m.tex[3]) {
+        texture_sample(tex[m.tex[3] - 1], tu, tv, v);
+        m.roughness1 = v[0];
+        if (m.type != PB2_SURFACE_CONDUCTOR && m.type != PB2_SURFACE_PLASTIC) m.ay = pb2_remap_roughness(v[0]);
+    }
+}
 
 // LOBE_GGX_VNDF is the conductor extension's lobe (no reference counterpart): the same GGX reflection
 // value as LOBE_MF_REFL, sampled with exact visible-normal sampling (Heitz 2018, "Sampling the GGX

@@ -117,6 +117,36 @@ class MeshData:
     material: int
     translation: tuple = (0.0, 0.0, 0.0)
     transform: np.ndarray | None = None  # (12,) float32 row-major 3x4 local-to-world, or None
+    texcoords: np.ndarray | None = None  # (V, 2) float32, or None
+
+
+@dataclass
+class TextureData:
+    """A pb2_texture: an image (texels (H, W, C) uint8, C in 1, 2, 4) or a checkerboard."""
+    kind: int
+    channel: int
+    texels: np.ndarray | None = None
+    wrap: int = 0
+    scale: float = 1.0
+    black: tuple = (0.0, 0.0, 0.0, 0.0)
+    white: tuple = (1.0, 1.0, 1.0, 1.0)
+
+
+def image_texture(texels, wrap: str = "Repeat") -> TextureData:
+    t = np.ascontiguousarray(texels, dtype=np.uint8)
+    if t.ndim == 2:
+        t = t[:, :, None]
+    if t.shape[2] == 3:  # RGB is loaded as RGBA (SampledTexture.cpp:133-138)
+        t = np.concatenate([t, np.full(t.shape[:2] + (1,), 255, np.uint8)], axis=2)
+    if t.shape[2] not in (1, 2, 4):
+        raise ValueError("an image texture has 1, 2, 3 or 4 channels")
+    return TextureData(capi.TEXTURE_IMAGE, int(t.shape[2]), t, capi.WRAP[wrap])
+
+
+def checkerboard(scale: float, black, white) -> TextureData:
+    if len(black) != len(white) or len(black) not in (1, 2, 4):
+        raise ValueError("black and white have the same 1, 2 or 4 channels")
+    return TextureData(capi.TEXTURE_CHECKERBOARD, len(black), None, 0, scale, tuple(black), tuple(white))
 
 
 @dataclass
@@ -125,6 +155,7 @@ class SceneData:
     planes: list = field(default_factory=list)        # capi.Plane
     area_lights: list = field(default_factory=list)   # (radiance, first_plane, plane_count, translation)
     materials: list = field(default_factory=list)     # capi.Material
+    textures: list = field(default_factory=list)      # TextureData; material.texture[k] = 1 + index
     env_radiance: tuple = (0.0, 0.0, 0.0)
     settings: capi.RenderSettings | None = None
     name: str = ""
@@ -148,6 +179,12 @@ class SceneData:
             meshes[i].tri_count = ix.shape[0]
             meshes[i].material = m.material
             meshes[i].translation[:] = [float(x) for x in m.translation]
+            if m.texcoords is not None:
+                tc = np.ascontiguousarray(m.texcoords, dtype=np.float32).reshape(-1, 2)
+                if tc.shape[0] != v.shape[0]:
+                    raise ValueError("texcoords must hold one (u, v) per vertex")
+                keep.append(tc)
+                meshes[i].texcoords = tc.ctypes.data
             if m.transform is not None:
                 t = np.ascontiguousarray(m.transform, dtype=np.float32).reshape(12)
                 keep.append(t)
@@ -172,12 +209,28 @@ class SceneData:
         sc.materials = C.cast(mats, C.POINTER(capi.Material))
         sc.material_count = len(self.materials)
         sc.env_radiance[:] = [float(x) for x in self.env_radiance]
-        keep += [meshes, planes, lights, mats]
+        texs = (capi.Texture * max(1, len(self.textures)))()
+        for i, t in enumerate(self.textures):
+            texs[i].kind, texs[i].channel, texs[i].wrap = t.kind, t.channel, t.wrap
+            if t.texels is not None:
+                tx = np.ascontiguousarray(t.texels, dtype=np.uint8)
+                keep.append(tx)
+                texs[i].height, texs[i].width = tx.shape[0], tx.shape[1]
+                texs[i].texels = tx.ctypes.data
+            texs[i].scale = float(t.scale)
+            texs[i].black[:] = [float(x) for x in list(t.black) + [0.0] * (4 - len(t.black))]
+            texs[i].white[:] = [float(x) for x in list(t.white) + [0.0] * (4 - len(t.white))]
+        sc.textures = C.cast(texs, C.POINTER(capi.Texture))
+        sc.texture_count = len(self.textures)
+        keep += [meshes, planes, lights, mats, texs]
         return sc, keep
 
 
-def material(kind: str, color0=(0, 0, 0, 0), color1=(0, 0, 0, 0), roughness=(0.0, 0.0)) -> capi.Material:
+def material(kind: str, color0=(0, 0, 0, 0), color1=(0, 0, 0, 0), roughness=(0.0, 0.0),
+             textures=(0, 0, 0, 0)) -> capi.Material:
+    """`textures`: per (color0, color1, roughness[0], roughness[1]), 0 or 1 + an index into SceneData.textures."""
     m = capi.Material()
+    m.texture[:] = [int(x) for x in textures]
     m.type = capi.SURFACE[kind]
     c0 = list(color0) + [0.0] * (4 - len(color0))
     c1 = list(color1) + [0.0] * (4 - len(color1))
@@ -295,6 +348,38 @@ def instanced_room(seed: int = 0, width: int = 64, height: int = 64, spp: int = 
     t = c - r[:, :3] @ c
     m = np.concatenate([r[:, :3], t[:, None].astype(np.float32)], axis=1).astype(np.float32)
     sd.planes = [plane_transform(light, m)]
+    return sd
+
+
+def textured_room(seed: int = 0, width: int = 48, height: int = 48, spp: int = 8, max_depth: int = 8,
+                  min_rr_depth: int = 3) -> SceneData:
+    """The Cornell room with textured materials: a checkerboard floor, an RGB image on the back wall (texcoords
+    running past [0, 1], wrap Repeat), a Plastic box whose roughness is a grey image (wrap Mirror) and a Substrate
+    box with a roughness checkerboard, plus a textured material on a mesh without texcoords (which samples at
+    (0, 0)).  Images are seeded noise, 8-bit."""
+    rng = np.random.default_rng(seed)
+    sd = cornell_box(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, min_rr_depth=min_rr_depth)
+    sd.name = f"textured_room(seed={seed})"
+    img = rng.integers(0, 256, size=(13, 17, 3), dtype=np.uint8)
+    grey = rng.integers(0, 256, size=(9, 7), dtype=np.uint8)
+    sd.textures = [checkerboard(6.0, (0.1, 0.1, 0.1, 1.0), (0.8, 0.75, 0.7, 1.0)),  # 1: floor color
+                   image_texture(img, "Repeat"),                                   # 2: back wall color
+                   image_texture(grey, "Mirror"),                                  # 3: plastic roughness
+                   checkerboard(3.0, (0.05,), (0.6,)),                             # 4: substrate roughness x
+                   image_texture(grey[::-1].copy(), "Repeat")]                     # 5: substrate roughness y
+    sd.materials += [material("Matte", (0, 0, 0), textures=(1, 0, 0, 0)),
+                     material("Matte", (0, 0, 0), textures=(2, 0, 0, 0)),
+                     material("Plastic", (0.3, 0.4, 0.6), (0.5, 0.5, 0.5), (0.2, 0.0), textures=(0, 0, 3, 0)),
+                     material("Substrate", (0.5, 0.3, 0.2), (0.3, 0.3, 0.3), (0.1, 0.1), textures=(0, 0, 4, 5))]
+    sd.meshes[0].material = 3       # floor
+    sd.meshes[0].texcoords = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    sd.meshes[2].material = 4       # back wall
+    sd.meshes[2].texcoords = np.array([[-0.3, 0.1], [2.2, 0.1], [2.2, 1.7], [-0.3, 1.7]], np.float32)
+    sd.meshes[1].material = 3       # ceiling: textured material, no texcoords
+    for k, m in ((5, 5), (6, 6)):
+        sd.meshes[k].material = m
+        n = sd.meshes[k].vertices.shape[0]
+        sd.meshes[k].texcoords = rng.uniform(-1.5, 2.5, size=(n, 2)).astype(np.float32)
     return sd
 
 

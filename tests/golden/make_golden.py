@@ -10,6 +10,7 @@ Writes:
   cornell_32x32_4spp.npz    per-sample (film point, radiance) of the Cornell-box scene, seed 0, rendered
                             by the reference kernels (single thread), plus sampled Sobol values of the
                             reference's sobolGenerate
+  textured_room_32x32_4spp.npz  the same for the textured room (checkerboard and image textures, texcoords)
 """
 import os
 import sys
@@ -42,6 +43,9 @@ def main():
     sob = np.array([(float(i), float(d), ref.ref_sobol_generate(int(i), int(d))) for i, d in zip(idx, dim)])
     # store exact integers for the index (float64 holds them exactly below 2^53)
     np.savez_compressed(os.path.join(HERE, "cornell_32x32_4spp.npz"), samples=samples, seed=0, sobol=sob)
+    sd = scenes.textured_room(seed=0, width=32, height=32, spp=4)
+    _, samples = oracle_py.RefScene(sd, use_bvh=False).render(threads=1)
+    np.savez_compressed(os.path.join(HERE, "textured_room_32x32_4spp.npz"), samples=samples, seed=0)
     print("golden vectors written")
 
 

@@ -81,7 +81,7 @@ def test_ctypes_structs_match_the_header(tmp_path):
              "AreaLight": "pb2_area_light", "Material": "pb2_material", "Camera": "pb2_camera", "Scene": "pb2_scene",
              "RenderSettings": "pb2_render_settings", "Rect": "pb2_rect", "NDCTransform": "pb2_ndc_transform",
              "AccelInfo": "pb2_accel_info", "LaunchStats": "pb2_launch_stats", "BatchConfig": "pb2_batch_config",
-             "GuideSettings": "pb2_guide_settings", "SRT": "pb2_srt"}
+             "GuideSettings": "pb2_guide_settings", "SRT": "pb2_srt", "Texture": "pb2_texture"}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "piper2_b200.h"', "int main(void) {"]
     for py, c in pairs.items():
         cls = getattr(capi, py)
