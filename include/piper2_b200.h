@@ -514,6 +514,75 @@ int pb2_batch_timing(const pb2_batch* batch, float* scene_ms, uint32_t count, fl
                      uint32_t* iterations);
 int pb2_batch_get_stats(const pb2_batch* batch, pb2_launch_stats* stats);
 
+/* ---- Accelerator: buffers, tiled outputs, resource lookup tables, generic kernel launches ---------
+ * The CUDA Accelerator plugin of the reference (Src/Interface/Infrastructure/Accelerator.hpp:130-161,
+ * Src/Infrastructure/Accelerator/CUDA/CUDA.cpp:497-927) without its LLVM-IR JIT: a kernel is native sm_100a
+ * code compiled against include/piper2_b200_device.cuh and registered by entry name, in place of
+ * compileKernel's link of LLVM modules.  One accelerator drives one device (the current device at creation;
+ * the reference opens a context per device, CUDA.cpp:718-780) through `streams` CUDA streams (its "Steams"
+ * option, CUDA.cpp:723-726; 0 = 4).  Every operation is ordered by futures as in the reference: a buffer's
+ * upload, a tiled output's last marked writer and a launch each complete a future, and a launch waits for the
+ * futures of every resource its lookup table reaches (CUDA.cpp:817-824).  Resources and futures are
+ * reference counted (the reference's SharedPtr): *_release drops one reference; a lookup table holds its
+ * entries, a launch holds its kernel, table and resources until it completes. */
+typedef struct pb2_accelerator pb2_accelerator;
+typedef struct pb2_resource pb2_resource;
+typedef struct pb2_kernel pb2_kernel;
+typedef struct pb2_future pb2_future;
+/* Fills `size` bytes of staging memory at `dst` (the Function<void, Ptr> of createBuffer). */
+typedef void (*pb2_fill_fn)(void* dst, size_t size, void* user);
+
+int pb2_acc_create(uint32_t streams, pb2_accelerator** out);
+/* Waits for all work, then frees the accelerator (resources, kernels and futures must be released first). */
+int pb2_acc_destroy(pb2_accelerator* acc);
+/* "NVIDIA CUDA" (getNativePlatform, CUDA.cpp:791-793). */
+const char* pb2_acc_native_platform(const pb2_accelerator* acc);
+/* Device index of the accelerator's context and its stream count (enumerateContexts). */
+int pb2_acc_get_info(const pb2_accelerator* acc, int* device, uint32_t* streams);
+/* createBuffer (CUDA.cpp:913-916, CUDABufferInstance :513-566): `fill` writes the initial bytes into pinned
+ * staging memory before the call returns (NULL fill = zeros); the upload to the device is asynchronous and
+ * completes the buffer's future.  `alignment` is a power of two (the device address is aligned to it). */
+int pb2_acc_create_buffer(pb2_accelerator* acc, size_t size, size_t alignment, pb2_fill_fn fill, void* user,
+                          pb2_resource** out);
+/* createTiledOutput (CUDA.cpp:922-924, CUDATiledBufferInstance :585-640): a zeroed device buffer that kernels
+ * write; pb2_tiled_output_mark_dirty names the launch whose writes a download must wait for. */
+int pb2_acc_create_tiled_output(pb2_accelerator* acc, size_t size, size_t alignment, pb2_resource** out);
+/* createResourceLUT (CUDA.cpp:919-921, ResourceLookUpTableInstance :665-697): entries are buffers, tiled
+ * outputs or other tables; a launch flattens the tables (root first, each nested table's entries appended
+ * after its parent's, the parent's entry holding the handle index where they start). */
+int pb2_acc_create_resource_lut(pb2_accelerator* acc, pb2_resource* const* resources, uint32_t count,
+                                pb2_resource** out);
+/* ResourceInstance::getHandle: the device address of a buffer or tiled output (tables have none). */
+int pb2_resource_get_handle(const pb2_resource* res, uint64_t* handle);
+int pb2_resource_release(pb2_resource* res);
+/* TiledOutput::markDirty (CUDA.cpp:656-658). */
+int pb2_tiled_output_mark_dirty(pb2_resource* output, pb2_future* writer);
+/* TiledOutput::download (CUDA.cpp:627-637): waits for the marked writer, copies `size` bytes (at most the
+ * output's size) to `dst_host` and returns when they are there. */
+int pb2_tiled_output_download(pb2_resource* output, void* dst_host, size_t size);
+/* compileKernel without the JIT: `entry` names a kernel registered on this accelerator; unknown names fail
+ * with PB2_ERR_NOT_SUPPORTED naming the entry (the reference fails to link an unknown symbol). */
+int pb2_acc_compile_kernel(pb2_accelerator* acc, const char* entry, pb2_kernel** out);
+/* Registers a generic kernel: `cu_function` is the CUfunction of an entry declared with PB2_KERNEL_ENTRY
+ * (from cudaGetFuncBySymbol or cuModuleGetFunction) in the accelerator's device context. */
+int pb2_acc_register_kernel(pb2_accelerator* acc, const char* entry, void* cu_function);
+int pb2_kernel_release(pb2_kernel* kernel);
+/* launchKernel (CUDA.cpp:803-910): packs the flattened handles of `root` and the arguments (`arg_desc` holds
+ * arg_count (offset, size) pairs into `arg_data`, the reference's ArgumentPackage) into a launch buffer and
+ * launches the kernel over dim[0] x dim[1] x dim[2] tasks on a stream (the first idle one, else round robin)
+ * after the futures of every resource reached through `root`.  An empty launch is rejected (CUDA.cpp:
+ * 805-806).  *out (optional) is the launch's future. */
+int pb2_acc_launch_kernel(pb2_accelerator* acc, const uint32_t dim[3], pb2_kernel* kernel, pb2_resource* root,
+                          const void* arg_data, const uint32_t* arg_desc, uint32_t arg_count, pb2_future** out);
+/* The launch buffer layout alone (no device): writes it for `handles` and the arguments to `dst` (when
+ * dst_size suffices) and its size to *needed.  The layout is documented in piper2_b200_device.cuh. */
+int pb2_acc_pack_launch(const uint64_t* handles, uint32_t handle_count, const void* arg_data, const uint32_t* arg_desc,
+                        uint32_t arg_count, void* dst, size_t dst_size, size_t* needed);
+/* Future<void>: wait, poll, release (the reference's FutureImpl::wait / ready). */
+int pb2_future_wait(pb2_future* future);
+int pb2_future_ready(pb2_future* future, int* ready);
+int pb2_future_release(pb2_future* future);
+
 #ifdef __cplusplus
 }
 #endif

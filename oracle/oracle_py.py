@@ -43,6 +43,8 @@ def oracle():
         h = _load(ORACLE_SO)
         h.or_sobol_sample.restype = C.c_float
         h.or_sobol_sample.argtypes = [C.c_uint64, C.c_uint32]
+        h.or_conv.restype = None
+        h.or_conv.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32]
         h.or_sobol_sample_scrambled.restype = C.c_float
         h.or_sobol_sample_scrambled.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
         h.or_sobol_interval_to_index.restype = C.c_uint64
@@ -101,6 +103,18 @@ def oracle_fp64():
         _bind_pixels(h)
         _or64 = h
     return _or64
+
+
+def conv(x, y, width, height, kernel_size):
+    """The Accelerator test's convolution (Src/Test/conv.hpp:22-37) of a float32 image x (height x width) with a
+    float32 kernel y (kernel_size x kernel_size), accumulated in float in the reference's loop order."""
+    import numpy as np
+
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    z = np.empty(width * height, np.float32)
+    oracle().or_conv(x.ctypes.data, y.ctypes.data, z.ctypes.data, width, height, kernel_size)
+    return z
 
 
 def ref_available() -> bool:

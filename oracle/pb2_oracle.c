@@ -1886,3 +1886,23 @@ int or_render_pixels(const or_scene* s, const pb2_render_settings* st, const uin
     }
     return overflow ? -3 : 0;
 }
+
+/* conv (Src/Test/conv.hpp:22-37): z[idx] = sum over the kernel window inside the image of x * y, accumulated in
+ * float in the reference's loop order (i over x offsets, then j over y offsets). */
+void or_conv(const float* x, const float* y, float* z, uint32_t width, uint32_t height, uint32_t kernel_size) {
+    const uint32_t half = kernel_size / 2;
+    const uint32_t count = width * height;
+    for (uint32_t idx = 0; idx < count; ++idx) {
+        const uint32_t py = idx / width, px = idx % width;
+        float res = 0.0f;
+        for (int32_t i = 0; i < (int32_t)kernel_size; ++i) {
+            const int32_t nx = (int32_t)(px + (uint32_t)i - half);
+            if (nx >= 0 && nx < (int32_t)width)
+                for (int32_t j = 0; j < (int32_t)kernel_size; ++j) {
+                    const int32_t ny = (int32_t)(py + (uint32_t)j - half);
+                    if (ny >= 0 && ny < (int32_t)height) res += x[ny * (int32_t)width + nx] * y[i * (int32_t)kernel_size + j];
+                }
+        }
+        z[idx] = res;
+    }
+}

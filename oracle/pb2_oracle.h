@@ -81,6 +81,10 @@ void or_bsdf_sample(const or_scene* s, uint32_t mat, int front, const float wo[3
 void or_bsdf_eval(const or_scene* s, uint32_t mat, int front, const float wo[3], uint32_t n, const float* wi,
                   float* f, float* pdf);
 
+/* The Accelerator test's convolution kernel (Src/Test/conv.hpp:22-37), every output of a width x height image
+ * (the CPU loop of Src/Test/Accelerator-Test.cpp:79-81). */
+void or_conv(const float* x, const float* y, float* z, uint32_t width, uint32_t height, uint32_t kernel_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libpiper2_b200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["bvh_build.cu", "traverse.cu", "render.cu", "capi.cu", "nalloc.cu", "guiding.cu", "guiding_tc.cu",
+SOURCES = ["bvh_build.cu", "accelerator.cu", "traverse.cu", "render.cu", "capi.cu", "nalloc.cu", "guiding.cu", "guiding_tc.cu",
            "guiding_train_tc.cu", "materialize.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]

@@ -15,6 +15,11 @@ LIB_PATH = os.path.join(HERE, "_lib", "libpiper2_b200.so")
 
 PB2_OK = 0
 PB2_ERR_INVALID_ARGUMENT = 1
+PB2_ERR_CUDA = 2
+PB2_ERR_OUT_OF_MEMORY = 3
+PB2_ERR_NOT_SUPPORTED = 4
+PB2_ERR_DEVICE_TIMEOUT = 5
+PB2_ERR_QUEUE_OVERFLOW = 6
 PB2_INVALID_PRIM = 0xFFFFFFFF
 PB2_PLANE_FLAG = 0x80000000
 
@@ -207,7 +212,33 @@ SIGNATURES = [
                                     C.c_void_p]),
     ("pb2_pipeline_train_guide", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float),
                                             C.c_void_p]),
+    # accelerator (Accelerator.hpp:130-161)
+    ("pb2_acc_create", C.c_int, [C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("pb2_acc_destroy", C.c_int, [C.c_void_p]),
+    ("pb2_acc_native_platform", C.c_char_p, [C.c_void_p]),
+    ("pb2_acc_get_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint32)]),
+    ("pb2_acc_create_buffer", C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_void_p)]),
+    ("pb2_acc_create_tiled_output", C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("pb2_acc_create_resource_lut", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("pb2_resource_get_handle", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("pb2_resource_release", C.c_int, [C.c_void_p]),
+    ("pb2_tiled_output_mark_dirty", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pb2_tiled_output_download", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("pb2_acc_compile_kernel", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("pb2_acc_register_kernel", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p]),
+    ("pb2_kernel_release", C.c_int, [C.c_void_p]),
+    ("pb2_acc_launch_kernel", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("pb2_acc_pack_launch", C.c_int, [C.POINTER(C.c_uint64), C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32,
+                                      C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("pb2_future_wait", C.c_int, [C.c_void_p]),
+    ("pb2_future_ready", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("pb2_future_release", C.c_int, [C.c_void_p]),
 ]
+
+# void (*)(void* dst, size_t size, void* user): fills a buffer's initial bytes (pb2_acc_create_buffer)
+FILL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_size_t, C.c_void_p)
 
 
 # int (*)(float* grad_dev, uint32_t count, void* stream, void* user)
