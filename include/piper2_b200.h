@@ -533,7 +533,8 @@ typedef struct pb2_future pb2_future;
 typedef void (*pb2_fill_fn)(void* dst, size_t size, void* user);
 
 int pb2_acc_create(uint32_t streams, pb2_accelerator** out);
-/* Waits for all work, then frees the accelerator (resources, kernels and futures must be released first). */
+/* Waits for all work and drops the caller's reference; the streams live on until the last resource made by the
+ * accelerator is released. */
 int pb2_acc_destroy(pb2_accelerator* acc);
 /* "NVIDIA CUDA" (getNativePlatform, CUDA.cpp:791-793). */
 const char* pb2_acc_native_platform(const pb2_accelerator* acc);

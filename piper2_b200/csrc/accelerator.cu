@@ -79,6 +79,9 @@ struct pb2_kernel {
 };
 
 struct pb2_accelerator {
+    // one reference for the caller (pb2_acc_destroy drops it) and one per live resource, so resources released
+    // after pb2_acc_destroy still find their streams
+    std::atomic<int> refs{ 1 };
     int device = 0;
     std::vector<cudaStream_t> streams;
     uint32_t next_stream = 0;
@@ -115,6 +118,22 @@ void future_drop(pb2_future* f) {
 
 void resource_retain(pb2_resource* r) { r->refs.fetch_add(1, std::memory_order_relaxed); }
 
+void reap_locked(pb2_accelerator* acc, bool wait);
+
+void acc_drop(pb2_accelerator* acc) {
+    if (acc->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    DeviceScope scope(acc->device);
+    for (cudaStream_t s : acc->streams) cudaStreamSynchronize(s);
+    {
+        std::lock_guard<std::mutex> lk(acc->mu);
+        reap_locked(acc, true);
+        for (auto& st : acc->pool) cudaFreeHost(st.ptr);
+        acc->pool.clear();
+    }
+    for (cudaStream_t s : acc->streams) cudaStreamDestroy(s);
+    delete acc;
+}
+
 void resource_drop(pb2_resource* r) {
     if (!r || r->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
     if (r->raw) {
@@ -125,7 +144,9 @@ void resource_drop(pb2_resource* r) {
     }
     future_drop(r->future);
     for (pb2_resource* e : r->entries) resource_drop(e);
+    pb2_accelerator* acc = r->acc;
     delete r;
+    acc_drop(acc);
 }
 
 void kernel_drop(pb2_kernel* k) {
@@ -220,6 +241,7 @@ int make_device_resource(pb2_accelerator* acc, int kind, size_t size, size_t ali
         return cuda_fail(e, "cudaMallocAsync resource");
     }
     r->handle = ((uint64_t)(uintptr_t)r->raw + alignment - 1) & ~(uint64_t)(alignment - 1);
+    acc->refs.fetch_add(1, std::memory_order_relaxed);
     *out = r;
     *stream = s;
     return PB2_OK;
@@ -307,16 +329,13 @@ int pb2_acc_create(uint32_t streams, pb2_accelerator** out) {
 
 int pb2_acc_destroy(pb2_accelerator* acc) {
     if (!acc) return PB2_OK;
-    DeviceScope scope(acc->device);
-    for (cudaStream_t s : acc->streams) cudaStreamSynchronize(s);
     {
+        DeviceScope scope(acc->device);
+        for (cudaStream_t s : acc->streams) cudaStreamSynchronize(s);
         std::lock_guard<std::mutex> lk(acc->mu);
         reap_locked(acc, true);
-        for (auto& st : acc->pool) cudaFreeHost(st.ptr);
-        acc->pool.clear();
     }
-    for (cudaStream_t s : acc->streams) cudaStreamDestroy(s);
-    delete acc;
+    acc_drop(acc);
     return PB2_OK;
 }
 
@@ -399,6 +418,7 @@ int pb2_acc_create_resource_lut(pb2_accelerator* acc, pb2_resource* const* resou
     auto* t = new pb2_resource;
     t->kind = kTable;
     t->acc = acc;
+    acc->refs.fetch_add(1, std::memory_order_relaxed);
     for (uint32_t i = 0; i < count; ++i) {
         resource_retain(resources[i]);
         t->entries.push_back(resources[i]);

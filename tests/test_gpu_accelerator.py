@@ -4,6 +4,7 @@ createResourceLUT / compileKernel / launchKernel / markDirty / download) against
 kernel, bit for bit; nested lookup tables, every argument kind and the task index mapping; futures and errors.
 The kernels are native sm_100a code (tests/kernels/generic_kernels.cu) registered by entry name."""
 import ctypes as C
+import os
 import sys
 
 import numpy as np
@@ -18,7 +19,7 @@ pytestmark = pytest.mark.gpu
 def acc():
     from piper2_b200 import accelerator
 
-    sys.path.insert(0, __import__("os").path.join(__import__("os").path.dirname(__file__), "kernels"))
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "kernels"))
     import build_kernels
 
     kl = C.CDLL(build_kernels.build())
