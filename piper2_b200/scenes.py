@@ -573,23 +573,60 @@ def mixed_materials(seed: int = 0, width: int = 1920, height: int = 1080, spp: i
     return sd
 
 
+def _grid_cells(p0, p1, p3, n):
+    """The parallelogram p0 + [0,1](p1 - p0) + [0,1](p3 - p0) as an n x n grid of cells, two triangles each, wound
+    as the quad [p0, p1, p2], [p0, p2, p3] (vectorised)."""
+    p0, p1, p3 = (np.asarray(x, dtype=np.float64) for x in (p0, p1, p3))
+    a = np.linspace(0.0, 1.0, n + 1)
+    A, B = np.meshgrid(a, a, indexing="ij")
+    verts = (p0 + A[..., None] * (p1 - p0) + B[..., None] * (p3 - p0)).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    p00 = (i * (n + 1) + j).reshape(-1)
+    p10, p01 = p00 + (n + 1), p00 + 1
+    p11 = p10 + 1
+    idx = np.stack([np.stack([p00, p10, p11], 1), np.stack([p00, p11, p01], 1)], 1).reshape(-1, 3)
+    return verts, idx.astype(np.uint32)
+
+
+def cornell_variant(seed: int = 0, triangles: int = 10_000, width: int = 256, height: int = 256, spp: int = 16,
+                    max_depth: int = 16, min_rr_depth: int = 3) -> SceneData:
+    """A variant of the Cornell-box generator with about `triangles` triangles: the seed draws the boxes' angles
+    as :func:`cornell_box` does, and the five room quads are tessellated into equal grids (same surfaces, same
+    image, more geometry to traverse)."""
+    sd = cornell_box(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, min_rr_depth=min_rr_depth)
+    n = max(1, int(np.sqrt(max(triangles - 24, 10) / 10)))
+    for m in sd.meshes[:5]:
+        v = m.vertices.astype(np.float64)
+        gv, gi = _grid_cells(v[0], v[1], v[3], n)
+        m.vertices, m.indices = gv.astype(np.float32), gi
+    sd.name = f"cornell_variant(seed={seed}, {sd.triangle_count} tris)"
+    return sd
+
+
 def batch_workload(seed: int = 0, count: int = 64, max_depth: int = 16) -> list:
-    """The batching workload: `count` scenes from the mixed-materials generator, each with its own seed,
-    triangle count log-uniform in [10k, 2M] (terrain grid and icosphere count chosen to match), film side
-    log-uniform in [128, 1024] (16:9, the generator's sensor), and spp uniform in [4, 64] rounded up to a
-    power of two (the reference's sampler rounds the same way, ScrambledSobolSampler.cpp:43-50)."""
+    """The batching workload: `count` scenes, each a seed-drawn variant of the Cornell-box generator
+    (:func:`cornell_variant`) or of the mixed-materials generator (:func:`mixed_materials`), chosen with equal
+    probability, with its own seed, a triangle count log-uniform in [10k, 2M] (room grid, or terrain grid and
+    icosphere count, chosen to match), film side log-uniform in [128, 1024] (16:9), and spp uniform in [4, 64]
+    rounded up to a power of two (the reference's sampler rounds the same way,
+    ScrambledSobolSampler.cpp:43-50)."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(count):
         tris = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
-        n_spheres = int(min(200, (0.3 * tris) // 5120))
-        grid = max(8, int(np.sqrt(max(tris - 5120 * n_spheres, 128) / 2)))
         side = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
         width, height = side, max(8, int(round(side * 9 / 16)))
         spp = 1 << int(np.ceil(np.log2(rng.integers(4, 65))))
-        sd = mixed_materials(seed=seed * 1000 + k + 1, width=width, height=height, spp=spp, max_depth=max_depth,
-                             grid=grid, n_spheres=n_spheres)
-        sd.name = f"batch[{k}] {2 * grid * grid + 5120 * n_spheres} tris {width}x{height} {spp} spp"
+        if rng.uniform() < 0.5:
+            sd = cornell_variant(seed=seed * 1000 + k + 1, triangles=tris, width=width, height=height, spp=spp,
+                                 max_depth=max_depth)
+            sd.name = f"batch[{k}] cornell {sd.triangle_count} tris {width}x{height} {spp} spp"
+        else:
+            n_spheres = int(min(200, (0.3 * tris) // 5120))
+            grid = max(8, int(np.sqrt(max(tris - 5120 * n_spheres, 128) / 2)))
+            sd = mixed_materials(seed=seed * 1000 + k + 1, width=width, height=height, spp=spp, max_depth=max_depth,
+                                 grid=grid, n_spheres=n_spheres)
+            sd.name = f"batch[{k}] mixed {2 * grid * grid + 5120 * n_spheres} tris {width}x{height} {spp} spp"
         out.append(sd)
     return out
 

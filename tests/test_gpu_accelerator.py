@@ -69,8 +69,8 @@ def test_nested_tables_arguments_and_task_indices(acc):
     t = acc.create_tiled_output(4 * n, 256)
     h = acc.create_tiled_output(8 * 16, 8)
     b0 = acc.create_buffer(4 * n, 4096, lambda v: v.__setitem__(slice(None), base.view(np.uint8)))
-    b1 = acc.create_buffer(4, 4, lambda v: v.__setitem__(slice(None), np.uint32(1000).tobytes()))
-    b2 = acc.create_buffer(4, 4, lambda v: v.__setitem__(slice(None), np.uint32(20000).tobytes()))
+    b1 = acc.create_buffer(4, 4, lambda v: v.__setitem__(slice(None), np.array([1000], np.uint32).view(np.uint8)))
+    b2 = acc.create_buffer(4, 4, lambda v: v.__setitem__(slice(None), np.array([20000], np.uint32).view(np.uint8)))
     n2 = acc.create_resource_lut([b2])
     n1 = acc.create_resource_lut([b1, n2])
     root = acc.create_resource_lut([t, h, n1, b0])
