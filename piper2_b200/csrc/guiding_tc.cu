@@ -30,10 +30,13 @@ struct FeatureRows {
     __device__ __forceinline__ void output(uint32_t, const float (&)[kOut]) const {}
 };
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_forward_tc(GuideView gv, const float* __restrict__ features, uint32_t n,
-                                                           float* __restrict__ out, uint32_t* __restrict__ error) {
+using FwdLayout = TcLayout<kTcGroupsForward>;
+
+__global__ void __launch_bounds__(FwdLayout::kThreads, 1) k_forward_tc(GuideView gv, const float* __restrict__ features,
+                                                                     uint32_t n, float* __restrict__ out,
+                                                                     uint32_t* __restrict__ error) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    forward_tc_tiles(gv, n, FeatureRows{ features, out }, error, smem);
+    forward_tc_tiles<kTcGroupsForward>(gv, n, FeatureRows{ features, out }, error, smem);
 }
 
 }  // namespace
@@ -43,14 +46,15 @@ cudaError_t guide_forward_tc(const GuideView& gv, const float* features, uint32_
     using namespace guide;
     if (n == 0) return cudaSuccess;
     static std::atomic<int> attr[kMaxDevices];
-    const cudaError_t e = smem_attr_once((const void*)k_forward_tc, forward_tc_smem(), attr);
+    const cudaError_t e = smem_attr_once((const void*)k_forward_tc, forward_tc_smem<kTcGroupsForward>(), attr);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    const int grid = (int)std::min<uint32_t>((tiles + kTcGroups - 1) / kTcGroups, (uint32_t)sms);
-    k_forward_tc<<<grid, kTcThreads, forward_tc_smem(), stream>>>(gv, features, n, out, error);
+    const int grid = (int)std::min<uint32_t>((tiles + kTcGroupsForward - 1) / kTcGroupsForward, (uint32_t)sms);
+    k_forward_tc<<<grid, FwdLayout::kThreads, forward_tc_smem<kTcGroupsForward>(), stream>>>(gv, features, n, out,
+                                                                                              error);
     return cudaGetLastError();
 }
 

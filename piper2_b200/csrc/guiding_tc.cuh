@@ -1,7 +1,7 @@
 // guiding_tc.cuh -- the guiding network's forward pass on the 5th-generation tensor cores (tcgen05).
 //
-// A CTA holds the weights of all five layers once in shared memory and runs kTcGroups independent warp
-// groups of 4 warps; each group evaluates its own 128-row tiles, so while one group waits for its MMAs
+// A CTA holds the weights of all five layers once in shared memory and runs G independent warp
+// groups of 4 warps (TcLayout<G>); each group evaluates its own 128-row tiles, so while one group waits for its MMAs
 // another encodes inputs or drains its accumulator (the tensor pipe is shared by the groups of the SM).
 // The encoded inputs and each hidden layer's output are bf16 operands in shared memory in the canonical
 // K-major, no-swizzle UMMA layout (8-row x 16-byte core matrices; within a tile, core matrices adjacent in
@@ -9,9 +9,9 @@
 // layout.  For each layer one thread of the group issues K/16 `tcgen05.mma.cta_group::1.kind::f16`
 // (M = 128, N = 64 or 48, BF16 x BF16 -> FP32) into the group's 64 TMEM columns and commits them to the
 // group's mbarrier; every warp of the group then reads its 32 rows back with `tcgen05.ld.32x32b`, adds the
-// bias, applies ReLU, and writes the next layer's bf16 operand.  A group's two operand buffers alternate
-// between layers (input tile -> H -> A -> H -> A), and after the last layer the input buffer stages the
-// fp32 outputs so that a row-major output is written with coalesced stores.  Shared-memory writes that
+// bias, applies ReLU, and writes the next layer's bf16 operand over the one the completed MMAs read (a group has
+// one operand buffer), and after the last layer the buffer stages the fp32 outputs so that a row-major output
+// is written with coalesced stores.  Shared-memory writes that
 // an MMA reads are made visible to the tensor core's async proxy with `fence.proxy.async.shared::cta`
 // before the group's named barrier.
 //
@@ -27,32 +27,43 @@ namespace pb2 {
 namespace guide {
 
 constexpr int kTcRows = 128;
-constexpr int kTcGroups = 4;                       // independent 128-row tiles in flight per CTA
 constexpr int kTcGroupThreads = 128;
-constexpr int kTcThreads = kTcGroupThreads * kTcGroups;
 constexpr uint32_t kTmemColsPerGroup = 64;
-constexpr uint32_t kTmemCols = kTmemColsPerGroup * kTcGroups;  // 256: a power of two, as tcgen05.alloc needs
 constexpr uint32_t kWaitLimit = 1u << 20;  // mbarrier polls before a wait counts as failed
 
 __host__ __device__ constexpr int tc_w_offset(int l) {  // bytes of layer l's weights in the staged image
     return l == 0 ? 0 : tc_w_offset(l - 1) + layer_out(l - 1) * layer_in(l - 1) * 2;
 }
 constexpr int kTcWBytes = tc_w_offset(kLayers);                        // 43,008
-constexpr int kTcABytes = kTcRows * kIn * 2;                           // 24,576: input tile, odd layers' output,
-                                                                       // and the fp32 output staging (128 x 48)
-constexpr int kTcHBytes = kTcRows * kHid * 2;                          // 16,384
-constexpr int kTcGroupBytes = kTcABytes + kTcHBytes;
-constexpr int kTcOffW = 0;
-constexpr int kTcOffGroups = kTcWBytes;                                // 1024-aligned below
-constexpr int kTcOffBias = kTcOffGroups + kTcGroups * kTcGroupBytes;
-constexpr int kTcOffBar = kTcOffBias + kBiasElems * 4;                 // kTcGroups mbarriers
-constexpr int kTcOffSlot = kTcOffBar + 8 * kTcGroups;                  // TMEM base address
-constexpr int kTcOffFail = kTcOffSlot + 4;                             // kTcGroups failure flags
-constexpr int kTcSmem = kTcOffFail + 4 * kTcGroups;
-static_assert(kTcOffGroups % 1024 == 0 && kTcABytes % 1024 == 0 && kTcGroupBytes % 1024 == 0, "operand alignment");
-static_assert(kTcABytes >= kTcRows * kOut * 4, "output staging fits the input buffer");
-static_assert(kTcOffBar % 8 == 0, "mbarrier alignment");
-static_assert(kTcSmem <= 227 * 1024, "shared memory per CTA");
+constexpr int kTcABytes = kTcRows * kIn * 2;                           // 24,576: a group's one operand buffer (the
+                                                                       // input tile, each hidden layer's output written
+                                                                       // over the input its MMA has consumed, and the
+                                                                       // fp32 output staging, 128 x 48)
+
+// Shared-memory layout and sizes of a CTA of G warp groups.
+template <int G>
+struct TcLayout {
+    static constexpr int kGroups = G;
+    static constexpr int kThreads = kTcGroupThreads * G;
+    static constexpr uint32_t kTmemCols = G * kTmemColsPerGroup <= 128 ? 128u : G * kTmemColsPerGroup <= 256 ? 256u : 512u;
+    static constexpr int kOffW = 0;
+    static constexpr int kOffGroups = kTcWBytes;                       // 1024-aligned
+    static constexpr int kOffBias = kOffGroups + G * kTcABytes;
+    static constexpr int kOffBar = kOffBias + kBiasElems * 4;          // G mbarriers
+    static constexpr int kOffSlot = kOffBar + 8 * G;                   // TMEM base address
+    static constexpr int kOffFail = kOffSlot + 4;                      // G failure flags
+    static constexpr int kSmem = kOffFail + 4 * G;
+    static_assert(kOffGroups % 1024 == 0 && kTcABytes % 1024 == 0, "operand alignment");
+    static_assert(kTcABytes >= kTcRows * kOut * 4, "output staging fits the operand buffer");
+    static_assert(kOffBar % 8 == 0, "mbarrier alignment");
+    static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
+    static_assert(G * kTmemColsPerGroup <= 512, "tensor memory per SM");
+};
+// The batched forward (k_forward_tc): seven groups, as many 128-row tiles in flight as shared memory holds
+// (7 x 24 KB of operands beside the 43 KB of weights).  The in-render inference keeps four (its epilogue holds
+// a row's 48 outputs in registers for the mixture).
+constexpr int kTcGroupsForward = 7;
+constexpr int kTcGroupsInfer = 4;
 
 // Byte offset of element (row, k) of a K-major operand with `kdim` columns in the core-matrix layout.
 __host__ __device__ constexpr uint32_t core_offset(uint32_t row, uint32_t k, uint32_t kdim) {
@@ -124,35 +135,68 @@ __device__ __forceinline__ void group_sync(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(kTcGroupThreads) : "memory");
 }
 
-// The tile loop of the tensor-core forward pass, for a CTA of kTcThreads threads with forward_tc_smem() bytes
-// of dynamic shared memory.  Rows: thread t of a group handles row tile * 128 + t of the n rows;
-// rows.features(row, f, key) fills the 9 input features and a key the thread keeps.  Outputs: with
+// The encoded input row written straight into the operand buffer, 8 bf16 (16 bytes) at a time, with encode_row's
+// arithmetic: 7 blob features of 12 bins (position xyz, the normal's and the outgoing direction's angles), a
+// constant 1 at 84, zeros to 96.  Only the 7 scaled features live in registers.
+__device__ __forceinline__ void encode_row_tile(const float (&f)[9], unsigned char* tile, uint32_t row) {
+    float s[7];
+    s[0] = fminf(fmaxf(f[0], 0.f), 1.f) * 12.f;
+    s[1] = fminf(fmaxf(f[1], 0.f), 1.f) * 12.f;
+    s[2] = fminf(fmaxf(f[2], 0.f), 1.f) * 12.f;
+    float th, ph;
+    dir_angles(f[3], f[4], f[5], th, ph);
+    s[3] = fminf(fmaxf(th, 0.f), 1.f) * 12.f;
+    s[4] = fminf(fmaxf(ph, 0.f), 1.f) * 12.f;
+    dir_angles(f[6], f[7], f[8], th, ph);
+    s[5] = fminf(fmaxf(th, 0.f), 1.f) * 12.f;
+    s[6] = fminf(fmaxf(ph, 0.f), 1.f) * 12.f;
+#pragma unroll
+    for (int kc = 0; kc < kIn / 8; ++kc) {
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = kc * 8 + i;
+            float x = 0.f;
+            if (e < 84) x = fmaxf(0.f, 1.f - fabsf(s[e / 12] - ((float)(e % 12) + 0.5f)));
+            else if (e == 84) x = 1.f;
+            v[i] = __float2bfloat16_rn(x);
+        }
+        *reinterpret_cast<int4*>(tile + core_offset(row, kc * 8, kIn)) = *reinterpret_cast<const int4*>(v);
+    }
+}
+
+// The tile loop of the tensor-core forward pass, for a CTA of TcLayout<G>::kThreads threads with
+// TcLayout<G>::kSmem bytes of dynamic shared memory.  Rows: thread t of a group handles row tile * 128 + t of the
+// n rows; rows.features(row, f, key) fills the 9 input features and a key the thread keeps.  Outputs: with
 // Rows::kStaged, rows.store_tile(row0, count, staged, t, threads) writes rows [row0, row0 + count) from the
 // group's staged fp32 outputs (row-major, 48 per row) cooperatively; otherwise rows.output(key, y) receives
 // the 48 raw outputs of a row below n.  error[0] is set when a tensor-core wait timed out.
-template <class Rows>
+//
+// Each group has one operand buffer: layer l's MMAs read it, and once they have completed (the group waited on
+// its mbarrier) the epilogue writes layer l + 1's operand over it; after the last layer it stages the outputs.
+template <int G, class Rows>
 __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n, const Rows& rows, uint32_t* error,
                                                  unsigned char* smem) {
+    using L = TcLayout<G>;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int g = tid / kTcGroupThreads, gt = tid % kTcGroupThreads;  // group and thread within it
-    unsigned char* w_s = smem + kTcOffW;
-    unsigned char* buf[2] = { smem + kTcOffGroups + g * kTcGroupBytes,                // A: input tile
-                              smem + kTcOffGroups + g * kTcGroupBytes + kTcABytes };  // H
-    float* b_s = reinterpret_cast<float*>(smem + kTcOffBias);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcOffBar) + g;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffSlot);
-    volatile uint32_t& s_fail = reinterpret_cast<uint32_t*>(smem + kTcOffFail)[g];
+    unsigned char* w_s = smem + L::kOffW;
+    unsigned char* buf = smem + L::kOffGroups + g * kTcABytes;
+    float* b_s = reinterpret_cast<float*>(smem + L::kOffBias);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::kOffBar) + g;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::kOffSlot);
+    volatile uint32_t& s_fail = reinterpret_cast<uint32_t*>(smem + L::kOffFail)[g];
 
     // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time (all groups)
     for (int l = 0; l < kLayers; ++l) {
         const int in = layer_in(l), outd = layer_out(l), chunks = outd * (in / 8);
-        for (int c = tid; c < chunks; c += kTcThreads) {
+        for (int c = tid; c < chunks; c += L::kThreads) {
             const int o = c / (in / 8), kc = c % (in / 8);
             const int4 v = *reinterpret_cast<const int4*>(gv.w16 + w16_offset(l) + o * layer_stride(l) + kc * 8);
             *reinterpret_cast<int4*>(w_s + tc_w_offset(l) + core_offset(o, kc * 8, in)) = v;
         }
     }
-    for (int i = tid; i < kBiasElems; i += kTcThreads) b_s[i] = gv.b32[i];
+    for (int i = tid; i < kBiasElems; i += L::kThreads) b_s[i] = gv.b32[i];
     if (gt == 0) {
         s_fail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
@@ -160,7 +204,7 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemCols));
+                     "r"(L::kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     fence_async_smem();
@@ -173,30 +217,24 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     bool failed = false;
 
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    const uint32_t stride = gridDim.x * kTcGroups;
-    for (uint32_t tile = blockIdx.x * kTcGroups + g; tile < tiles && !failed; tile += stride) {
+    const uint32_t stride = gridDim.x * G;
+    for (uint32_t tile = blockIdx.x * G + g; tile < tiles && !failed; tile += stride) {
         const uint32_t row = tile * kTcRows + gt;
         uint32_t key = 0;
-        float y[kOut];
         {
             float f[9] = { 0.5f, 0.5f, 0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 1.0f };
             if (row < n) rows.features(row, f, key);
-            __align__(16) __nv_bfloat16 enc[kIn];
-            encode_row(f, enc);
-#pragma unroll
-            for (int kc = 0; kc < kIn / 8; ++kc)
-                *reinterpret_cast<int4*>(buf[0] + core_offset(gt, kc * 8, kIn)) = *reinterpret_cast<const int4*>(enc + kc * 8);
+            encode_row_tile(f, buf, (uint32_t)gt);
         }
         fence_async_smem();
         tc_fence_before();
         group_sync(g);
         tc_fence_after();
+        float y[Rows::kStaged ? 1 : kOut];
         for (int l = 0; l < kLayers; ++l) {
             const uint32_t kdim = layer_in(l), ndim = layer_out(l);
-            const unsigned char* a_buf = buf[l & 1];       // layer l reads A, H, A, H, A
-            unsigned char* o_buf = buf[(l + 1) & 1];       // and writes H, A, H, A
             if (gt == 0) {
-                const uint32_t a0 = smem_u32(a_buf), b0 = smem_u32(w_s + tc_w_offset(l));
+                const uint32_t a0 = smem_u32(buf), b0 = smem_u32(w_s + tc_w_offset(l));
                 for (uint32_t k = 0; k < kdim / 16; ++k)
                     mma_bf16(tmem, smem_desc(a0 + 256 * k, 128, kdim * 16), smem_desc(b0 + 256 * k, 128, kdim * 16),
                              instr_desc(ndim), k > 0 ? 1u : 0u);
@@ -213,8 +251,10 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
                 failed = true;
                 break;
             }
-            // epilogue: this warp's 32 rows (TMEM lanes 32 (warp % 4) ..), 16 columns at a time
+            // epilogue: this warp's 32 rows (TMEM lanes 32 (warp % 4) ..), 16 columns at a time; the layer's MMAs
+            // have completed, so the operand buffer is free for the next layer's operand (or the staged outputs)
             const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            float* st = reinterpret_cast<float*>(buf);
             for (uint32_t c0 = 0; c0 < ndim; c0 += 16) {
                 float v[16];
                 tmem_ld16(lane_base + c0, v);
@@ -224,9 +264,14 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
                     __align__(16) __nv_bfloat16 hv[16];
 #pragma unroll
                     for (int i = 0; i < 16; ++i) hv[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[i], 0.0f));
-                    *reinterpret_cast<int4*>(o_buf + core_offset(gt, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(o_buf + core_offset(gt, c0 + 8, kHid)) =
-                        *reinterpret_cast<const int4*>(hv + 8);
+                    *reinterpret_cast<int4*>(buf + core_offset(gt, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
+                    *reinterpret_cast<int4*>(buf + core_offset(gt, c0 + 8, kHid)) = *reinterpret_cast<const int4*>(hv + 8);
+                } else if constexpr (Rows::kStaged) {
+                    // fp32 outputs row-major over the consumed operand
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4)
+                        *reinterpret_cast<float4*>(st + gt * kOut + c0 + i) =
+                            make_float4(v[i] + bias[i], v[i + 1] + bias[i + 1], v[i + 2] + bias[i + 2], v[i + 3] + bias[i + 3]);
                 } else {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[c0 + i] = v[i] + bias[i];
@@ -234,11 +279,6 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
             }
             if (l == kLayers - 1) {
                 if constexpr (Rows::kStaged) {
-                    // the last MMA has read A: stage the fp32 outputs there, row-major
-                    float* st = reinterpret_cast<float*>(buf[0]);
-#pragma unroll
-                    for (int i = 0; i < kOut; i += 4)
-                        *reinterpret_cast<float4*>(st + gt * kOut + i) = make_float4(y[i], y[i + 1], y[i + 2], y[i + 3]);
                     group_sync(g);
                     const uint32_t row0 = tile * kTcRows;
                     rows.store_tile(row0, min((uint32_t)kTcRows, n - row0), st, gt, kTcGroupThreads);
@@ -259,11 +299,11 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTmemCols));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(L::kTmemCols));
 }
 
-
-constexpr size_t forward_tc_smem() { return (size_t)kTcSmem; }
+template <int G>
+constexpr size_t forward_tc_smem() { return (size_t)TcLayout<G>::kSmem; }
 
 }  // namespace guide
 }  // namespace pb2

@@ -293,10 +293,11 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t* counter) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
+// Adds the active lanes' v to a 64-bit counter with one atomic per warp (any subset of lanes may call it).
 __device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t v) {
     const unsigned mask = __activemask();
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
-    if ((int)(threadIdx.x & 31u) == __ffs(mask) - 1) atomicAdd(counter, (unsigned long long)v);
+    const uint32_t sum = __reduce_add_sync(mask, v);
+    if ((int)(threadIdx.x & 31u) == __ffs(mask) - 1) atomicAdd(counter, (unsigned long long)sum);
 }
 
 // Debug index checks (LaunchParams::checks): the first failure is recorded and the access skipped.
@@ -553,7 +554,13 @@ __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, 
     if constexpr (Ctx::kBatch) {
         const uint32_t scene = ps.scene[slot];
         ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
-        if (atomicSub(&ctx.remaining[scene], 1u) == 1u) ctx.done_ns[scene] = globaltimer();
+        // one atomic per scene among the lanes finishing together (every finished path of a scene counts the
+        // same word down, so a per-path atomic serialises at that word's L2 slice)
+        const unsigned grp = __match_any_sync(__activemask(), scene);
+        if ((int)(threadIdx.x & 31u) == __ffs(grp) - 1) {
+            const uint32_t cnt = (uint32_t)__popc(grp);
+            if (atomicSub(&ctx.remaining[scene], cnt) == cnt) ctx.done_ns[scene] = globaltimer();
+        }
     } else {
         if (ctx.sample_out) {  // at the path's launch-relative index (a slot serves many paths)
             float* o = ctx.sample_out + 5 * (size_t)ps.scene[slot];
@@ -1024,10 +1031,11 @@ struct GuideRows {
 };
 
 // The guide's mixture for every vertex of the guided material types, on the tcgen05 tensor cores.
-__global__ void __launch_bounds__(guide::kTcThreads, 1) k_guide_infer(SceneView sv, Paths ps, GuideState gs) {
+__global__ void __launch_bounds__(guide::TcLayout<guide::kTcGroupsInfer>::kThreads, 1) k_guide_infer(SceneView sv, Paths ps,
+                                                                                               GuideState gs) {
     extern __shared__ __align__(1024) unsigned char smem[];
     GuideRows rows{ sv, ps, gs };
-    guide::forward_tc_tiles(gs.net, ps.counts[C_GUIDE], rows, ps.counts + C_TC_ERROR, smem);
+    guide::forward_tc_tiles<guide::kTcGroupsInfer>(gs.net, ps.counts[C_GUIDE], rows, ps.counts + C_TC_ERROR, smem);
 }
 
 // Per spatial cell (res^3 cells over the scene box) sum and count of the records' weights.
@@ -1362,7 +1370,7 @@ static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
     return PB2_OK;
 }
 
-static size_t infer_smem() { return guide::forward_tc_smem(); }
+static size_t infer_smem() { return guide::forward_tc_smem<guide::kTcGroupsInfer>(); }
 
 // Carves the SoA path state of `c` slots out of `base` (or only measures it when base is null); returns the
 // bytes used.  `batch` adds the per-slot scene ids and the two freed-slot queues.
@@ -1911,7 +1919,8 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         checked("k_trace_queue<extend>");
         k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
         checked("k_classify");
-        if (gs.enabled) k_guide_infer<<<pl->sms, guide::kTcThreads, infer_smem(), stream>>>(sv, ps, gs);
+        if (gs.enabled)
+            k_guide_infer<<<pl->sms, guide::TcLayout<guide::kTcGroupsInfer>::kThreads, infer_smem(), stream>>>(sv, ps, gs);
         checked("k_guide_infer");
         // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
         const uint32_t tm = pl->type_mask;
@@ -2523,15 +2532,19 @@ int pb2_batch_autotune(pb2_batch* b, void* stream_ptr, pb2_batch_config* chosen,
     cudaStream_t stream;
     if (const int rc = batch_stream(b, stream_ptr, &stream)) return rc;
     const pb2_batch_config base = b->config;
-    // Candidates are scored by path vertices shaded per ms over a fixed number of iterations from a fresh
-    // start (the fill phase included, as in a real render): capacity first, then the launch shapes.
+    // Candidates are scored by path vertices shaded per ms over 24 iterations after 16 from a fresh start: the
+    // wavefront has filled and holds paths of as many scenes as the capacity lets in, as through most of a render
+    // (a score over the fill alone favours the largest capacity, whose full wavefront then mixes more scenes'
+    // trees in the cache and renders slower).  Capacity first, then the launch shapes.
     auto score = [&](const pb2_batch_config& c, double* out) -> int {
         b->config = c;
         int rc = batch_reset(b, stream);
         if (rc) return rc;
         float ms = 0.0f;
+        if ((rc = batch_run(b, stream, 16, &ms))) return rc;
+        const unsigned long long v0 = b->stats.path_vertices;
         if ((rc = batch_run(b, stream, 24, &ms))) return rc;
-        *out = ms > 0.0f ? (double)b->stats.path_vertices / ms : 0.0;
+        *out = ms > 0.0f ? (double)(b->stats.path_vertices - v0) / ms : 0.0;
         return PB2_OK;
     };
     const auto t0 = std::chrono::steady_clock::now();
@@ -2547,7 +2560,7 @@ int pb2_batch_autotune(pb2_batch* b, void* stream_ptr, pb2_batch_config* chosen,
         }
         return PB2_OK;
     };
-    const uint32_t caps[] = { 1u << 20, 1u << 21, 1u << 22, 1u << 23 };
+    const uint32_t caps[] = { 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23 };
     for (uint32_t cap : caps) {
         if (cap > std::max<unsigned long long>(b->total_paths, 1u << 20)) break;
         pb2_batch_config c = base;
