@@ -584,8 +584,11 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 // Turns the path's pending guided vertices into training records: the incident radiance estimate along
 // the sampled direction is (radiance gathered after the vertex) / (throughput before the vertex's
 // sampling) x pdf / (f cos), so target / pdf = lum(S_end - S_v) / lum(pf_v).
+// The two record counters are shared by every path of the launch, so both are added to once per warp, not once per
+// record.
 __device__ __forceinline__ void flush_records(const GuideState& gs, uint32_t slot, float4 s_end) {
     const uint32_t n = gs.nrec[slot];
+    uint32_t seen = 0;
     for (uint32_t r = 0; r < n; ++r) {
         const float4 a = gs.rec[(r * 5 + 0) * gs.cap + slot];
         const float4 b = gs.rec[(r * 5 + 1) * gs.cap + slot];
@@ -597,10 +600,10 @@ __device__ __forceinline__ void flush_records(const GuideState& gs, uint32_t slo
         if (!(dl > 0.f && lpf > 0.f)) continue;
         const float w = dl / lpf;
         if (!(w < 3.0e38f)) continue;
-        atomicAdd(&gs.train_count[1], 1u);
+        ++seen;
         const float u = (float)(hash32(slot * 3u + r + gs.salt * 0x9E3779B9u) >> 8) * (1.0f / 16777216.0f);
         if (u >= gs.accept_prob) continue;
-        const uint32_t idx = atomicAdd(&gs.train_count[0], 1u);
+        const uint32_t idx = warp_push(&gs.train_count[0]);
         if (idx >= gs.train_capacity) continue;
         float4* o = reinterpret_cast<float4*>(gs.train + 16 * (size_t)idx);
         o[0] = make_float4(a.x, a.y, a.z, a.w);
@@ -608,6 +611,9 @@ __device__ __forceinline__ void flush_records(const GuideState& gs, uint32_t slo
         o[2] = make_float4(c.x, c.y, c.z, c.w);
         o[3] = make_float4(w, 0.f, 0.f, 0.f);
     }
+    const unsigned mask = __activemask();
+    const uint32_t seen_warp = __reduce_add_sync(mask, seen);
+    if ((int)(threadIdx.x & 31u) == __ffs(mask) - 1 && seen_warp) atomicAdd(&gs.train_count[1], seen_warp);
     gs.nrec[slot] = 0;
 }
 
