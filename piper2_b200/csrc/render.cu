@@ -786,8 +786,12 @@ __host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_
 // sweep of register budgets for 4-8 resident 128-thread blocks changed render times by under 2 %.)
 // kGuided: the variant launched while a guide is attached (guided sampling and training records compiled in);
 // plain launches use the variant without them, which needs fewer registers.
+// The plain variants are held to 64 registers (__launch_bounds__(512, 2): two 512-thread blocks, or eight of 128,
+// per SM): the kernel is latency-bound, and the texture lookups had taken the Matte variant to 72 registers and
+// 28 resident warps.
 template <int kType, class Ctx, bool kGuided = false>
-__global__ void k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs, uint32_t cur) {
+__global__ void __launch_bounds__(512, kGuided ? 1 : 2) k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs,
+                                                                 uint32_t cur) {
     const uint32_t n = ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
