@@ -645,8 +645,10 @@ __global__ void k_classify(const __grid_constant__ Ctx ctx, Paths ps, GuideState
             PB2_CHECK(sv.prim_material[prim] < sv.material_count, 4, K_CLASSIFY, slot, sv.prim_material[prim]);
             const uint32_t type = sv.materials[sv.prim_material[prim]].type;
             PB2_CHECK(type < (uint32_t)kNumSurfaceTypes, 5, K_CLASSIFY, slot, type);
-            ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
+            // a vertex that samples the guide is shaded by its type's guided kernel over the guide queue, every
+            // other one by the plain kernel over its type's queue
             if (guide_vertex(gs, type, ps.depth[slot])) ps.guide_q[warp_push(&ps.counts[C_GUIDE])] = slot;
+            else ps.surf[type][warp_push(&ps.counts[C_SURF0 + type])] = slot;
             continue;
         }
         // a miss or an area light: emission on specular paths, pass-through, termination
@@ -792,18 +794,23 @@ __host__ __device__ constexpr bool guided_type(int t) { return t == PB2_SURFACE_
 template <int kType, class Ctx, bool kGuided = false>
 __global__ void __launch_bounds__(512, kGuided ? 1 : 2) k_shade(const __grid_constant__ Ctx ctx, Paths ps, GuideState gs,
                                                                  uint32_t cur) {
-    const uint32_t n = ps.counts[C_SURF0 + kType];
+    // the guided variant shades the guide queue (the vertices of the guided types that sample the guide), taking
+    // the vertices of its own type; the plain variant shades its type's queue
+    const uint32_t* queue = kGuided ? ps.guide_q : ps.surf[kType];
+    const uint32_t n = kGuided ? ps.counts[C_GUIDE] : ps.counts[C_SURF0 + kType];
     uint32_t vertices = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PB2_CHECK(n <= ctx.capacity(), 10, K_SHADE, 0, n);
-        const uint32_t slot = ps.surf[kType][i];
+        const uint32_t slot = queue[i];
         PB2_CHECK(slot < ctx.capacity(), 11, K_SHADE, slot, i);
         const LaunchParams& lp = ctx.P(slot);
         const SceneView& sv = ctx.S(slot);
-        ++vertices;
         const float4 h = ps.hit[slot];
         const uint32_t prim = __float_as_uint(h.y);
         PB2_CHECK(prim < sv.bvh.tri_count, 12, K_SHADE, slot, prim);
+        if constexpr (kGuided)
+            if (sv.materials[sv.prim_material[prim]].type != (uint32_t)kType) continue;  // another guided type's vertex
+        ++vertices;
         PB2_CHECK(ps.hit_slot[slot] < sv.bvh.tri_count, 13, K_SHADE, slot, ps.hit_slot[slot]);
         PB2_CHECK(ps.dim[slot] <= PB2_SOBOL_DIMS, 14, K_SHADE, slot, ps.dim[slot]);
         const float4 o4 = ps.o[slot], d4 = ps.d[slot], pf4 = ps.pf[slot];
@@ -1935,8 +1942,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
         // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
         const uint32_t tm = pl->type_mask;
         if (tm & (1u << PB2_SURFACE_MATTE)) {
-            if (gs.enabled) k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            else k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            if (gs.enabled && ((gs.types >> PB2_SURFACE_MATTE) & 1u))
+                k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<matte>");
         }
         if (tm & (1u << PB2_SURFACE_PLASTIC)) {
@@ -1956,9 +1964,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             checked("k_shade<substrate>");
         }
         if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
-            if (gs.enabled)
+            k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
+            if (gs.enabled && ((gs.types >> PB2_SURFACE_CONDUCTOR) & 1u))
                 k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            else k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
             checked("k_shade<conductor>");
         }
         if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
