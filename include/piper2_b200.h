@@ -423,11 +423,16 @@ int pb2_guide_set_params(pb2_guide* guide, const float* params_host, uint32_t co
 int pb2_guide_get_params(const pb2_guide* guide, float* params_host, uint32_t count);
 /* features_dev (16-byte aligned): n rows of 12 floats (position in the unit cube xyz, normal xyz, outgoing dir xyz, unused);
  * out_dev (16-byte aligned): n rows of 48 raw outputs (8 x (weight logit, mean xyz, concentration), 8 unused).
- * Runs on the tcgen05 tensor cores (four independent 128-row tiles per CTA, TMEM accumulators); synchronises
- * `stream` to check that no tensor-core wait timed out (PB2_ERR_DEVICE_TIMEOUT). */
+ * Runs on the tcgen05 tensor cores (one CTA per SM of seven independent 128-row warp groups, TMEM
+ * accumulators); synchronises `stream` to check that no tensor-core wait timed out (PB2_ERR_DEVICE_TIMEOUT). */
 int pb2_guide_forward(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev, void* stream);
+/* pb2_guide_forward without the host synchronisation, for work queued on a stream or captured in a CUDA graph
+ * (no reference counterpart): a tensor-core wait that timed out sets *status_dev (a device word) to 1; the
+ * caller clears it beforehand and reads it after synchronising.  Nothing is allocated. */
+int pb2_guide_forward_async(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev,
+                            uint32_t* status_dev, void* stream);
 /* The same forward pass on mma.sync tiles (16 rows per warp), asynchronous; the cross-check of the tcgen05
- * path and the form the integrator's per-bounce inference uses. */
+ * path. */
 int pb2_guide_forward_mma(const pb2_guide* guide, const float* features_dev, uint32_t n, float* out_dev,
                           void* stream);
 /* records_dev: n rows of 16 floats (position xyz, normal xyz, outgoing xyz, sampled direction xyz, weight =

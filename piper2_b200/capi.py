@@ -187,6 +187,7 @@ SIGNATURES = [
     ("pb2_guide_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("pb2_guide_get_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("pb2_guide_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("pb2_guide_forward_async", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pb2_guide_forward_mma", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("pb2_guide_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_float),
                                       C.c_void_p]),

@@ -467,6 +467,17 @@ int pb2_guide_forward(const pb2_guide* g, const float* features, uint32_t n, flo
     return PB2_OK;
 }
 
+int pb2_guide_forward_async(const pb2_guide* g, const float* features, uint32_t n, float* out, uint32_t* status,
+                            void* stream) {
+    if (!g || !status || (n && (!features || !out)))
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward_async: null argument");
+    if (n == 0) return PB2_OK;
+    if ((reinterpret_cast<uintptr_t>(features) | reinterpret_cast<uintptr_t>(out)) & 15u)
+        return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward_async: features and outputs must be 16-byte aligned");
+    const cudaError_t e = guide_forward_tc(g->view(), features, n, out, status, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PB2_OK : cuda_fail(e, "pb2_guide_forward_async");
+}
+
 int pb2_guide_forward_mma(const pb2_guide* g, const float* features, uint32_t n, float* out, void* stream) {
     if (!g || (n && (!features || !out))) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_guide_forward_mma: null argument");
     const cudaError_t e = guide_forward(g->view(), features, n, out, static_cast<cudaStream_t>(stream));

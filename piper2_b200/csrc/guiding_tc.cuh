@@ -9,9 +9,10 @@
 // layout.  For each layer one thread of the group issues K/16 `tcgen05.mma.cta_group::1.kind::f16`
 // (M = 128, N = 64 or 48, BF16 x BF16 -> FP32) into the group's 64 TMEM columns and commits them to the
 // group's mbarrier; every warp of the group then reads its 32 rows back with `tcgen05.ld.32x32b`, adds the
-// bias, applies ReLU, and writes the next layer's bf16 operand over the one the completed MMAs read (a group has
-// one operand buffer), and after the last layer the buffer stages the fp32 outputs so that a row-major output
-// is written with coalesced stores.  Shared-memory writes that
+// bias, and writes the next layer's bf16 operand (ReLU and rounding of two columns in one `cvt.rn.relu.bf16x2`)
+// over the one the completed MMAs read (a group has one operand buffer), and after the last layer the buffer
+// stages the fp32 outputs so that a row-major output is written with coalesced stores.  Each thread loads its
+// next tile's input row while the current tile's layers run.  Shared-memory writes that
 // an MMA reads are made visible to the tensor core's async proxy with `fence.proxy.async.shared::cta`
 // before the group's named barrier.
 //
@@ -125,6 +126,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Two floats rounded to bf16 and packed (lo in the low half), with and without ReLU; `cvt.rn.relu` clamps the
+// rounded value at 0, which for any float equals rounding max(x, 0).
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ uint32_t pack_relu_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -152,16 +166,16 @@ __device__ __forceinline__ void encode_row_tile(const float (&f)[9], unsigned ch
     s[6] = fminf(fmaxf(ph, 0.f), 1.f) * 12.f;
 #pragma unroll
     for (int kc = 0; kc < kIn / 8; ++kc) {
-        __align__(16) __nv_bfloat16 v[8];
+        float x[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int e = kc * 8 + i;
-            float x = 0.f;
-            if (e < 84) x = fmaxf(0.f, 1.f - fabsf(s[e / 12] - ((float)(e % 12) + 0.5f)));
-            else if (e == 84) x = 1.f;
-            v[i] = __float2bfloat16_rn(x);
+            x[i] = 0.f;
+            if (e < 84) x[i] = fmaxf(0.f, 1.f - fabsf(s[e / 12] - ((float)(e % 12) + 0.5f)));
+            else if (e == 84) x[i] = 1.f;
         }
-        *reinterpret_cast<int4*>(tile + core_offset(row, kc * 8, kIn)) = *reinterpret_cast<const int4*>(v);
+        *reinterpret_cast<uint4*>(tile + core_offset(row, kc * 8, kIn)) =
+            make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), pack_bf16x2(x[6], x[7]));
     }
 }
 
@@ -218,13 +232,20 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
 
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
     const uint32_t stride = gridDim.x * G;
+    // the next tile's input row is loaded while this tile's layers run
+    float fn[9] = { 0.5f, 0.5f, 0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 1.0f };
+    uint32_t key_next = 0;
+    {
+        const uint32_t row0 = (blockIdx.x * G + g) * kTcRows + gt;
+        if (row0 < n) rows.features(row0, fn, key_next);
+    }
     for (uint32_t tile = blockIdx.x * G + g; tile < tiles && !failed; tile += stride) {
         const uint32_t row = tile * kTcRows + gt;
-        uint32_t key = 0;
+        encode_row_tile(fn, buf, (uint32_t)gt);
+        const uint32_t key = key_next;
         {
-            float f[9] = { 0.5f, 0.5f, 0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 1.0f };
-            if (row < n) rows.features(row, f, key);
-            encode_row_tile(f, buf, (uint32_t)gt);
+            const uint32_t nrow = (tile + stride) * kTcRows + gt;
+            if (tile + stride < tiles && nrow < n) rows.features(nrow, fn, key_next);
         }
         fence_async_smem();
         tc_fence_before();
@@ -246,11 +267,7 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
             }
             phase ^= 1u;
             tc_fence_after();
-            group_sync(g);
-            if (s_fail) {
-                failed = true;
-                break;
-            }
+            // (a wait that gave up is agreed on at the group barrier after the epilogue, which every thread reaches)
             // epilogue: this warp's 32 rows (TMEM lanes 32 (warp % 4) ..), 16 columns at a time; the layer's MMAs
             // have completed, so the operand buffer is free for the next layer's operand (or the staged outputs)
             const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
@@ -261,11 +278,12 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
                 tmem_wait_ld();
                 const float* bias = b_s + bias_offset(l) + c0;
                 if (l < kLayers - 1) {
-                    __align__(16) __nv_bfloat16 hv[16];
+                    // bias, ReLU and the bf16 rounding of two columns per instruction
+                    uint32_t hw[8];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) hv[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[i], 0.0f));
-                    *reinterpret_cast<int4*>(buf + core_offset(gt, c0, kHid)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(buf + core_offset(gt, c0 + 8, kHid)) = *reinterpret_cast<const int4*>(hv + 8);
+                    for (int i = 0; i < 8; ++i) hw[i] = pack_relu_bf16x2(v[2 * i] + bias[2 * i], v[2 * i + 1] + bias[2 * i + 1]);
+                    *reinterpret_cast<uint4*>(buf + core_offset(gt, c0, kHid)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(buf + core_offset(gt, c0 + 8, kHid)) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
                 } else if constexpr (Rows::kStaged) {
                     // fp32 outputs row-major over the consumed operand
 #pragma unroll
@@ -290,6 +308,10 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
             tc_fence_before();
             group_sync(g);
             tc_fence_after();
+            if (s_fail) {
+                failed = true;
+                break;
+            }
         }
     }
     if (failed && gt == 0) {

@@ -102,6 +102,42 @@ def test_forward_tcgen05_matches_mma_tiles(n):
     assert np.array_equal(g.forward(f, tiles="tcgen05"), tc)
 
 
+@pytest.mark.parametrize("n", [1, 129, 7 * 148 * 128 + 5, 3 * 7 * 148 * 128 + 77])
+def test_forward_async_equals_forward(n):
+    """pb2_guide_forward_async (no host synchronisation, time-out flag in a caller's device word) writes the
+    outputs of pb2_guide_forward bit for bit; sizes beyond one tile per warp group of every SM run the loop that
+    loads the next tile's rows during the current tile's layers."""
+    import ctypes as C
+
+    import torch
+
+    from piper2_b200 import capi
+
+    api = _api()
+    rng = np.random.default_rng(2000 + n)
+    g = api.Guide(seed=5)
+    params = _trained_params(5)
+    g.set_params(params)
+    f = _features(rng, n)
+    ref = g.forward(f)
+    feat = torch.from_numpy(f).cuda()
+    out = torch.full((n, 48), float("nan"), dtype=torch.float32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    capi.check(capi.lib().pb2_guide_forward_async(g.h, C.c_void_p(feat.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                                  C.c_void_p(status.data_ptr()), stream))
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    y = out.cpu().numpy()
+    assert np.array_equal(y.view(np.uint32), ref.view(np.uint32))
+    if n > 100000:  # the last rows against the float64 model with the kernel's roundings
+        tail = slice(n - 4096, n)
+        r = _forward_bf16(params, f[tail])
+        assert np.linalg.norm(y[tail, :40] - r[:, :40]) / np.linalg.norm(r[:, :40]) <= 5e-3
+    assert capi.lib().pb2_guide_forward_async(g.h, C.c_void_p(feat.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                              None, stream) == capi.PB2_ERR_INVALID_ARGUMENT
+
+
 def _records(rng, n, concentrated=False):
     f = _features(rng, n)
     wi = _unit(rng, n)
