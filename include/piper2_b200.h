@@ -397,6 +397,12 @@ int pb2_pipeline_get_trace_counters(const pb2_pipeline* pipeline, uint64_t* coun
  * state (about 260 bytes per slot, plus about 400 with a guide attached) stays bounded.  The samples and
  * the film are those of the same launch without the bound.  Shrinking the bound frees the larger state. */
 int pb2_pipeline_set_path_slots(pb2_pipeline* pipeline, uint32_t slots);
+/* The bounce loop of a single-scene launch as CUDA graphs (on by default; no reference counterpart, the
+ * reference runs one CPU task per pixel and sample): after the first four bounces, every four bounces
+ * (between two host checks of the extend queue) replay one graph, captured for the launch's parameters on
+ * the pipeline's own stream and updated in place from launch to launch.  Off: plain launches (the form
+ * PB2_DEBUG_SYNC=1 always uses).  Samples and films are the same either way. */
+int pb2_pipeline_set_graphs(pb2_pipeline* pipeline, int enabled);
 /* Resolve radiance = rgb / w (FixedSampler.cpp:122-131) into rgb_dev (width * height * 3). */
 int pb2_film_resolve(const float* rgbw_dev, uint32_t pixel_count, float* rgb_dev, void* stream);
 int pb2_pipeline_get_stats(const pb2_pipeline* pipeline, pb2_launch_stats* stats, void* stream);

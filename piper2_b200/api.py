@@ -271,6 +271,10 @@ class Pipeline:
         """Bound the path slots in flight; a larger launch refills freed slots with its remaining paths."""
         capi.check(capi.lib().pb2_pipeline_set_path_slots(self.h, int(slots)))
 
+    def set_graphs(self, enable: bool):
+        """Run the bounce loop of later launches as CUDA graphs (the default) or as plain launches."""
+        capi.check(capi.lib().pb2_pipeline_set_graphs(self.h, 1 if enable else 0))
+
     def resolve(self, film):
         torch = _torch()
         rgb = torch.empty((self.settings.height, self.settings.width, 3), dtype=torch.float32, device="cuda")

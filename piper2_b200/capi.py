@@ -197,6 +197,7 @@ SIGNATURES = [
     ("pb2_guide_set_gradient_hook", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pb2_pipeline_set_guide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(GuideSettings)]),
     ("pb2_pipeline_set_path_slots", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pb2_pipeline_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("pb2_pipeline_set_counting", C.c_int, [C.c_void_p, C.c_int]),
     ("pb2_pipeline_get_trace_counters", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pb2_pipeline_set_guide_dump", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),

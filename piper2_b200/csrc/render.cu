@@ -1368,6 +1368,11 @@ struct pb2_pipeline {
     uint32_t g_train_capacity = 0, g_batch_capacity = 0;
     uint32_t g_offered = 0;  // records offered by the launches since the last training call (host estimate)
     uint32_t g_salt = 0;
+    // CUDA graphs of the bounce loop (pb2_pipeline_set_graphs): 0 refills freed slots, 1 drains; the stream
+    // they are captured on
+    bool use_graphs = true;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec[2] = { nullptr, nullptr };
 };
 
 static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
@@ -1738,7 +1743,16 @@ int pb2_pipeline_destroy(pb2_pipeline* pl) {
     cudaFree(pl->g_train);
     cudaFree(pl->g_batch);
     cudaFree(pl->g_count);
+    for (cudaGraphExec_t& x : pl->gexec)
+        if (x) cudaGraphExecDestroy(x);
+    if (pl->cap_stream) cudaStreamDestroy(pl->cap_stream);
     delete pl;
+    return PB2_OK;
+}
+
+int pb2_pipeline_set_graphs(pb2_pipeline* pl, int enabled) {
+    if (!pl) return fail(PB2_ERR_INVALID_ARGUMENT, "pb2_pipeline_set_graphs: null pipeline");
+    pl->use_graphs = enabled != 0;
     return PB2_OK;
 }
 
@@ -1872,7 +1886,6 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     const int qblocks = resident_grid_cached((const void*)k_trace_queue<Q_EXTEND, SingleCtx>, kQThreads, 0, qcache);
     const int qblocks_any =
         resident_grid_cached((const void*)k_trace_queue<Q_SHADOW, SingleCtx>, kQThreads, 0, qcache_any);
-    uint32_t cur = 0;
     // generous bound: every path needs at most (max depth + light pass-throughs) bounces, and a slot serves
     // about paths / slots of them one after another
     const uint64_t max_bounces = (paths / slots + 2) * (4ull * (pl->settings.max_depth + 2) + 64);
@@ -1901,9 +1914,117 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     // every kCheckEvery bounces (a bounce with empty queues costs only its launches) and the launches of
     // the bounces between checks queue up without a host round trip.
     constexpr int kCheckEvery = 4;
+    // one bounce on stream `s` with extend-queue parity `c`; `refill_step` first starts the launch's next paths in
+    // the slots the previous bounce freed
+    auto bounce = [&](cudaStream_t s, bool refill_step, uint32_t c) {
+        if (refill_step) {
+            k_batch_claim<<<1, 1, 0, s>>>(ps, pl->refill, c, work);  // also clears the trace work counters
+            k_single_regen<<<grid, 256, 0, s>>>(lp, ps, gs, pl->refill, c);
+            checked("k_single_regen");
+        } else {
+            cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, s);
+        }
+        // the persistent trace blocks stop when the queue is drained
+        const int qgrid = qblocks;
+        if (pl->trace_counters)
+            k_trace_queue<Q_EXTEND, SingleCtx, true><<<qgrid, kQThreads, 0, s>>>(
+                ctx, ps, ps.ext[c], ps.counts + C_EXT_CUR, work, stats, pl->trace_counters);
+        else
+            k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, s>>>(ctx, ps, ps.ext[c], ps.counts + C_EXT_CUR, work,
+                                                                     stats);
+        checked("k_trace_queue<extend>");
+        k_classify<<<grid, 256, 0, s>>>(ctx, ps, gs, c);
+        checked("k_classify");
+        if (gs.enabled)
+            k_guide_infer<<<pl->sms, guide::TcLayout<guide::kTcGroupsInfer>::kThreads, infer_smem(), s>>>(sv, ps, gs);
+        checked("k_guide_infer");
+        // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
+        const uint32_t tm = pl->type_mask;
+        if (tm & (1u << PB2_SURFACE_MATTE)) {
+            k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            if (gs.enabled && ((gs.types >> PB2_SURFACE_MATTE) & 1u))
+                k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<matte>");
+        }
+        if (tm & (1u << PB2_SURFACE_PLASTIC)) {
+            k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<plastic>");
+        }
+        if (tm & (1u << PB2_SURFACE_GLASS)) {
+            k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<glass>");
+        }
+        if (tm & (1u << PB2_SURFACE_MIRROR)) {
+            k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<mirror>");
+        }
+        if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
+            k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<substrate>");
+        }
+        if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
+            k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            if (gs.enabled && ((gs.types >> PB2_SURFACE_CONDUCTOR) & 1u))
+                k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<conductor>");
+        }
+        if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
+            k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, s>>>(ctx, ps, gs, c);
+            checked("k_shade<blackbody>");
+        }
+        if (pl->trace_counters)
+            k_trace_queue<Q_SHADOW, SingleCtx, true><<<qblocks_any, kQThreads, 0, s>>>(
+                ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1, sstats, pl->trace_counters);
+        else
+            k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, s>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
+                                                                           work + 1, sstats);
+        checked("k_trace_queue<shadow>");
+        if (pl->trace_counters)
+            k_trace_queue<Q_MIS, SingleCtx, true><<<qblocks_any, kQThreads, 0, s>>>(
+                ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats, pl->trace_counters);
+        else
+            k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, s>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
+                                                                        stats);
+        checked("k_trace_queue<mis>");
+        k_finish<<<grid, 256, 0, s>>>(ctx, ps, gs, c);
+        checked("k_finish");
+        k_advance<<<1, 1, 0, s>>>(ps.counts);
+        checked("k_advance");
+    };
+    // CUDA graphs of kCheckEvery bounces (parities 0, 1, 0, 1; graph 0 refills, graph 1 drains), captured on the
+    // pipeline's own stream for this launch's parameters and updated in place when the pipeline already holds a
+    // graph of the same shape.  The first kCheckEvery bounces run as plain launches, and the graph the next ones
+    // need is captured while the device runs them.
+    const bool graphs = pl->use_graphs && !debug_sync;
+    bool captured[2] = { false, false };
+    auto capture = [&](int mode) -> cudaError_t {
+        cudaError_t err;
+        if (!pl->cap_stream && (err = cudaStreamCreateWithFlags(&pl->cap_stream, cudaStreamNonBlocking))) return err;
+        if ((err = cudaStreamBeginCapture(pl->cap_stream, cudaStreamCaptureModeThreadLocal))) return err;
+        for (int k = 0; k < kCheckEvery; ++k) bounce(pl->cap_stream, mode == 0, (uint32_t)(k & 1));
+        const cudaError_t le = cudaGetLastError();
+        cudaGraph_t g = nullptr;
+        err = cudaStreamEndCapture(pl->cap_stream, &g);
+        if (le != cudaSuccess || err != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return le != cudaSuccess ? le : err;
+        }
+        if (pl->gexec[mode]) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(pl->gexec[mode], g, &info) != cudaSuccess) {
+                cudaGetLastError();  // a graph of another shape: instantiate anew
+                cudaGraphExecDestroy(pl->gexec[mode]);
+                pl->gexec[mode] = nullptr;
+            }
+        }
+        err = pl->gexec[mode] ? cudaSuccess : cudaGraphInstantiate(&pl->gexec[mode], g, 0);
+        cudaGraphDestroy(g);
+        if (err == cudaSuccess) captured[mode] = true;
+        return err;
+    };
     bool refilling = true;
-    for (uint64_t bounce = 0; !failed; ++bounce) {
-        if (bounce % kCheckEvery == 0 && bounce > 0) {
+    for (uint64_t group = 0; !failed; ++group) {
+        if (group > 0) {
             uint32_t active = 0;
             unsigned long long next = paths;  // once every path has started, only the queue is read
             if ((e = cudaMemcpyAsync(&active, ps.counts + C_EXT_CUR, sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -1915,84 +2036,20 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
             if (active == 0 && next == paths) break;
             if (next == paths) refilling = false;  // every path has been started
         }
-        if (bounce > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
-        if (refilling) {
-            k_batch_claim<<<1, 1, 0, stream>>>(ps, pl->refill, cur, work);  // also clears the trace work counters
-            k_single_regen<<<grid, 256, 0, stream>>>(lp, ps, gs, pl->refill, cur);
-            checked("k_single_regen");
+        if (group * kCheckEvery > max_bounces) return fail(PB2_ERR_DEVICE_TIMEOUT, "path loop did not terminate");
+        const int mode = refilling ? 0 : 1;
+        if (graphs && group > 0) {
+            if (!captured[mode] && (e = capture(mode))) return cuda_fail(e, "capture of the bounce graph");
+            if ((e = cudaGraphLaunch(pl->gexec[mode], stream))) return cuda_fail(e, "bounce graph launch");
+            continue;
+        }
+        for (int k = 0; k < kCheckEvery && !failed; ++k) {
+            bounce(stream, refilling, (uint32_t)(k & 1));
             // all paths fit the slots: the first claim started every one of them
             if (slots == paths) refilling = false;
-        } else {
-            cudaMemsetAsync(work, 0, sizeof(uint32_t) * 3, stream);
+            if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
         }
-        // the persistent trace blocks stop when the queue is drained
-        const int qgrid = qblocks;
-        if (pl->trace_counters)
-            k_trace_queue<Q_EXTEND, SingleCtx, true><<<qgrid, kQThreads, 0, stream>>>(
-                ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work, stats, pl->trace_counters);
-        else
-            k_trace_queue<Q_EXTEND><<<qgrid, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, work,
-                                                                     stats);
-        checked("k_trace_queue<extend>");
-        k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_classify");
-        if (gs.enabled)
-            k_guide_infer<<<pl->sms, guide::TcLayout<guide::kTcGroupsInfer>::kThreads, infer_smem(), stream>>>(sv, ps, gs);
-        checked("k_guide_infer");
-        // one shading kernel per surface type the scene's materials use (the others' queues stay empty)
-        const uint32_t tm = pl->type_mask;
-        if (tm & (1u << PB2_SURFACE_MATTE)) {
-            k_shade<PB2_SURFACE_MATTE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            if (gs.enabled && ((gs.types >> PB2_SURFACE_MATTE) & 1u))
-                k_shade<PB2_SURFACE_MATTE, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<matte>");
-        }
-        if (tm & (1u << PB2_SURFACE_PLASTIC)) {
-            k_shade<PB2_SURFACE_PLASTIC><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<plastic>");
-        }
-        if (tm & (1u << PB2_SURFACE_GLASS)) {
-            k_shade<PB2_SURFACE_GLASS><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<glass>");
-        }
-        if (tm & (1u << PB2_SURFACE_MIRROR)) {
-            k_shade<PB2_SURFACE_MIRROR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<mirror>");
-        }
-        if (tm & (1u << PB2_SURFACE_SUBSTRATE)) {
-            k_shade<PB2_SURFACE_SUBSTRATE><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<substrate>");
-        }
-        if (tm & (1u << PB2_SURFACE_CONDUCTOR)) {
-            k_shade<PB2_SURFACE_CONDUCTOR><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            if (gs.enabled && ((gs.types >> PB2_SURFACE_CONDUCTOR) & 1u))
-                k_shade<PB2_SURFACE_CONDUCTOR, SingleCtx, true><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<conductor>");
-        }
-        if (tm & (1u << PB2_SURFACE_BLACKBODY)) {
-            k_shade<PB2_SURFACE_BLACKBODY><<<grid, 128, 0, stream>>>(ctx, ps, gs, cur);
-            checked("k_shade<blackbody>");
-        }
-        if (pl->trace_counters)
-            k_trace_queue<Q_SHADOW, SingleCtx, true><<<qblocks_any, kQThreads, 0, stream>>>(
-                ctx, ps, ps.shadow_q, ps.counts + C_SHADOW, work + 1, sstats, pl->trace_counters);
-        else
-            k_trace_queue<Q_SHADOW><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.shadow_q, ps.counts + C_SHADOW,
-                                                                           work + 1, sstats);
-        checked("k_trace_queue<shadow>");
-        if (pl->trace_counters)
-            k_trace_queue<Q_MIS, SingleCtx, true><<<qblocks_any, kQThreads, 0, stream>>>(
-                ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2, stats, pl->trace_counters);
-        else
-            k_trace_queue<Q_MIS><<<qblocks_any, kQThreads, 0, stream>>>(ctx, ps, ps.mis_q, ps.counts + C_MIS, work + 2,
-                                                                        stats);
-        checked("k_trace_queue<mis>");
-        k_finish<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);
-        checked("k_finish");
-        k_advance<<<1, 1, 0, stream>>>(ps.counts);
-        checked("k_advance");
-        if (!failed && (e = cudaGetLastError())) return cuda_fail(e, "bounce launch");
-        cur ^= 1u;
+        if (graphs && group == 0 && (e = capture(refilling ? 0 : 1))) return cuda_fail(e, "capture of the bounce graph");
     }
     if (failed) return fail(PB2_ERR_CUDA, std::string(failed) + ": " + cudaGetErrorString(e));
     uint32_t counts[C_COUNT];

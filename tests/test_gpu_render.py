@@ -316,3 +316,41 @@ def test_two_devices_in_one_process(oracle):
         assert np.array_equal(samples.view(np.uint32), osamples.view(np.uint32)), dev
     torch.cuda.set_device(0)
     capi.check(capi.lib().pb2_set_device(0))
+
+
+def test_bounce_graphs_equal_plain_launches(oracle):
+    """The bounce loop replayed as CUDA graphs (the default: every four bounces after the first four) gives the
+    samples of plain launches bit for bit, over launches in a row on one pipeline whose parameters change (a
+    sub-rect, another sample range, a slot bound that makes the launch refill), so the graphs are updated in
+    place from one launch to the next; the first launch is also checked against the oracle."""
+    import torch
+
+    from piper2_b200 import capi
+
+    sd = scenes.cornell_box(seed=4, width=48, height=32, spp=8)
+    full = capi.Rect(0, 0, 48, 32)
+    sub = capi.Rect(5, 3, 30, 20)
+    cases = [(full, 0, 8, None), (sub, 3, 5, 300), (full, 2, 6, 1 << 24), (full, 0, 8, None)]
+
+    def run(pl, graphs):
+        pl.set_graphs(graphs)
+        outs = []
+        for rect, begin, count, slots in cases:
+            if slots is not None:
+                pl.set_path_slots(slots)
+            film = pl.new_film()
+            out = torch.zeros((rect.height, rect.width, count, 5), dtype=torch.float32, device="cuda")
+            pl.launch(film, rect, sample_begin=begin, sample_count=count, sample_out=out)
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy())
+        return outs
+
+    with _api().Pipeline(sd) as pl:
+        plain = run(pl, False)
+        graphed = run(pl, True)
+        graphed_again = run(pl, True)
+    for k, (a, b, c) in enumerate(zip(plain, graphed, graphed_again)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"launch {k}: graphs differ from plain launches"
+        assert np.array_equal(a.view(np.uint32), c.view(np.uint32)), f"launch {k}: updated graphs differ"
+    _, osamples = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
+    assert np.array_equal(graphed[0].view(np.uint32), osamples.view(np.uint32))
