@@ -70,6 +70,9 @@ __device__ __forceinline__ bool mbar_wait_timed(uint32_t bar, uint32_t parity) {
     }
 }
 
+// A bf16 (low 16 bits of h) greater than zero: sign clear and not +0 (activations are ReLU outputs, never NaN).
+__device__ __forceinline__ bool bf16_positive(uint32_t h) { return h != 0u && (h & 0x8000u) == 0u; }
+
 // kind::f16 instruction descriptor with operand majorness: a_mn / b_mn = 1 reads that operand MN-major.
 __device__ __forceinline__ uint32_t instr_desc_major(uint32_t n, uint32_t a_mn, uint32_t b_mn) {
     return instr_desc(n) | (a_mn << 15) | (b_mn << 16);
@@ -210,13 +213,14 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
                 tmem_wait_ld();
                 const float* bias = b_s + bias_offset(l) + c0;
                 if (l < kLayers - 1) {
-                    __align__(16) __nv_bfloat16 hv[16];
+                    // bias, ReLU and the bf16 rounding of two columns per instruction
+                    uint32_t hw[8];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) hv[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[i], 0.0f));
+                    for (int i = 0; i < 8; ++i) hw[i] = pack_relu_bf16x2(v[2 * i] + bias[2 * i], v[2 * i + 1] + bias[2 * i + 1]);
                     unsigned char* dst = act(smem, l + 1);
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0, kActDim)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(dst + core_offset(tid, c0 + 8, kActDim)) =
-                        *reinterpret_cast<const int4*>(hv + 8);
+                    *reinterpret_cast<uint4*>(dst + core_offset(tid, c0, kActDim)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(dst + core_offset(tid, c0 + 8, kActDim)) =
+                        make_uint4(hw[4], hw[5], hw[6], hw[7]);
                 } else {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[c0 + i] = v[i] + bias[i];
@@ -231,18 +235,32 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
             float dy[kOut];
             const float lq = mixture_loss_grad(y, r[9], r[10], r[11], g, dy);
             if (row < n) loss_acc += g * lq;
-            __align__(16) __nv_bfloat16 dv[kOut];
-#pragma unroll
-            for (int i = 0; i < kOut; ++i) dv[i] = __float2bfloat16_rn(dy[i]);
 #pragma unroll
             for (int kc = 0; kc < kOut / 8; ++kc)
-                *reinterpret_cast<int4*>(smem + kTrOffDY + core_offset(tid, kc * 8, kOut)) =
-                    *reinterpret_cast<const int4*>(dv + kc * 8);
+                *reinterpret_cast<uint4*>(smem + kTrOffDY + core_offset(tid, kc * 8, kOut)) =
+                    make_uint4(pack_bf16x2(dy[8 * kc], dy[8 * kc + 1]), pack_bf16x2(dy[8 * kc + 2], dy[8 * kc + 3]),
+                               pack_bf16x2(dy[8 * kc + 4], dy[8 * kc + 5]), pack_bf16x2(dy[8 * kc + 6], dy[8 * kc + 7]));
+            // warp sums of the 48 outputs' dY by recursive halving (padded to 64): at the step with lane offset o
+            // a lane keeps the half of its partial sums that its lane bit o selects and adds the partner's copy of
+            // it, so that lane l ends with the sums of outputs 2l and 2l + 1
+            {
+                float t[64];
 #pragma unroll
-            for (int i = 0; i < kOut; ++i) {
-                float s = dy[i];
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-                if (lane == 0 && s != 0.f) atomicAdd(&gb4[i], s);
+                for (int i = 0; i < 64; ++i) t[i] = i < kOut ? dy[i] : 0.f;
+#pragma unroll
+                for (int h = 32, o = 16; h >= 2; h >>= 1, o >>= 1) {
+                    const bool up = (lane & o) != 0;
+#pragma unroll
+                    for (int i = 0; i < h; ++i) {
+                        const float send = up ? t[i] : t[i + h];
+                        const float keep = up ? t[i + h] : t[i];
+                        t[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
+                    }
+                }
+                if (2 * lane < kOut) {
+                    if (t[0] != 0.f) atomicAdd(&gb4[2 * lane], t[0]);
+                    if (t[1] != 0.f) atomicAdd(&gb4[2 * lane + 1], t[1]);
+                }
             }
         }
         publish();
@@ -281,16 +299,17 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
                     float v[16];
                     tmem_ld16(lane_base + kAccCol + c0, v);
                     tmem_wait_ld();
-                    __align__(16) __nv_bfloat16 hv[16];
-                    *reinterpret_cast<int4*>(hv) = *reinterpret_cast<const int4*>(a + core_offset(tid, c0, kActDim));
-                    *reinterpret_cast<int4*>(hv + 8) =
-                        *reinterpret_cast<const int4*>(a + core_offset(tid, c0 + 8, kActDim));
+                    // a_l > 0 tested on the bf16 bits (a ReLU output: +0 or positive), two columns per word
+                    uint4 w0 = *reinterpret_cast<const uint4*>(a + core_offset(tid, c0, kActDim));
+                    uint4 w1 = *reinterpret_cast<const uint4*>(a + core_offset(tid, c0 + 8, kActDim));
+                    uint32_t aw[8] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        hv[i] = __float2bfloat16_rn(__bfloat162float(hv[i]) > 0.f ? v[i] : 0.f);
-                    *reinterpret_cast<int4*>(a + core_offset(tid, c0, kActDim)) = *reinterpret_cast<const int4*>(hv);
-                    *reinterpret_cast<int4*>(a + core_offset(tid, c0 + 8, kActDim)) =
-                        *reinterpret_cast<const int4*>(hv + 8);
+                    for (int i = 0; i < 8; ++i)
+                        aw[i] = pack_bf16x2(bf16_positive(aw[i] & 0xFFFFu) ? v[2 * i] : 0.f,
+                                            bf16_positive(aw[i] >> 16) ? v[2 * i + 1] : 0.f);
+                    *reinterpret_cast<uint4*>(a + core_offset(tid, c0, kActDim)) = make_uint4(aw[0], aw[1], aw[2], aw[3]);
+                    *reinterpret_cast<uint4*>(a + core_offset(tid, c0 + 8, kActDim)) =
+                        make_uint4(aw[4], aw[5], aw[6], aw[7]);
                 }
                 publish();
             }
