@@ -73,13 +73,13 @@ def test_full_size_stress_properties():
 
 
 def test_host_calls_chunked_equal_device_calls():
-    """The host-array calls pipeline batches above 2^19 rays in chunks over three streams; a 1.3M-ray batch
-    (three chunks, the last one partial) gives the same hits and flags as the device-pointer calls, and the
-    same traversal counters."""
+    """The host-array calls pipeline batches above 2^20 rays in chunks over three streams (2^20 rays each, a
+    quarter and a half chunk at either end from 2^21 rays on); a 2.4M-ray batch (the ramped schedule, one body
+    chunk partial) gives the same hits and flags as the device-pointer calls, and the same traversal counters."""
     import torch
 
     soup = scenes.triangle_soup(1 << 18, seed=4)
-    n = (1 << 20) + 300_001
+    n = (1 << 21) + 300_001
     rays = scenes.soup_rays(n, seed=5, kind="closest")
     srays = scenes.soup_rays(n, seed=6, kind="any")
     with _api().Accel(soup) as acc:
