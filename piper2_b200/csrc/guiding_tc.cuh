@@ -200,6 +200,9 @@ __device__ __forceinline__ void forward_tc_tiles(const GuideView& gv, uint32_t n
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::kOffBar) + g;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::kOffSlot);
     volatile uint32_t& s_fail = reinterpret_cast<uint32_t*>(smem + L::kOffFail)[g];
+    // a CTA without a tile (the in-render queue is often empty or short) leaves before staging weights or
+    // allocating tensor memory; the condition is the same for all its threads
+    if ((uint64_t)blockIdx.x * G * kTcRows >= n) return;
 
     // weights: padded row-major bf16 image -> core-matrix layout, 16 bytes at a time (all groups)
     for (int l = 0; l < kLayers; ++l) {
