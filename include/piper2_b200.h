@@ -279,9 +279,10 @@ int pb2_trace_closest(const pb2_accel* accel, const pb2_ray* rays_dev, uint32_t 
 int pb2_trace_any(const pb2_accel* accel, const pb2_ray* rays_dev, uint32_t n, uint32_t* occluded_dev,
                   void* stream);
 /* The same two calls with host arrays: copies in, traces, copies out, synchronises `stream`.  Batches
- * of more than 2^19 rays are cut into chunks of 2^19 that three internal streams (created on the first
- * such call, kept until pb2_accel_destroy) upload, trace and download in turn, so the copies of one chunk
- * overlap the traversal of another; host arrays should be pinned for the copies to overlap. */
+ * of more than 2^20 rays are cut into chunks of 2^20 (from 2^21 rays on with a quarter and a half chunk at
+ * either end) that three internal streams (created on the first such call, kept until pb2_accel_destroy)
+ * upload, trace and download in turn, so the copies of one chunk overlap the traversal of another; host
+ * arrays should be pinned for the copies to overlap. */
 int pb2_trace_closest_host(const pb2_accel* accel, const pb2_ray* rays_host, uint32_t n,
                            pb2_hit* hits_host, void* stream);
 int pb2_trace_any_host(const pb2_accel* accel, const pb2_ray* rays_host, uint32_t n,
