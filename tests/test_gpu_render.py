@@ -354,3 +354,23 @@ def test_bounce_graphs_equal_plain_launches(oracle):
         assert np.array_equal(a.view(np.uint32), c.view(np.uint32)), f"launch {k}: updated graphs differ"
     _, osamples = oracle.OracleScene(sd, use_bvh=False).render(sd.settings)
     assert np.array_equal(graphed[0].view(np.uint32), osamples.view(np.uint32))
+
+
+def test_refill_over_many_bitmap_blocks_bitexact():
+    """A refilled launch whose free-slot bitmap spans several 1024-word scan blocks (2^21 slots: 64 blocks) gives
+    the samples of the same launch with every path in its own slot, bit for bit."""
+    import torch
+
+    sd = scenes.cornell_box(seed=6, width=256, height=256, spp=48)  # 3.1M paths
+    outs = []
+    with _api().Pipeline(sd) as pl:
+        for slots in (1 << 21, 1 << 22):
+            pl.set_path_slots(slots)
+            film = pl.new_film()
+            out = torch.zeros((256, 256, 48, 5), dtype=torch.float32, device="cuda")
+            pl.launch(film, pl.rect, 0, 48, sample_out=out)
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy())
+            del out
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.all(outs[0][..., 4] >= 0.0) and np.count_nonzero(outs[0][..., 0]) > 0
