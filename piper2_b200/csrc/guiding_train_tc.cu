@@ -30,7 +30,7 @@ namespace pb2 {
 namespace guide {
 namespace {
 
-constexpr int kTrThreads = 128;
+constexpr int kTrThreads = 256;  // two warps per TMEM lane quarter: warps w and w + 4 split a layer's columns
 constexpr int kActDim = 72;                            // a_1..a_4: 64 features, the constant 1, 7 zeros
 constexpr int kTrXBytes = kTcRows * kIn * 2;           // a_0: 24,576
 constexpr int kTrABytes = kTcRows * kActDim * 2;       // a_1..a_4: 18,432 each
@@ -89,6 +89,11 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
                                                           uint32_t* __restrict__ error, uint32_t skip_commit) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // warps 0-3 own the tile's records (thread tid = record and TMEM lane tid); warp w + 4 serves the same 32
+    // TMEM lanes as warp w and drains the other half of each accumulator's 16-column chunks
+    const bool owner = tid < kTcRows;
+    const int rowt = (warp & 3) * 32 + lane;        // this thread's record row / TMEM lane
+    const uint32_t half = (uint32_t)(warp >> 2);     // its chunks: c0 = 16 half, 16 half + 32, ...
     unsigned char* w_s = smem + kTrOffW;
     float* b_s = reinterpret_cast<float*>(smem + kTrOffBias);
     float* gb4 = reinterpret_cast<float*>(smem + kTrOffBias4);
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     }
     for (int i = tid; i < kBiasElems; i += kTrThreads) b_s[i] = gv.b32[i];
     for (int i = tid; i < kOut; i += kTrThreads) gb4[i] = 0.f;
-    for (int l = 1; l < kLayers; ++l) {
+    for (int l = 1; l < kLayers && owner; ++l) {
         __align__(16) __nv_bfloat16 one[8];
         for (int i = 0; i < 8; ++i) one[i] = __float2bfloat16_rn(i == 0 ? 1.f : 0.f);
         *reinterpret_cast<int4*>(act(smem, l) + core_offset(tid, 64, kActDim)) = *reinterpret_cast<const int4*>(one);
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t bar_addr = smem_u32(bar);
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 TMEM lanes
+    const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's 32 TMEM lanes
     uint32_t phase = 0;
     bool failed = false;
     const float wsum = scalars[0];
@@ -171,7 +176,10 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
         const uint32_t row = tile * kTcRows + tid;
         cur_tile = tile;
         float r[16];
-        if (row < n) {
+        if (!owner) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) r[q] = 0.f;
+        } else if (row < n) {
             const float4* p = reinterpret_cast<const float4*>(rec + 16 * (size_t)row);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -183,7 +191,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
             for (int q = 0; q < 16; ++q) r[q] = 0.f;
             r[5] = 1.f; r[8] = 1.f; r[11] = 1.f;  // unit directions, zero weight: no contribution
         }
-        {
+        if (owner) {
             __align__(16) __nv_bfloat16 enc[kIn];
             encode_row(r, enc);
 #pragma unroll
@@ -207,21 +215,30 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
                 failed = true;
                 break;
             }
-            for (uint32_t c0 = 0; c0 < ndim; c0 += 16) {
-                float v[16];
-                tmem_ld16(lane_base + kAccCol + c0, v);
-                tmem_wait_ld();
-                const float* bias = b_s + bias_offset(l) + c0;
-                if (l < kLayers - 1) {
+            if (l < kLayers - 1) {
+                // hidden layers: both warps of a lane quarter, alternate 16-column chunks
+                for (uint32_t c0 = 16u * half; c0 < ndim; c0 += 32u) {
+                    float v[16];
+                    tmem_ld16(lane_base + kAccCol + c0, v);
+                    tmem_wait_ld();
+                    const float* bias = b_s + bias_offset(l) + c0;
                     // bias, ReLU and the bf16 rounding of two columns per instruction
                     uint32_t hw[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) hw[i] = pack_relu_bf16x2(v[2 * i] + bias[2 * i], v[2 * i + 1] + bias[2 * i + 1]);
                     unsigned char* dst = act(smem, l + 1);
-                    *reinterpret_cast<uint4*>(dst + core_offset(tid, c0, kActDim)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    *reinterpret_cast<uint4*>(dst + core_offset(tid, c0 + 8, kActDim)) =
+                    *reinterpret_cast<uint4*>(dst + core_offset(rowt, c0, kActDim)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(dst + core_offset(rowt, c0 + 8, kActDim)) =
                         make_uint4(hw[4], hw[5], hw[6], hw[7]);
-                } else {
+                }
+            } else if (owner) {
+                // the output layer: the record owners, all 48 columns (y stays in registers for the loss gradient)
+#pragma unroll
+                for (int c0 = 0; c0 < kOut; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(lane_base + kAccCol + c0, v);
+                    tmem_wait_ld();
+                    const float* bias = b_s + bias_offset(l) + c0;
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[c0 + i] = v[i] + bias[i];
                 }
@@ -230,7 +247,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
         }
         if (failed) break;
         // ---- loss gradient of this record (fp32), its bf16 copy for the MMAs, the output-bias sums ----
-        {
+        if (owner) {
             const float g = r[12] * gscale;
             float dy[kOut];
             const float lq = mixture_loss_grad(y, r[9], r[10], r[11], g, dy);
@@ -295,20 +312,20 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
             if (l > 0) {
                 // dZ_{l-1} = bf16(dA_l) where a_l > 0, over a_l (this thread's row only)
                 unsigned char* a = act(smem, l);
-                for (uint32_t c0 = 0; c0 < in; c0 += 16) {
+                for (uint32_t c0 = 16u * half; c0 < in; c0 += 32u) {
                     float v[16];
                     tmem_ld16(lane_base + kAccCol + c0, v);
                     tmem_wait_ld();
                     // a_l > 0 tested on the bf16 bits (a ReLU output: +0 or positive), two columns per word
-                    uint4 w0 = *reinterpret_cast<const uint4*>(a + core_offset(tid, c0, kActDim));
-                    uint4 w1 = *reinterpret_cast<const uint4*>(a + core_offset(tid, c0 + 8, kActDim));
+                    uint4 w0 = *reinterpret_cast<const uint4*>(a + core_offset(rowt, c0, kActDim));
+                    uint4 w1 = *reinterpret_cast<const uint4*>(a + core_offset(rowt, c0 + 8, kActDim));
                     uint32_t aw[8] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
 #pragma unroll
                     for (int i = 0; i < 8; ++i)
                         aw[i] = pack_bf16x2(bf16_positive(aw[i] & 0xFFFFu) ? v[2 * i] : 0.f,
                                             bf16_positive(aw[i] >> 16) ? v[2 * i + 1] : 0.f);
-                    *reinterpret_cast<uint4*>(a + core_offset(tid, c0, kActDim)) = make_uint4(aw[0], aw[1], aw[2], aw[3]);
-                    *reinterpret_cast<uint4*>(a + core_offset(tid, c0 + 8, kActDim)) =
+                    *reinterpret_cast<uint4*>(a + core_offset(rowt, c0, kActDim)) = make_uint4(aw[0], aw[1], aw[2], aw[3]);
+                    *reinterpret_cast<uint4*>(a + core_offset(rowt, c0 + 8, kActDim)) =
                         make_uint4(aw[4], aw[5], aw[6], aw[7]);
                 }
                 publish();
@@ -325,11 +342,11 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
     // ---- this CTA's partial gradient: dW_l^T row f (this thread's TMEM lane) -> W_l[:, f]; the constant
     // feature's row -> the bias of layers 0..3; the output bias from the fp32 sums ----
     float* out = partial + (size_t)blockIdx.x * kParams;
-    const uint32_t f = (uint32_t)tid;
+    const uint32_t f = (uint32_t)rowt;
     for (int l = 0; l < kLayers; ++l) {
         const uint32_t in = layer_in(l), outd = layer_out(l);
         const uint32_t bias_row = l == 0 ? 84u : 64u;
-        for (uint32_t c0 = 0; c0 < outd; c0 += 16) {
+        for (uint32_t c0 = 16u * half; c0 < outd; c0 += 32u) {
             float v[16];
             tmem_ld16(lane_base + dw_col(l) + c0, v);
             tmem_wait_ld();
