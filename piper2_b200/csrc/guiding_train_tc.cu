@@ -1,6 +1,8 @@
 // guiding_train_tc.cu -- the guiding network's loss gradient on the 5th-generation tensor cores (tcgen05).
 //
-// One CTA of 4 warps per SM walks 128-record tiles.  Per tile, with thread t owning record t:
+// One CTA of 8 warps per SM walks 128-record tiles.  Thread t < 128 owns record t; thread t + 128 (warp w + 4)
+// serves the same record and TMEM lane: it drains alternate 16-column chunks of the hidden-layer, backward-data and
+// final epilogues and computes lobes 4-7 of the record's loss gradient.  Per tile:
 //   forward   5 MMAs  a_l (128 x in_l, K-major) x W_l^T -> TMEM; epilogue bias + ReLU -> bf16 a_{l+1}
 //   loss      per record: dY = d(-g log q)/dy from the 48 raw outputs (fp32; bf16 copy for the MMAs)
 //   backward  for l = 4 .. 0:
@@ -43,7 +45,12 @@ constexpr int kTrOffSlack = kTrOffDY + kTrDYBytes;     // rows past a tile's fea
 constexpr int kTrOffBias = kTrOffSlack + 2048;
 constexpr int kTrOffBias4 = kTrOffBias + kBiasElems * 4;  // fp32 output-bias gradient of this CTA
 constexpr int kTrOffBar = kTrOffBias4 + kOut * 4;
-constexpr int kTrSmem = kTrOffBar + 16;
+// the loss gradient's exchange between a record's two threads, per record: the raw outputs of lobes 4-7 (20), the
+// sampled direction and loss weight (4), the two halves' softmax maxima, sums and density parts (6), the second
+// half's output deltas (20); 52 floats with padding
+constexpr int kXchStride = 52;
+constexpr int kTrOffXch = kTrOffBar + 16;
+constexpr int kTrSmem = kTrOffXch + kTcRows * kXchStride * 4;
 static_assert(kTrOffX % 1024 == 0 && kTrOffA1 % 1024 == 0 && kTrABytes % 1024 == 0 && kTrOffDY % 1024 == 0,
               "operand alignment");
 static_assert(kTrSmem <= 227 * 1024, "shared memory per CTA");
@@ -247,36 +254,126 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_grad_tc(GuideView gv, const f
         }
         if (failed) break;
         // ---- loss gradient of this record (fp32), its bf16 copy for the MMAs, the output-bias sums ----
-        if (owner) {
-            const float g = r[12] * gscale;
-            float dy[kOut];
-            const float lq = mixture_loss_grad(y, r[9], r[10], r[11], g, dy);
-            if (row < n) loss_acc += g * lq;
+        // The record's two threads split the mixture's eight lobes (half 0: lobes 0-3, half 1: lobes 4-7, as
+        // mixture_loss_grad computes them) and combine the softmax maximum and sum and the density q through xr.
+        {
+            float* xr = reinterpret_cast<float*>(smem + kTrOffXch) + (size_t)rowt * kXchStride;
+            float g = 0.f, wx = 0.f, wy = 0.f, wz = 0.f;
+            float yl[20];
+            if (owner) {
+                g = r[12] * gscale;
+                wx = r[9];
+                wy = r[10];
+                wz = r[11];
 #pragma unroll
-            for (int kc = 0; kc < kOut / 8; ++kc)
-                *reinterpret_cast<uint4*>(smem + kTrOffDY + core_offset(tid, kc * 8, kOut)) =
-                    make_uint4(pack_bf16x2(dy[8 * kc], dy[8 * kc + 1]), pack_bf16x2(dy[8 * kc + 2], dy[8 * kc + 3]),
-                               pack_bf16x2(dy[8 * kc + 4], dy[8 * kc + 5]), pack_bf16x2(dy[8 * kc + 6], dy[8 * kc + 7]));
-            // warp sums of the 48 outputs' dY by recursive halving (padded to 64): at the step with lane offset o
-            // a lane keeps the half of its partial sums that its lane bit o selects and adds the partner's copy of
-            // it, so that lane l ends with the sums of outputs 2l and 2l + 1
-            {
-                float t[64];
+                for (int i = 0; i < 20; ++i) xr[i] = y[20 + i];
+                xr[20] = wx;
+                xr[21] = wy;
+                xr[22] = wz;
+                xr[23] = g;
+            }
+            __syncthreads();
+            if (owner) {
 #pragma unroll
-                for (int i = 0; i < 64; ++i) t[i] = i < kOut ? dy[i] : 0.f;
+                for (int i = 0; i < 20; ++i) yl[i] = y[i];
+            } else {
 #pragma unroll
-                for (int h = 32, o = 16; h >= 2; h >>= 1, o >>= 1) {
-                    const bool up = (lane & o) != 0;
+                for (int i = 0; i < 20; ++i) yl[i] = xr[i];
+                wx = xr[20];
+                wy = xr[21];
+                wz = xr[22];
+                g = xr[23];
+            }
+            float mx = -3.0e38f;
 #pragma unroll
-                    for (int i = 0; i < h; ++i) {
-                        const float send = up ? t[i] : t[i + h];
-                        const float keep = up ? t[i + h] : t[i];
-                        t[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
-                    }
+            for (int k = 0; k < 4; ++k) mx = fmaxf(mx, yl[5 * k]);
+            xr[24 + half] = mx;
+            __syncthreads();
+            mx = fmaxf(xr[24], xr[25]);
+            float wl[4], sum = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                wl[k] = expf(yl[5 * k] - mx);
+                sum += wl[k];
+            }
+            xr[26 + half] = sum;
+            __syncthreads();
+            sum = xr[26] + xr[27];
+            float mu[4][3], kap[4], comp[4], qpart = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                wl[k] /= sum;
+                const float vx = yl[5 * k + 1], vy = yl[5 * k + 2], vz = yl[5 * k + 3];
+                const float nv = sqrtf(vx * vx + vy * vy + vz * vz);
+                if (nv > 1e-12f) { mu[k][0] = vx / nv; mu[k][1] = vy / nv; mu[k][2] = vz / nv; }
+                else { mu[k][0] = 0.f; mu[k][1] = 0.f; mu[k][2] = 1.f; }
+                kap[k] = fminf(softplus(yl[5 * k + 4]) + kKappaMin, kKappaMax);
+                comp[k] = vmf_eval(mu[k], kap[k], wx, wy, wz);
+                qpart += wl[k] * comp[k];
+            }
+            xr[28 + half] = qpart;
+            __syncthreads();
+            const float qs = fmaxf(xr[28] + xr[29], 1e-30f);
+            float dl[20];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float resp = wl[k] * comp[k] / qs;
+                dl[5 * k] = g * (resp - wl[k]);
+                const float kk = kap[k];
+                const float mdw = mu[k][0] * wx + mu[k][1] * wy + mu[k][2] * wz;
+                const float dlogk = 1.f / kk - 2.f / expm1f(2.f * kk) + (mdw - 1.f);
+                const float raw = yl[5 * k + 4];
+                const float sig = 1.f / (1.f + expf(-raw));
+                const bool free_k = softplus(raw) + kKappaMin < kKappaMax;
+                dl[5 * k + 4] = free_k ? g * resp * dlogk * sig : 0.f;
+                const float vx = yl[5 * k + 1], vy = yl[5 * k + 2], vz = yl[5 * k + 3];
+                const float vn = fmaxf(sqrtf(vx * vx + vy * vy + vz * vz), 1e-30f);
+                const float sc = g * resp * kk / vn;
+                dl[5 * k + 1] = sc * (wx - mdw * mu[k][0]);
+                dl[5 * k + 2] = sc * (wy - mdw * mu[k][1]);
+                dl[5 * k + 3] = sc * (wz - mdw * mu[k][2]);
+            }
+            if (!owner) {
+#pragma unroll
+                for (int i = 0; i < 20; ++i) xr[30 + i] = dl[i];
+            }
+            __syncthreads();
+            if (owner) {
+                float dy[kOut];
+    #pragma unroll
+                for (int i = 0; i < 20; ++i) {
+                    dy[i] = dl[i];
+                    dy[20 + i] = xr[30 + i];
                 }
-                if (2 * lane < kOut) {
-                    if (t[0] != 0.f) atomicAdd(&gb4[2 * lane], t[0]);
-                    if (t[1] != 0.f) atomicAdd(&gb4[2 * lane + 1], t[1]);
+    #pragma unroll
+                for (int i = 5 * kLobes; i < kOut; ++i) dy[i] = 0.f;
+                if (row < n) loss_acc += g * logf(qs);
+    #pragma unroll
+                for (int kc = 0; kc < kOut / 8; ++kc)
+                    *reinterpret_cast<uint4*>(smem + kTrOffDY + core_offset(tid, kc * 8, kOut)) =
+                        make_uint4(pack_bf16x2(dy[8 * kc], dy[8 * kc + 1]), pack_bf16x2(dy[8 * kc + 2], dy[8 * kc + 3]),
+                                   pack_bf16x2(dy[8 * kc + 4], dy[8 * kc + 5]), pack_bf16x2(dy[8 * kc + 6], dy[8 * kc + 7]));
+                // warp sums of the 48 outputs' dY by recursive halving (padded to 64): at the step with lane offset o
+                // a lane keeps the half of its partial sums that its lane bit o selects and adds the partner's copy of
+                // it, so that lane l ends with the sums of outputs 2l and 2l + 1
+                {
+                    float t[64];
+    #pragma unroll
+                    for (int i = 0; i < 64; ++i) t[i] = i < kOut ? dy[i] : 0.f;
+    #pragma unroll
+                    for (int h = 32, o = 16; h >= 2; h >>= 1, o >>= 1) {
+                        const bool up = (lane & o) != 0;
+    #pragma unroll
+                        for (int i = 0; i < h; ++i) {
+                            const float send = up ? t[i] : t[i + h];
+                            const float keep = up ? t[i + h] : t[i];
+                            t[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
+                        }
+                    }
+                    if (2 * lane < kOut) {
+                        if (t[0] != 0.f) atomicAdd(&gb4[2 * lane], t[0]);
+                        if (t[1] != 0.f) atomicAdd(&gb4[2 * lane + 1], t[1]);
+                    }
                 }
             }
         }
